@@ -1,0 +1,278 @@
+"""B200 Flux Reconstruction residual and RK update (FlurryPP's solver path).
+
+Python binding of ``libfr_b200.so`` (C ABI in ``include/fr_b200.h``).  The
+``Solver`` class mirrors the reference ``solver`` interface
+(``include/solver.hpp:147-178``): it is set up from a reference input deck,
+``calc_residual(step)`` fills ``divF_spts[step]`` and ``update()`` advances one
+time step.  State arrays keep the reference layout
+``[point][element][field]``.
+
+The compute path is the CUDA library only: if ``libfr_b200.so`` is missing or
+does not load, importing :mod:`flurrypp_b200` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfr_b200.so")
+
+FR_OK = 0
+FR_ERR_ARG = 1
+FR_ERR_SETUP = 2
+FR_ERR_CUDA = 3
+FR_ERR_NONFINITE = 4
+FR_ERR_BUDGET = 5
+FR_ERR_TIMEOUT = 6
+FR_ERR_UNSUPPORTED = 7
+FR_ERR_STATE = 8
+
+FR_PREC_FP64 = 0
+FR_PREC_MIXED = 1
+
+IC_DECK, IC_VORTEX, IC_TGV, IC_UNIFORM = 0, 1, 2, 3
+
+
+class FrError(RuntimeError):
+    """A non-zero status from the library, with its message."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[fr status {code}] {msg}")
+        self.code = code
+
+
+class SetupOpts(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int),
+        ("perturb", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong),
+        ("perturb_frac", ctypes.c_double),
+        ("mu_override", ctypes.c_int),
+        ("mu_inf", ctypes.c_double),
+        ("visc_flux_quirk", ctypes.c_int),
+        ("debug_arrays", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class Mesh(ctypes.Structure):
+    _fields_ = [
+        ("nDims", ctypes.c_int),
+        ("nVerts", ctypes.c_int),
+        ("xv", ctypes.POINTER(ctypes.c_double)),
+        ("nEles", ctypes.c_int),
+        ("nNodes", ctypes.c_int),
+        ("c2v", ctypes.POINTER(ctypes.c_int)),
+        ("nBndFaces", ctypes.c_int),
+        ("bndFaceVerts", ctypes.POINTER(ctypes.c_int)),
+        ("bndFaceBc", ctypes.POINTER(ctypes.c_int)),
+        ("period", ctypes.c_double * 3),
+    ]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("nDims", ctypes.c_int),
+        ("nFields", ctypes.c_int),
+        ("order", ctypes.c_int),
+        ("nEles", ctypes.c_int),
+        ("nSpts", ctypes.c_int),
+        ("nFpts", ctypes.c_int),
+        ("nFaces", ctypes.c_int),
+        ("nFacePts", ctypes.c_int),
+        ("nRKSteps", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("dtType", ctypes.c_int),
+        ("timeType", ctypes.c_int),
+        ("iter", ctypes.c_longlong),
+        ("time", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("launches", ctypes.c_longlong),
+    ]
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    i = ctypes.c_int
+    dp = ctypes.POINTER(ctypes.c_double)
+    sz = ctypes.c_size_t
+    sigs = {
+        "fr_setup_opts_default": (None, [ctypes.POINTER(SetupOpts)]),
+        "fr_create_from_deck": (i, [ctypes.c_char_p, ctypes.POINTER(SetupOpts), ctypes.POINTER(P)]),
+        "fr_create_with_mesh": (i, [ctypes.c_char_p, ctypes.POINTER(Mesh), ctypes.POINTER(SetupOpts), ctypes.POINTER(P)]),
+        "fr_destroy": (None, [P]),
+        "fr_last_error": (ctypes.c_char_p, [P]),
+        "fr_get_info": (i, [P, ctypes.POINTER(Info)]),
+        "fr_set_stream": (i, [P, P]),
+        "fr_init_solution": (i, [P, i, dp, i]),
+        "fr_set_state": (i, [P, dp, sz]),
+        "fr_get_state": (i, [P, dp, sz]),
+        "fr_calc_residual": (i, [P, i]),
+        "fr_get_residual": (i, [P, i, dp, sz]),
+        "fr_update": (i, [P, i]),
+        "fr_run": (i, [P, i]),
+        "fr_calc_dt": (i, [P, dp]),
+        "fr_set_dt": (i, [P, ctypes.c_double]),
+        "fr_residual_norm": (i, [P, i, dp, i]),
+        "fr_check_state": (i, [P]),
+        "fr_get_array": (i, [P, ctypes.c_char_p, P, ctypes.POINTER(sz)]),
+        "fr_device_ptr": (i, [P, ctypes.c_char_p, ctypes.POINTER(P), ctypes.POINTER(sz)]),
+        "fr_synchronize": (i, [P]),
+        "fr_bench_kernel": (i, [P, ctypes.c_char_p, i]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def default_opts(**kw) -> SetupOpts:
+    o = SetupOpts()
+    lib.fr_setup_opts_default(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """One FR case on the GPU (the reference ``solver`` + its ``input``)."""
+
+    def __init__(self, deck: str, mesh: dict | None = None, **opts):
+        self._c = ctypes.c_void_p()
+        o = default_opts(**opts)
+        if mesh is None:
+            st = lib.fr_create_from_deck(deck.encode(), ctypes.byref(o), ctypes.byref(self._c))
+        else:
+            self._mesh_keep = m = _make_mesh(mesh)
+            st = lib.fr_create_with_mesh(deck.encode(), ctypes.byref(m[0]), ctypes.byref(o), ctypes.byref(self._c))
+        if st != FR_OK:
+            msg = lib.fr_last_error(self._c).decode() if self._c else "allocation failed"
+            lib.fr_destroy(self._c)
+            self._c = None
+            raise FrError(st, msg)
+        inf = self.info()
+        self.nDims, self.nFields, self.order = inf.nDims, inf.nFields, inf.order
+        self.nEles, self.nSpts, self.nFpts = inf.nEles, inf.nSpts, inf.nFpts
+        self.nRKSteps = inf.nRKSteps
+        self.shape = (self.nSpts, self.nEles, self.nFields)
+
+    def __del__(self):
+        if getattr(self, "_c", None):
+            lib.fr_destroy(self._c)
+            self._c = None
+
+    def close(self):
+        self.__del__()
+
+    def _check(self, st: int):
+        if st != FR_OK:
+            raise FrError(st, lib.fr_last_error(self._c).decode())
+
+    def info(self) -> Info:
+        inf = Info()
+        self._check(lib.fr_get_info(self._c, ctypes.byref(inf)))
+        return inf
+
+    def initialize_solution(self, kind: int = IC_DECK, prm=()):
+        p = np.ascontiguousarray(prm, dtype=np.float64)
+        self._check(lib.fr_init_solution(self._c, kind, _dptr(p) if p.size else None, int(p.size)))
+
+    def set_state(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self._check(lib.fr_set_state(self._c, _dptr(U), U.size))
+
+    def get_state(self) -> np.ndarray:
+        U = np.empty(self.shape, dtype=np.float64)
+        self._check(lib.fr_get_state(self._c, _dptr(U), U.size))
+        return U
+
+    def calc_residual(self, step: int = 0):
+        self._check(lib.fr_calc_residual(self._c, step))
+
+    def get_residual(self, step: int = 0) -> np.ndarray:
+        d = np.empty(self.shape, dtype=np.float64)
+        self._check(lib.fr_get_residual(self._c, step, _dptr(d), d.size))
+        return d
+
+    def update(self, pmg_source: bool = False):
+        self._check(lib.fr_update(self._c, int(pmg_source)))
+
+    def run(self, nsteps: int):
+        self._check(lib.fr_run(self._c, nsteps))
+
+    def calc_dt(self) -> float:
+        d = ctypes.c_double()
+        self._check(lib.fr_calc_dt(self._c, ctypes.byref(d)))
+        return d.value
+
+    def set_dt(self, dt: float):
+        self._check(lib.fr_set_dt(self._c, float(dt)))
+
+    def residual_norm(self, res_type: int = 2) -> np.ndarray:
+        out = np.empty(self.nFields, dtype=np.float64)
+        self._check(lib.fr_residual_norm(self._c, res_type, _dptr(out), self.nFields))
+        return out
+
+    def check_state(self):
+        self._check(lib.fr_check_state(self._c))
+
+    def synchronize(self):
+        self._check(lib.fr_synchronize(self._c))
+
+    def get_array(self, name: str) -> np.ndarray:
+        n = ctypes.c_size_t(0)
+        self._check(lib.fr_get_array(self._c, name.encode(), None, ctypes.byref(n)))
+        dt = np.int32 if name.startswith("face_") else np.float64
+        a = np.empty(n.value, dtype=dt)
+        self._check(lib.fr_get_array(self._c, name.encode(), a.ctypes.data_as(ctypes.c_void_p), ctypes.byref(n)))
+        return a
+
+    def set_stream(self, stream_handle: int):
+        """Run this case's kernels on a given cudaStream_t (e.g. torch's)."""
+        self._check(lib.fr_set_stream(self._c, ctypes.c_void_p(stream_handle)))
+
+    def bench_kernel(self, kernel: str, reps: int):
+        self._check(lib.fr_bench_kernel(self._c, kernel.encode(), reps))
+
+    def device_ptr(self, name: str):
+        p = ctypes.c_void_p()
+        b = ctypes.c_size_t()
+        self._check(lib.fr_device_ptr(self._c, name.encode(), ctypes.byref(p), ctypes.byref(b)))
+        return p.value, b.value
+
+
+def _make_mesh(m: dict):
+    xv = np.ascontiguousarray(m["xv"], dtype=np.float64)
+    c2v = np.ascontiguousarray(m["c2v"], dtype=np.int32)
+    bfv = np.ascontiguousarray(m["bnd_face_verts"], dtype=np.int32).reshape(-1, 4)
+    bfb = np.ascontiguousarray(m["bnd_face_bc"], dtype=np.int32)
+    M = Mesh()
+    M.nDims = int(xv.shape[1])
+    M.nVerts = int(xv.shape[0])
+    M.xv = xv.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    M.nEles = int(c2v.shape[0])
+    M.nNodes = int(c2v.shape[1])
+    M.c2v = c2v.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    M.nBndFaces = int(bfb.size)
+    M.bndFaceVerts = bfv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    M.bndFaceBc = bfb.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    per = m.get("period", (1e300, 1e300, 1e300))
+    for d in range(3):
+        M.period[d] = float(per[d])
+    return (M, xv, c2v, bfv, bfb)

@@ -1,0 +1,879 @@
+// fr_case: one FR solver instance on the GPU, and the C ABI (include/fr_b200.h).
+//
+// The host side mirrors the reference `solver` (src/solver.cpp): setup builds
+// mesh, faces, operators and metrics on the host, then everything the stages
+// touch lives in device memory for the life of the case.  update() issues the
+// same sequence of steps as solver::update (solver.cpp:319-363), each stage as
+// a face kernel plus a fused element kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fr_b200.h"
+#include "host/fr_host.hpp"
+#include "kernels/stage.hpp"
+
+namespace {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct fr_case {
+  std::string err;
+  fr_setup_opts opts;
+  fr::Input in;
+  fr::Mesh mesh;
+  fr::Geometry geo;
+  fr::Operators op;
+  std::vector<fr::Face> faces;
+  int nDims = 0, nF = 0, nS = 0, nFp = 0, E = 0, nPF = 0, nRK = 0;
+  long long iter = 0;
+  long long launches = 0;  // kernels launched (graph replays counted per kernel)
+  int graphKernels = 0;    // kernels in the captured step
+  double hostDt = 0.0;
+  bool stateSet = false;
+  bool fptsFresh = false;  // U_fpts holds the extrapolation of U_spts
+  cudaStream_t stream = nullptr;
+  std::vector<DevBuf> allocs;
+
+  // device arrays
+  double *U = nullptr, *U0 = nullptr, *acc = nullptr, *Ufpts = nullptr, *Fn = nullptr;
+  std::vector<double *> divF;
+  double *waveSp = nullptr, *detJ = nullptr, *JGinv = nullptr, *norm = nullptr, *dA = nullptr;
+  double *wSpt = nullptr, *wSurf = nullptr, *eleDt = nullptr, *dt = nullptr, *timeAcc = nullptr;
+  double *eleRes = nullptr, *src = nullptr;
+  double *Fdbg = nullptr, *disFnDbg = nullptr;
+  unsigned long long *dtBits = nullptr;
+  unsigned int *bad = nullptr;
+  frk::FaceTable ft;
+  frk::Csr grad[3], extFn[3], corr, ext;
+  int EB = 1;
+  frk::Phys ph{};
+  cudaGraphExec_t graph = nullptr;
+  bool ownStream = false;
+  bool hostOnly = false;  // set up without a device: setup arrays only
+
+  ~fr_case() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &b : allocs) cudaFree(b.p);
+    if (ownStream && ownedStream) cudaStreamDestroy(ownedStream);
+  }
+  cudaStream_t ownedStream = nullptr;
+
+  bool fail(int, const std::string &m) {
+    err = m;
+    return false;
+  }
+  template <typename T>
+  bool alloc(T *&p, size_t count) {
+    void *q = nullptr;
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+      err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return false;
+    }
+    cudaMemsetAsync(q, 0, bytes, stream);
+    allocs.push_back({q, bytes});
+    p = (T *)q;
+    return true;
+  }
+  template <typename T>
+  bool upload(T *&p, const std::vector<T> &h) {
+    if (!alloc(p, h.size())) return false;
+    cudaError_t e = cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+      err = std::string("cudaMemcpy: ") + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  }
+  bool cuda_ok(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      err = std::string(what) + ": " + cudaGetErrorString(e);
+      return false;
+    }
+    return true;
+  }
+
+  bool make_csr(const std::vector<double> &A, int rows, int cols, frk::Csr &out) {
+    std::vector<int> rp(rows + 1, 0), ci;
+    std::vector<double> v;
+    for (int r = 0; r < rows; r++) {
+      for (int c = 0; c < cols; c++) {
+        double a = A[(size_t)r * cols + c];
+        if (a != 0.0) {
+          ci.push_back(c);
+          v.push_back(a);
+        }
+      }
+      rp[r + 1] = (int)ci.size();
+    }
+    int *drp, *dci;
+    double *dv;
+    if (!upload(drp, rp) || !upload(dci, ci) || !upload(dv, v)) return false;
+    out.nRows = rows;
+    out.nCols = cols;
+    out.rowptr = drp;
+    out.col = dci;
+    out.val = dv;
+    return true;
+  }
+
+  bool setup(const fr_setup_opts &o) {
+    opts = o;
+    hostOnly = o.device < 0;
+    if (hostOnly) return setup_host();
+    if (cudaSetDevice(o.device) != cudaSuccess) return fail(FR_ERR_CUDA, "cudaSetDevice failed");
+    if (!stream && cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "stream create");
+    ownStream = true;
+    ownedStream = stream;
+    if (o.precision != FR_PREC_FP64)
+      return fail(FR_ERR_UNSUPPORTED, "mixed precision is served by the batch API");
+    if (in.viscous) return fail(FR_ERR_UNSUPPORTED, "viscous path not built into this case type");
+    if (!setup_host()) return false;
+
+    size_t nU = (size_t)nS * E * nF, nUf = (size_t)nFp * E * nF;
+    if (!alloc(U, nU) || !alloc(U0, nU) || !alloc(acc, nU) || !alloc(Ufpts, nUf) || !alloc(Fn, nUf))
+      return false;
+    divF.assign(nRK, nullptr);
+    for (int s = 0; s < nRK; s++)
+      if (!alloc(divF[s], nU)) return false;
+    if (!alloc(waveSp, (size_t)nFp * E) || !alloc(eleDt, E) || !alloc(dt, 1) || !alloc(timeAcc, 1) ||
+        !alloc(eleRes, (size_t)E * nF) || !alloc(dtBits, 1) || !alloc(bad, 1))
+      return false;
+    if (o.debug_arrays)
+      if (!alloc(Fdbg, (size_t)nDims * nU) || !alloc(disFnDbg, nUf)) return false;
+    if (!upload(detJ, geo.detJac_spts) || !upload(JGinv, geo.JGinv_spts) ||
+        !upload(norm, geo.norm_fpts) || !upload(dA, geo.dA_fpts))
+      return false;
+    if (!upload(wSpt, fr::spt_weights(nDims, in.order)) || !upload(wSurf, fr::face_weights(nDims, in.order)))
+      return false;
+    for (int d = 0; d < nDims; d++) {
+      if (!make_csr(op.grad[d], nS, nS, grad[d])) return false;
+      if (!make_csr(op.extFn[d], nFp, nS, extFn[d])) return false;
+    }
+    if (!make_csr(op.corr, nS, nFp, corr) || !make_csr(op.ext, nFp, nS, ext)) return false;
+
+    // face-point table, sorted by left slot for coalesced gathers
+    struct FP {
+      int sL, sR;
+      double n[3], aL, aR;
+    };
+    std::vector<FP> fps;
+    fps.reserve(faces.size() * nPF);
+    for (auto &f : faces)
+      for (int j = 0; j < nPF; j++) {
+        FP p{};
+        int fL = f.locL * nPF + j;
+        p.sL = fL * E + f.eL;
+        for (int d = 0; d < nDims; d++) p.n[d] = geo.norm_fpts[(size_t)p.sL * nDims + d];
+        p.aL = geo.dA_fpts[p.sL];
+        if (f.eR >= 0) {
+          p.sR = f.fptR[j] * E + f.eR;
+          p.aR = geo.dA_fpts[p.sR];
+        } else {
+          p.sR = -(f.bc + 2);
+          p.aR = 0.0;
+        }
+        fps.push_back(p);
+      }
+    std::sort(fps.begin(), fps.end(), [](const FP &a, const FP &b) { return a.sL < b.sL; });
+    std::vector<int> sL(fps.size()), sR(fps.size());
+    std::vector<double> nrm(fps.size() * nDims), aL(fps.size()), aR(fps.size());
+    for (size_t i = 0; i < fps.size(); i++) {
+      sL[i] = fps[i].sL;
+      sR[i] = fps[i].sR;
+      for (int d = 0; d < nDims; d++) nrm[i * nDims + d] = fps[i].n[d];
+      aL[i] = fps[i].aL;
+      aR[i] = fps[i].aR;
+    }
+    int *dsL, *dsR;
+    double *dn, *daL, *daR;
+    if (!upload(dsL, sL) || !upload(dsR, sR) || !upload(dn, nrm) || !upload(daL, aL) || !upload(daR, aR))
+      return false;
+    ft.n = (int)fps.size();
+    ft.slotL = dsL;
+    ft.slotR = dsR;
+    ft.nrm = dn;
+    ft.dAL = daL;
+    ft.dAR = daR;
+
+    ph.gamma = in.gamma;
+    ph.rhoBound = in.rhoBound;
+    ph.uBound = in.uBound;
+    ph.vBound = in.vBound;
+    ph.wBound = in.wBound;
+    ph.pBound = in.pBound;
+    ph.TWall = in.TWall;
+    ph.RGas = in.RGas;
+    ph.uWall = in.uWall;
+    ph.vWall = in.vWall;
+    ph.wWall = in.wWall;
+    ph.mu_inf = in.mu_inf;
+    ph.prandtl = in.prandtl;
+    ph.rt_inf = in.rt_inf;
+    ph.c_sth = in.c_sth;
+    ph.penFact = in.penFact;
+    ph.tau = in.tau;
+    ph.fixVis = in.fixVis;
+    ph.viscFluxQuirk = o.visc_flux_quirk;
+    ph.riemannType = in.riemannType;
+
+    // elements per block of the fused element kernel
+    EB = 1;
+    for (int c = 2; c <= 32; c *= 2) {
+      if (frk::elem_smem_bytes(nDims, nS, nFp, c) > 72 * 1024) break;
+      if ((long long)nS * c > 1024) break;
+      EB = c;
+    }
+    hostDt = in.dt;
+    if (cudaMemcpyAsync(dt, &hostDt, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "dt upload");
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(FR_ERR_CUDA, "setup sync");
+    return cuda_ok("setup");
+  }
+
+  // Mesh, faces, metrics and operators on the host (no device needed).
+  bool setup_host() {
+    if (opts.mu_override) in.mu_inf = opts.mu_inf;
+    nDims = in.nDims;
+    nF = in.nFields;
+    nRK = in.nRKSteps;
+    std::string e;
+    if (!fr::build_faces(mesh, in.order, in.sptsTypeQuad, faces, e)) return fail(FR_ERR_SETUP, e);
+    if (!fr::build_geometry(mesh, in.order, in.sptsTypeQuad, geo, e)) return fail(FR_ERR_SETUP, e);
+    fr::build_operators(nDims, in.order, in.sptsTypeQuad, in.vcjhSchemeQuad, op);
+    nS = op.nSpts;
+    nFp = op.nFpts;
+    E = mesh.nEles;
+    nPF = nDims == 2 ? in.order + 1 : (in.order + 1) * (in.order + 1);
+    return true;
+  }
+
+  frk::ElemArgs elem_args() {
+    frk::ElemArgs a;
+    a.E = E;
+    a.nS = nS;
+    a.nFp = nFp;
+    a.EB = EB;
+    a.U = U;
+    a.JGinv = JGinv;
+    a.detJ = detJ;
+    a.Fn = Fn;
+    for (int d = 0; d < nDims; d++) {
+      a.grad[d] = grad[d];
+      a.extFn[d] = extFn[d];
+    }
+    a.corr = corr;
+    a.ext = ext;
+    a.nRK = nRK;
+    a.dt = dt;
+    a.eleDt = in.dtType == 2 ? eleDt : nullptr;
+    a.U0 = U0;
+    a.acc = acc;
+    a.Uout = U;
+    a.gamma = in.gamma;
+    return a;
+  }
+
+  void extrapolate() {
+    frk::launch_apply_op(ext, U, Ufpts, (long long)E * nF, 1.0, 0.0, stream);
+    launches++;
+    fptsFresh = true;
+  }
+
+  // solver::calcDt (solver.cpp:447-468): the first iteration recomputes the
+  // wave speeds from U_fpts; afterwards the face kernel's (left-only) values.
+  void calc_dt_dev() {
+    if (iter == 1) {
+      frk::launch_wavesp_init(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
+      launches++;
+    }
+    launches += 3;
+    frk::launch_reset_min(dtBits, stream);
+    frk::launch_element_dt(nDims, nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA,
+                           in.CFL * fr::cfl_limit(in.order), eleDt, dtBits, stream);
+    frk::launch_store_min(dtBits, dt, timeAcc, stream);
+  }
+
+  void faces_pass() {
+    frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
+    launches++;
+  }
+  void element(const frk::ElemArgs &a) {
+    frk::launch_element_stage(nDims, a, stream);
+    launches++;
+  }
+
+  bool calc_residual(int step) {
+    if (step < 0 || step >= nRK) return fail(FR_ERR_ARG, "step out of range");
+    extrapolate();
+    faces_pass();
+    frk::ElemArgs a = elem_args();
+    a.mode = frk::MODE_RESIDUAL;
+    a.divF_out = divF[step];
+    a.F_dbg = Fdbg;
+    a.disFn_dbg = disFnDbg;
+    element(a);
+    return cuda_ok("calc_residual");
+  }
+
+  // solver::update (solver.cpp:319-363)
+  bool update_once(bool pmgSource) {
+    if (!fptsFresh) extrapolate();
+    const bool jameson = in.timeType >= 5;
+    for (int step = 0; step < nRK - 1; step++) {
+      if (step == 0 && in.dtType != 0) calc_dt_dev();
+      faces_pass();
+      frk::ElemArgs a = elem_args();
+      a.mode = jameson ? frk::MODE_JAMESON : frk::MODE_RK_STAGE;
+      a.stage = step;
+      a.rka_next = in.RKa[step + 1];
+      a.rkb = jameson ? 0.0 : in.RKb[step];
+      a.divF_out = step == 0 ? divF[0] : nullptr;
+      a.src = pmgSource ? src : nullptr;
+      a.Ufpts_out = Ufpts;
+      element(a);
+    }
+    faces_pass();
+    if (nRK == 1 && in.dtType != 0) calc_dt_dev();
+    frk::ElemArgs a = elem_args();
+    a.stage = nRK - 1;
+    a.src = pmgSource ? src : nullptr;
+    a.divF_out = nRK == 1 ? divF[0] : nullptr;
+    a.Ufpts_out = Ufpts;
+    if (jameson) {
+      a.mode = frk::MODE_JAMESON;
+      a.rka_next = in.RKa[nRK];
+    } else {
+      a.mode = frk::MODE_RK_FINAL;
+      a.rkb = in.RKb[nRK - 1];
+    }
+    element(a);
+    frk::launch_add_time(dt, timeAcc, stream);
+    launches++;
+    fptsFresh = true;
+    return cuda_ok("update");
+  }
+
+  bool update(bool pmgSource) {
+    if (!stateSet) return fail(FR_ERR_STATE, "no state set");
+    iter++;
+    return update_once(pmgSource);
+  }
+
+  bool run(int n) {
+    if (!stateSet) return fail(FR_ERR_STATE, "no state set");
+    if (n <= 0) return true;
+    // the first iteration differs (wave-speed initialisation); run it eagerly
+    while (n > 0 && (iter < 1 || !fptsFresh)) {
+      if (!update(false)) return false;
+      n--;
+    }
+    if (n <= 0) return true;
+    if (!graph) {
+      if (!stream) return fail(FR_ERR_STATE, "graph capture needs a non-default stream");
+      cudaGraph_t g;
+      long long saveIter = iter;
+      iter = 2;  // steady-state branch
+      if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(FR_ERR_CUDA, "begin capture");
+      long long before = launches;
+      update_once(false);
+      graphKernels = (int)(launches - before);
+      launches = before;
+      if (cudaStreamEndCapture(stream, &g) != cudaSuccess) return fail(FR_ERR_CUDA, "end capture");
+      iter = saveIter;
+      if (cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(FR_ERR_CUDA, "graph instantiate");
+      }
+      cudaGraphDestroy(g);
+    }
+    for (int i = 0; i < n; i++) {
+      iter++;
+      if (cudaGraphLaunch(graph, stream) != cudaSuccess) return fail(FR_ERR_CUDA, "graph launch");
+      launches += graphKernels;
+    }
+    return cuda_ok("run");
+  }
+
+  bool sync() {
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string("sync: ") + cudaGetErrorString(e));
+    return true;
+  }
+};
+
+namespace {
+
+int status_of(fr_case *c, bool ok, int code = FR_ERR_CUDA) {
+  if (ok) return FR_OK;
+  if (c->err.find("cudaMalloc") != std::string::npos) return FR_ERR_CUDA;
+  return code;
+}
+
+int create_common(const char *deck, const fr_mesh *mesh, const fr_setup_opts *opts, fr_case **out) {
+  if (!deck || !out) return FR_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<fr_case> c(new fr_case());
+  fr_setup_opts o;
+  if (opts)
+    o = *opts;
+  else
+    fr_setup_opts_default(&o);
+  std::string e;
+  if (!fr::read_deck(deck, c->in, e)) {
+    c->err = e;
+    *out = c.release();
+    return e.find("open") != std::string::npos ? FR_ERR_ARG : FR_ERR_UNSUPPORTED;
+  }
+  if (mesh) {
+    if (mesh->nDims != c->in.nDims || (mesh->nNodes != (mesh->nDims == 2 ? 4 : 8)) || mesh->nEles <= 0 ||
+        !mesh->xv || !mesh->c2v) {
+      c->err = "mesh does not match the deck (nDims / nNodes) or is empty";
+      *out = c.release();
+      return FR_ERR_ARG;
+    }
+    fr::Mesh &m = c->mesh;
+    m.nDims = mesh->nDims;
+    m.nVerts = mesh->nVerts;
+    m.xv.assign(mesh->xv, mesh->xv + (size_t)mesh->nVerts * mesh->nDims);
+    m.nEles = mesh->nEles;
+    m.nNodes = mesh->nNodes;
+    m.c2v.assign(mesh->c2v, mesh->c2v + (size_t)mesh->nEles * mesh->nNodes);
+    for (int i = 0; i < mesh->nBndFaces; i++) {
+      const int *v = &mesh->bndFaceVerts[(size_t)4 * i];
+      m.bndFaceVerts.push_back({v[0], v[1], mesh->nDims == 2 ? -1 : v[2], mesh->nDims == 2 ? -1 : v[3]});
+      m.bndFaceBc.push_back(mesh->bndFaceBc[i]);
+    }
+    for (int d = 0; d < 3; d++) m.period[d] = mesh->period[d];
+    m.periodicTol = c->in.periodicTol;
+  } else {
+    if (c->in.meshType != 1) {
+      c->err = "deck reads a mesh file: pass the mesh with fr_create_with_mesh";
+      *out = c.release();
+      return FR_ERR_UNSUPPORTED;
+    }
+    if (!fr::create_cartesian_mesh(c->in, c->mesh, e)) {
+      c->err = e;
+      *out = c.release();
+      return FR_ERR_SETUP;
+    }
+    if (o.perturb) fr::perturb_interior_vertices(c->in, c->mesh, o.seed, o.perturb_frac);
+  }
+  bool ok = c->setup(o);
+  int st = FR_OK;
+  if (!ok) {
+    st = c->err.find("mixed") != std::string::npos || c->err.find("viscous") != std::string::npos
+             ? FR_ERR_UNSUPPORTED
+             : (c->err.find("cuda") != std::string::npos ? FR_ERR_CUDA : FR_ERR_SETUP);
+  }
+  *out = c.release();
+  return st;
+}
+
+template <typename T>
+int copy_out(fr_case *c, const std::vector<T> &h, void *host, size_t *count) {
+  if (!count) return FR_ERR_ARG;
+  size_t cap = *count;
+  *count = h.size();
+  if (!host) return FR_OK;
+  if (cap < h.size()) return FR_ERR_ARG;
+  std::memcpy(host, h.data(), h.size() * sizeof(T));
+  (void)c;
+  return FR_OK;
+}
+
+int copy_dev(fr_case *c, const double *d, size_t n, void *host, size_t *count) {
+  if (!count) return FR_ERR_ARG;
+  if (!d) {
+    c->err = "array not kept (enable debug_arrays)";
+    return FR_ERR_STATE;
+  }
+  size_t cap = *count;
+  *count = n;
+  if (!host) return FR_OK;
+  if (cap < n) return FR_ERR_ARG;
+  if (!c->sync()) return FR_ERR_CUDA;
+  if (cudaMemcpy(host, d, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    c->err = "cudaMemcpy D2H failed";
+    return FR_ERR_CUDA;
+  }
+  return FR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fr_setup_opts_default(fr_setup_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = FR_PREC_FP64;
+  o->visc_flux_quirk = 1;
+}
+
+int fr_create_from_deck(const char *deck_path, const fr_setup_opts *opts, fr_case **out) {
+  return create_common(deck_path, nullptr, opts, out);
+}
+
+int fr_create_with_mesh(const char *deck_path, const fr_mesh *mesh, const fr_setup_opts *opts,
+                        fr_case **out) {
+  if (!mesh) return FR_ERR_ARG;
+  return create_common(deck_path, mesh, opts, out);
+}
+
+void fr_destroy(fr_case *c) { delete c; }
+
+const char *fr_last_error(const fr_case *c) { return c ? c->err.c_str() : "null case"; }
+
+int fr_get_info(fr_case *c, fr_info *info) {
+  if (!c || !info) return FR_ERR_ARG;
+  std::memset(info, 0, sizeof(*info));
+  info->nDims = c->nDims;
+  info->nFields = c->nF;
+  info->order = c->in.order;
+  info->nEles = c->E;
+  info->nSpts = c->nS;
+  info->nFpts = c->nFp;
+  info->nFaces = (int)c->faces.size();
+  info->nFacePts = c->ft.n;
+  info->nRKSteps = c->nRK;
+  info->precision = c->opts.precision;
+  info->dtType = c->in.dtType;
+  info->timeType = c->in.timeType;
+  info->iter = c->iter;
+  info->launches = c->launches;
+  if (c->U && !c->hostOnly) {
+    if (!c->sync()) return FR_ERR_CUDA;
+    cudaMemcpy(&info->time, c->timeAcc, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&info->dt, c->dt, sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  return FR_OK;
+}
+
+int fr_set_stream(fr_case *c, void *stream) {
+  if (!c) return FR_ERR_ARG;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  c->stream = (cudaStream_t)stream;
+  return FR_OK;
+}
+
+int fr_init_solution(fr_case *c, int kind, const double *prm, int nprm) {
+  if (!c) return FR_ERR_ARG;
+  if (!c->U) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  std::vector<double> U;
+  std::string e;
+  if (!fr::initial_condition(c->in, c->geo, c->nS, c->E, kind, prm, nprm, U, e)) {
+    c->err = e;
+    return FR_ERR_ARG;
+  }
+  return fr_set_state(c, U.data(), U.size());
+}
+
+int fr_set_state(fr_case *c, const double *U, size_t count) {
+  if (!c || !U) return FR_ERR_ARG;
+  if (!c->U) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  if (count != (size_t)c->nS * c->E * c->nF) {
+    c->err = "state size mismatch";
+    return FR_ERR_ARG;
+  }
+  if (cudaMemcpyAsync(c->U, U, count * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+    c->err = "cudaMemcpy H2D failed";
+    return FR_ERR_CUDA;
+  }
+  c->extrapolate();
+  if (c->in.dtType != 0)  // solver::initializeSolution, solver.cpp:1932-1938
+    frk::launch_wavesp_init(c->nDims, c->nFp, c->E, c->Ufpts, c->norm, c->in.gamma, c->waveSp, c->stream);
+  c->stateSet = true;
+  return c->cuda_ok("set_state") ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_get_state(fr_case *c, double *U, size_t count) {
+  if (!c || !U) return FR_ERR_ARG;
+  size_t n = (size_t)c->nS * c->E * c->nF;
+  if (count != n) {
+    c->err = "state size mismatch";
+    return FR_ERR_ARG;
+  }
+  return copy_dev(c, c->U, n, U, &count);
+}
+
+int fr_calc_residual(fr_case *c, int step) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  if (!c->stateSet) {
+    c->err = "no state set";
+    return FR_ERR_STATE;
+  }
+  return status_of(c, c->calc_residual(step), FR_ERR_ARG);
+}
+
+int fr_get_residual(fr_case *c, int step, double *divF, size_t count) {
+  if (!c || !divF || step < 0 || step >= c->nRK) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  size_t n = (size_t)c->nS * c->E * c->nF;
+  if (count != n) return FR_ERR_ARG;
+  return copy_dev(c, c->divF[step], n, divF, &count);
+}
+
+int fr_update(fr_case *c, int pmg_source) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  if (pmg_source && !c->src) {
+    c->err = "no P-multigrid source on this case";
+    return FR_ERR_STATE;
+  }
+  bool ok = c->update(pmg_source != 0);
+  return ok ? FR_OK : (c->err == "no state set" ? FR_ERR_STATE : FR_ERR_CUDA);
+}
+
+int fr_run(fr_case *c, int nsteps) {
+  if (!c || nsteps < 0) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  bool ok = c->run(nsteps);
+  return ok ? FR_OK : (c->err == "no state set" ? FR_ERR_STATE : FR_ERR_CUDA);
+}
+
+int fr_calc_dt(fr_case *c, double *dtOut) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  if (!c->stateSet) {
+    c->err = "no state set";
+    return FR_ERR_STATE;
+  }
+  if (c->in.CFL <= 0) {
+    c->err = "CFL not set";
+    return FR_ERR_ARG;
+  }
+  long long save = c->iter;
+  if (c->iter == 0) c->iter = 1;  // wave speeds from the current U_fpts
+  if (!c->fptsFresh) c->extrapolate();
+  c->calc_dt_dev();
+  c->iter = save;
+  if (!c->sync()) return FR_ERR_CUDA;
+  double d;
+  cudaMemcpy(&d, c->dt, sizeof(double), cudaMemcpyDeviceToHost);
+  c->hostDt = d;
+  if (dtOut) *dtOut = d;
+  return FR_OK;
+}
+
+int fr_set_dt(fr_case *c, double dt) {
+  if (!c || !(dt > 0)) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  c->hostDt = dt;
+  c->in.dt = dt;
+  if (cudaMemcpyAsync(c->dt, &c->hostDt, sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return FR_ERR_CUDA;
+  return c->sync() ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_residual_norm(fr_case *c, int resType, double *out, int nFields) {
+  if (!c || !out || nFields != c->nF || resType < 1 || resType > 3) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  frk::launch_residual_norm(c->nS, c->E, c->nF, c->divF[0], c->detJ, c->wSpt, resType, c->eleRes, c->stream);
+  std::vector<double> er((size_t)c->E * c->nF);
+  if (!c->sync()) return FR_ERR_CUDA;
+  cudaMemcpy(er.data(), c->eleRes, er.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  for (int k = 0; k < c->nF; k++) {
+    double r = 0;
+    for (int e = 0; e < c->E; e++) {
+      double v = er[(size_t)e * c->nF + k];
+      if (v != v) {
+        c->err = "NaN Encountered in Solution Residual!";
+        return FR_ERR_NONFINITE;
+      }
+      r = resType == 3 ? std::max(r, v) : r + v;
+    }
+    out[k] = resType == 2 ? std::sqrt(r) : r;
+  }
+  return FR_OK;
+}
+
+int fr_check_state(fr_case *c) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  cudaMemsetAsync(c->bad, 0, sizeof(unsigned), c->stream);
+  frk::launch_check_state(c->nS, c->E, c->nF, c->U, c->bad, c->stream);
+  unsigned b = 0;
+  if (!c->sync()) return FR_ERR_CUDA;
+  cudaMemcpy(&b, c->bad, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (b) {
+    c->err = "non-finite or non-positive density in the state";
+    return FR_ERR_NONFINITE;
+  }
+  return FR_OK;
+}
+
+int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
+  if (!c || !name || !count) return FR_ERR_ARG;
+  std::string n = name;
+  size_t nU = (size_t)c->nS * c->E * c->nF, nUf = (size_t)c->nFp * c->E * c->nF;
+  if (c->hostOnly && (n == "U_spts" || n == "U0" || n == "U_fpts" || n == "Fn_fpts" || n == "waveSp_fpts" ||
+                      n == "ele_dt" || n == "F_spts" || n == "disFn_fpts" || n.rfind("divF_", 0) == 0)) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  if (n == "U_spts") return copy_dev(c, c->U, nU, host, count);
+  if (n == "U0") return copy_dev(c, c->U0, nU, host, count);
+  if (n == "U_fpts") return copy_dev(c, c->Ufpts, nUf, host, count);
+  if (n == "Fn_fpts") return copy_dev(c, c->Fn, nUf, host, count);
+  if (n == "waveSp_fpts") return copy_dev(c, c->waveSp, (size_t)c->nFp * c->E, host, count);
+  if (n == "ele_dt") return copy_dev(c, c->eleDt, (size_t)c->E, host, count);
+  if (n == "F_spts") return copy_dev(c, c->Fdbg, (size_t)c->nDims * nU, host, count);
+  if (n == "disFn_fpts") return copy_dev(c, c->disFnDbg, nUf, host, count);
+  if (n.rfind("divF_", 0) == 0) {
+    int s = std::atoi(n.c_str() + 5);
+    if (s < 0 || s >= c->nRK) return FR_ERR_ARG;
+    return copy_dev(c, c->divF[s], nU, host, count);
+  }
+  if (n == "pos_spts") return copy_out(c, c->geo.pos_spts, host, count);
+  if (n == "detJac_spts") return copy_out(c, c->geo.detJac_spts, host, count);
+  if (n == "JGinv_spts") return copy_out(c, c->geo.JGinv_spts, host, count);
+  if (n == "norm_fpts") return copy_out(c, c->geo.norm_fpts, host, count);
+  if (n == "dA_fpts") return copy_out(c, c->geo.dA_fpts, host, count);
+  if (n == "xv") return copy_out(c, c->mesh.xv, host, count);
+  if (n == "opp_spts_to_fpts") return copy_out(c, c->op.ext, host, count);
+  if (n == "opp_correction") return copy_out(c, c->op.corr, host, count);
+  if (n == "opp_prolong") return copy_out(c, c->op.prolong, host, count);
+  if (n == "opp_restrict") return copy_out(c, c->op.restrict_, host, count);
+  for (int d = 0; d < c->nDims; d++) {
+    std::string sd = std::to_string(d);
+    if (n == "opp_grad_spts_" + sd) return copy_out(c, c->op.grad[d], host, count);
+    if (n == "opp_extrapolateFn_" + sd) return copy_out(c, c->op.extFn[d], host, count);
+    if (n == "opp_correctU_" + sd) return copy_out(c, c->op.corrU[d], host, count);
+  }
+  if (n.rfind("face_", 0) == 0) {
+    std::vector<int> v;
+    for (auto &f : c->faces) {
+      if (n == "face_eL") v.push_back(f.eL);
+      else if (n == "face_locL") v.push_back(f.locL);
+      else if (n == "face_eR") v.push_back(f.eR);
+      else if (n == "face_locR") v.push_back(f.locR);
+      else if (n == "face_bc") v.push_back(f.bc);
+      else if (n == "face_fptR") {
+        for (int j = 0; j < c->nPF; j++) v.push_back(f.eR >= 0 ? f.fptR[j] : -1);
+      } else
+        return FR_ERR_ARG;
+    }
+    return copy_out(c, v, host, count);
+  }
+  c->err = "unknown array " + n;
+  return FR_ERR_ARG;
+}
+
+int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes) {
+  if (!c || !name || !ptr) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  std::string n = name;
+  size_t nU = (size_t)c->nS * c->E * c->nF, nUf = (size_t)c->nFp * c->E * c->nF;
+  void *p = nullptr;
+  size_t b = 0;
+  if (n == "U_spts") {
+    p = c->U;
+    b = nU * 8;
+  } else if (n == "U_fpts") {
+    p = c->Ufpts;
+    b = nUf * 8;
+  } else if (n == "Fn_fpts") {
+    p = c->Fn;
+    b = nUf * 8;
+  } else if (n.rfind("divF_", 0) == 0) {
+    int s = std::atoi(n.c_str() + 5);
+    if (s < 0 || s >= c->nRK) return FR_ERR_ARG;
+    p = c->divF[s];
+    b = nU * 8;
+  } else {
+    return FR_ERR_ARG;
+  }
+  *ptr = p;
+  if (bytes) *bytes = b;
+  return FR_OK;
+}
+
+int fr_bench_kernel(fr_case *c, const char *kernel, int reps) {
+  if (!c || !kernel || reps < 0) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = "no device state";
+    return FR_ERR_STATE;
+  }
+  std::string k = kernel;
+  if (k == "faces") {
+    for (int i = 0; i < reps; i++) c->faces_pass();
+  } else if (k == "element_stage") {
+    frk::ElemArgs a = c->elem_args();
+    a.mode = c->in.timeType >= 5 ? frk::MODE_JAMESON : frk::MODE_RK_STAGE;
+    a.stage = c->nRK > 1 ? 1 : 0;
+    a.rka_next = c->in.RKa.size() > 2 ? c->in.RKa[2] : 0.0;
+    a.rkb = c->in.RKb.size() > 1 ? c->in.RKb[1] : 0.0;
+    a.Ufpts_out = c->Ufpts;
+    for (int i = 0; i < reps; i++) c->element(a);
+  } else {
+    c->err = "unknown kernel " + k;
+    return FR_ERR_ARG;
+  }
+  return c->cuda_ok("bench_kernel") ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_synchronize(fr_case *c) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  return c->sync() ? FR_OK : FR_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,378 @@
+// FP64 plain-form stage kernels for sm_100a.
+//
+// One RK stage is two kernels:
+//   faces   : common flux Fn at every face point, gathered from U_fpts through
+//             the face-point table (reference: solver.cpp:752-758);
+//   element : per block of EB elements, with the element's data staged in
+//             shared memory: transformed flux at the solution points
+//             (solver.cpp:707-736), flux divergence (925-954), extrapolated
+//             normal flux (956-1034), correction (1036-1058), the RK update
+//             (470-536) and the extrapolation of the new state to the flux
+//             points for the next stage's face kernel (556-572).
+// Operators are applied through their nonzero entries (Csr), which for the
+// tensor-product quad/hex operators removes the structural zeros of the
+// reference's dense cblas_dgemm without changing any sum.
+#include <cstdio>
+
+#include "stage.hpp"
+
+namespace frk {
+
+namespace {
+
+__global__ void k_apply_op(int nRows, const int *__restrict__ rp, const int *__restrict__ ci,
+                           const double *__restrict__ v, const double *__restrict__ in,
+                           double *__restrict__ out, long long N, double alpha, double beta) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (n >= N || r >= nRows) return;
+  double s = 0.0;
+  for (int j = rp[r]; j < rp[r + 1]; j++) s += v[j] * in[(long long)ci[j] * N + n];
+  double o = alpha * s;
+  if (beta != 0.0) o += beta * out[(long long)r * N + n];
+  out[(long long)r * N + n] = o;
+}
+
+template <int ND>
+__global__ void k_faces_inviscid(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
+                                 const double *__restrict__ nrm, const double *__restrict__ dAL,
+                                 const double *__restrict__ dAR, const double *__restrict__ Uf,
+                                 double *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
+  constexpr int NF = ND + 2;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int sL = slotL[i];
+  const int sR = slotR[i];
+  double UL[NF], UR[NF], nv[ND], F[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
+#pragma unroll
+  for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
+  const double gam = ph.gamma;
+  if (sR >= 0) {
+#pragma unroll
+    for (int k = 0; k < NF; k++) UR[k] = Uf[(long long)sR * NF + k];
+    if (ND == 2 && ph.riemannType == 1) {
+      roe2d<double>(UL, UR, nv, gam, F);
+    } else {
+      waveSp[sL] = rusanov<ND, double>(UL, UR, nv, gam, F);
+    }
+    const double aL = dAL[i], aR = dAR[i];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      Fn[(long long)sL * NF + k] = F[k] * aL;
+      Fn[(long long)sR * NF + k] = -F[k] * aR;
+    }
+  } else {
+    const int bc = -sR - 2;
+    boundary_state<ND, double>(bc, UL, nv, ph, UR);
+    // boundaries always use Rusanov (reference: face.cpp:174-176)
+    waveSp[sL] = rusanov<ND, double>(UL, UR, nv, gam, F);
+    const double aL = dAL[i];
+#pragma unroll
+    for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
+  }
+}
+
+__device__ __forceinline__ double csr_dot(const Csr &A, int row, const double *__restrict__ x,
+                                          int stride) {
+  double s = 0.0;
+  const int b = A.rowptr[row], e = A.rowptr[row + 1];
+  for (int j = b; j < e; j++) s += A.val[j] * x[A.col[j] * stride];
+  return s;
+}
+
+template <int ND>
+__global__ void __launch_bounds__(256) k_element_stage(ElemArgs a) {
+  constexpr int NF = ND + 2;
+  extern __shared__ double smem[];
+  const int EB = a.EB, nS = a.nS, nFp = a.nFp, E = a.E;
+  const int e0 = blockIdx.x * EB;
+  const int nValid = min(EB, E - e0);
+  const int rowS = EB * NF;  // doubles per point row of a tile
+  double *sU = smem;                      // [nS][EB][NF]
+  double *sF = sU + (size_t)nS * rowS;    // [ND][nS][EB][NF]
+  double *sQ = sF + (size_t)ND * nS * rowS;  // [nFp][EB][NF]
+  double *sD = sQ + (size_t)nFp * rowS;   // [nS][EB][NF]
+
+  // A: stage the state tile (coalesced: each point row is EB*NF contiguous)
+  for (int idx = threadIdx.x; idx < nS * rowS; idx += blockDim.x) {
+    const int s = idx / rowS, r = idx - s * rowS;
+    sU[idx] = (r < nValid * NF) ? a.U[((long long)s * E + e0) * NF + r] : 1.0;
+  }
+  __syncthreads();
+
+  // B: reference-space flux at the solution points
+  for (int it = threadIdx.x; it < nS * EB; it += blockDim.x) {
+    const int s = it / EB, el = it - s * EB;
+    const int e = e0 + el;
+    double Fp[ND][NF];
+    const double *u = &sU[(s * EB + el) * NF];
+    if (el < nValid) {
+      inviscid_flux<ND, double>(u, Fp, a.gamma);
+    } else {
+#pragma unroll
+      for (int d = 0; d < ND; d++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) Fp[d][k] = 0.0;
+    }
+#pragma unroll
+    for (int d1 = 0; d1 < ND; d1++) {
+      double J[ND];
+#pragma unroll
+      for (int d2 = 0; d2 < ND; d2++)
+        J[d2] = el < nValid ? a.JGinv[(((long long)d1 * nS + s) * E + e) * ND + d2] : 0.0;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        double f = 0.0;
+#pragma unroll
+        for (int d2 = 0; d2 < ND; d2++) f += J[d2] * Fp[d2][k];
+        sF[((d1 * nS + s) * EB + el) * NF + k] = f;
+        if (a.F_dbg && el < nValid) a.F_dbg[(((long long)d1 * nS + s) * E + e) * NF + k] = f;
+      }
+    }
+  }
+  __syncthreads();
+
+  // C: flux divergence at the solution points and (Fn - extrapolated normal
+  // flux) at the flux points
+  for (int it = threadIdx.x; it < (nS + nFp) * EB; it += blockDim.x) {
+    if (it < nS * EB) {
+      const int s = it / EB, el = it - s * EB;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        const double *x0 = &sF[el * NF + k];
+        double t = csr_dot(a.grad[0], s, x0, rowS);
+#pragma unroll
+        for (int d = 1; d < ND; d++) t = t + csr_dot(a.grad[d], s, x0 + (size_t)d * nS * rowS, rowS);
+        sD[(s * EB + el) * NF + k] = t;
+      }
+    } else {
+      const int j = it - nS * EB;
+      const int f = j / EB, el = j - f * EB;
+      const int e = e0 + el;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        const double *x0 = &sF[el * NF + k];
+        double t = csr_dot(a.extFn[0], f, x0, rowS);
+#pragma unroll
+        for (int d = 1; d < ND; d++) t = t + csr_dot(a.extFn[d], f, x0 + (size_t)d * nS * rowS, rowS);
+        double q = el < nValid ? a.Fn[((long long)f * E + e) * NF + k] - t : 0.0;
+        sQ[(f * EB + el) * NF + k] = q;
+        if (a.disFn_dbg && el < nValid) a.disFn_dbg[((long long)f * E + e) * NF + k] = q;
+      }
+    }
+  }
+  __syncthreads();
+
+  // D: correction, RK update
+  const double dtg = (a.mode != MODE_RESIDUAL && a.dt) ? *a.dt : 0.0;
+  for (int it = threadIdx.x; it < nS * EB; it += blockDim.x) {
+    const int s = it / EB, el = it - s * EB;
+    const int e = e0 + el;
+    if (el >= nValid) continue;
+    const double dJ = a.detJ[(long long)s * E + e];
+    const double dt = a.eleDt ? a.eleDt[e] : dtg;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const int li = (s * EB + el) * NF + k;
+      const long long gi = ((long long)s * E + e) * NF + k;
+      double div = csr_dot(a.corr, s, &sQ[el * NF + k], rowS) + sD[li];
+      if (a.divF_out) a.divF_out[gi] = div;
+      if (a.mode == MODE_RESIDUAL) continue;
+      if (a.src) div = div + a.src[gi];
+      const double u = sU[li];
+      double unew;
+      if (a.mode == MODE_RK_STAGE) {
+        const double u0 = a.stage == 0 ? u : a.U0[gi];
+        if (a.stage == 0) a.U0[gi] = u;
+        unew = u0 - a.rka_next * div / dJ * dt;
+        const double base = a.stage == 0 ? u0 : a.acc[gi];
+        a.acc[gi] = base - a.rkb * div / dJ * dt;
+      } else if (a.mode == MODE_RK_FINAL) {
+        const double base = a.nRK == 1 ? u : a.acc[gi];
+        unew = base - a.rkb * div / dJ * dt;
+      } else {  // MODE_JAMESON
+        const double u0 = a.stage == 0 ? u : a.U0[gi];
+        if (a.stage == 0) a.U0[gi] = u;
+        unew = u0 - a.rka_next * div / dJ * dt;
+      }
+      a.Uout[gi] = unew;
+      sU[li] = unew;
+    }
+  }
+  if (a.mode == MODE_RESIDUAL || !a.Ufpts_out) return;
+  __syncthreads();
+
+  // E: new state at the flux points
+  for (int it = threadIdx.x; it < nFp * EB; it += blockDim.x) {
+    const int f = it / EB, el = it - f * EB;
+    if (el >= nValid) continue;
+    const int e = e0 + el;
+#pragma unroll
+    for (int k = 0; k < NF; k++)
+      a.Ufpts_out[((long long)f * E + e) * NF + k] = csr_dot(a.ext, f, &sU[el * NF + k], rowS);
+  }
+}
+
+template <int ND>
+__global__ void k_wavesp_init(int nFp, int E, const double *__restrict__ Uf,
+                              const double *__restrict__ norm, double gam,
+                              double *__restrict__ waveSp) {
+  constexpr int NF = ND + 2;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nFp * E) return;
+  const double *U = &Uf[i * NF];
+  const double *n = &norm[i * ND];
+  double rho = U[0];
+  double u = U[1] / rho;
+  double v = U[2] / rho;
+  double w = 0;
+  if (ND == 3) w = U[3] / rho;
+  double rhoVSq = rho * (u * u + v * v + w * w);
+  double p = (gam - 1) * (U[ND + 1] - 0.5 * rhoVSq);
+  double vN = u * n[0] + v * n[1];
+  if (ND == 3) vN += w * n[ND - 1];
+  double csq = fmax(gam * p / rho, 0.0);
+  waveSp[i] = fabs(vN - 0.0) + sqrt(csq);
+}
+
+__global__ void k_element_dt(int nS, int nFp, int nPF, int E, const double *__restrict__ detJ,
+                             const double *__restrict__ wSpt, const double *__restrict__ wSurf,
+                             const double *__restrict__ waveSp, const double *__restrict__ dA,
+                             double cflFac, double *__restrict__ eleDt,
+                             unsigned long long *dtMinBits) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  double vol = 0;
+  for (int s = 0; s < nS; s++) vol += detJ[(long long)s * E + e] * wSpt[s];
+  double intWave = 0;
+  for (int f = 0; f < nFp; f++)
+    intWave += waveSp[(long long)f * E + e] * wSurf[f % nPF] * dA[(long long)f * E + e];
+  double dt = cflFac * 2 * vol / intWave;
+  if (eleDt) eleDt[e] = dt;
+  if (dtMinBits && dt >= 0.0 && dt == dt)
+    atomicMin(dtMinBits, (unsigned long long)__double_as_longlong(dt));
+}
+
+__global__ void k_reset_min(unsigned long long *bits) {
+  *bits = (unsigned long long)__double_as_longlong(__longlong_as_double(0x7ff0000000000000ll));
+}
+
+__global__ void k_store_min(const unsigned long long *bits, double *dt, double *time_acc) {
+  *dt = __longlong_as_double((long long)*bits);
+  (void)time_acc;
+}
+
+__global__ void k_add_time(const double *dt, double *time_acc) { *time_acc += *dt; }
+
+__global__ void k_residual_norm(int nS, int E, int nF, const double *__restrict__ divF,
+                                const double *__restrict__ detJ, const double *__restrict__ w,
+                                int resType, double *__restrict__ eleRes) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  for (int k = 0; k < nF; k++) {
+    double r = 0;
+    for (int s = 0; s < nS; s++) {
+      double d = divF[((long long)s * E + e) * nF + k];
+      if (resType == 1)
+        r += fabs(d) * w[s];
+      else if (resType == 2)
+        r += d * d / detJ[(long long)s * E + e] * w[s];
+      else
+        r = fmax(fabs(d) / detJ[(long long)s * E + e], r);
+    }
+    eleRes[(long long)e * nF + k] = r;
+  }
+}
+
+__global__ void k_check_state(long long n, int nF, const double *__restrict__ U, unsigned int *bad) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = U[i];
+  bool b = !(v == v) || isinf(v);
+  if ((i % nF) == 0 && !(v > 0.0)) b = true;
+  if (b) atomicAdd(bad, 1u);
+}
+
+}  // namespace
+
+void launch_apply_op(const Csr &A, const double *in, double *out, long long N, double alpha,
+                     double beta, cudaStream_t st) {
+  if (N <= 0 || A.nRows <= 0) return;
+  dim3 g((unsigned)((N + 255) / 256), (unsigned)A.nRows);
+  k_apply_op<<<g, 256, 0, st>>>(A.nRows, A.rowptr, A.col, A.val, in, out, N, alpha, beta);
+}
+
+void launch_faces_inviscid(int nDims, const FaceTable &ft, const double *Ufpts, double *Fn,
+                           double *waveSp, const Phys &ph, cudaStream_t st) {
+  if (ft.n <= 0) return;
+  int b = 256, g = (ft.n + b - 1) / b;
+  if (nDims == 2)
+    k_faces_inviscid<2><<<g, b, 0, st>>>(ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp, ph);
+  else
+    k_faces_inviscid<3><<<g, b, 0, st>>>(ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp, ph);
+}
+
+size_t elem_smem_bytes(int nDims, int nS, int nFp, int EB) {
+  int nF = nDims + 2;
+  return sizeof(double) * (size_t)EB * nF * ((size_t)nS * (2 + nDims) + nFp);
+}
+
+void launch_element_stage(int nDims, const ElemArgs &a, cudaStream_t st) {
+  if (a.E <= 0) return;
+  int g = (a.E + a.EB - 1) / a.EB;
+  size_t sm = elem_smem_bytes(nDims, a.nS, a.nFp, a.EB);
+  if (nDims == 2) {
+    cudaFuncSetAttribute(k_element_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_element_stage<2><<<g, 256, sm, st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_element_stage<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_element_stage<3><<<g, 256, sm, st>>>(a);
+  }
+}
+
+void launch_wavesp_init(int nDims, int nFp, int E, const double *Ufpts, const double *norm,
+                        double gamma, double *waveSp, cudaStream_t st) {
+  long long n = (long long)nFp * E;
+  if (n <= 0) return;
+  unsigned g = (unsigned)((n + 255) / 256);
+  if (nDims == 2)
+    k_wavesp_init<2><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
+  else
+    k_wavesp_init<3><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
+}
+
+void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double *detJ,
+                       const double *wSpt, const double *wSurf, const double *waveSp,
+                       const double *dA, double cflFac, double *eleDt,
+                       unsigned long long *dtMinBits, cudaStream_t st) {
+  (void)nDims;
+  if (E <= 0) return;
+  k_element_dt<<<(E + 127) / 128, 128, 0, st>>>(nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA,
+                                                 cflFac, eleDt, dtMinBits);
+}
+
+void launch_reset_min(unsigned long long *bits, cudaStream_t st) { k_reset_min<<<1, 1, 0, st>>>(bits); }
+
+void launch_store_min(const unsigned long long *bits, double *dt, double *time_acc, cudaStream_t st) {
+  k_store_min<<<1, 1, 0, st>>>(bits, dt, time_acc);
+}
+
+void launch_add_time(const double *dt, double *time_acc, cudaStream_t st) {
+  k_add_time<<<1, 1, 0, st>>>(dt, time_acc);
+}
+
+void launch_residual_norm(int nS, int E, int nF, const double *divF, const double *detJ,
+                          const double *wSpt, int resType, double *eleRes, cudaStream_t st) {
+  if (E <= 0) return;
+  k_residual_norm<<<(E + 127) / 128, 128, 0, st>>>(nS, E, nF, divF, detJ, wSpt, resType, eleRes);
+}
+
+void launch_check_state(int nS, int E, int nF, const double *U, unsigned int *bad, cudaStream_t st) {
+  long long n = (long long)nS * E * nF;
+  if (n <= 0) return;
+  k_check_state<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nF, U, bad);
+}
+
+}  // namespace frk

@@ -1,0 +1,173 @@
+/*
+ * fr_b200.h - C ABI of the B200 Flux Reconstruction residual / RK-update path.
+ *
+ * The library (flurrypp_b200/libfr_b200.so) replaces the explicit FR residual
+ * and Runge-Kutta update of FlurryPP's `solver` class with CUDA kernels for
+ * sm_100a.  One `fr_case` is one reference `solver` (one mesh, one order)
+ * together with the `input` options that drive it.  State arrays keep the
+ * reference layout [point][element][field] (last index fastest,
+ * include/matrix.hpp:52-116), so a host buffer filled for the reference's
+ * U_spts can be passed here unchanged.
+ *
+ * Conventions
+ *   - every entry point returns an int status (FR_OK == 0); none calls exit();
+ *     fr_last_error() gives the message of the last failure on a case;
+ *   - host pointers are plain C arrays of the stated size; the library copies
+ *     them to and from device memory it owns;
+ *   - one case is used by one host thread at a time; kernels run on the
+ *     case's CUDA stream (fr_set_stream), the host calls that return results
+ *     synchronise that stream.
+ */
+#ifndef FR_B200_H
+#define FR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FR_OK = 0,
+  FR_ERR_ARG = 1,         /* bad argument or size */
+  FR_ERR_SETUP = 2,       /* mesh / connectivity / metric failure (reference: FatalError) */
+  FR_ERR_CUDA = 3,        /* CUDA runtime error */
+  FR_ERR_NONFINITE = 4,   /* NaN/Inf or non-positive density in the state */
+  FR_ERR_BUDGET = 5,      /* device-memory budget exceeded (server admission) */
+  FR_ERR_TIMEOUT = 6,     /* a bounded wait ran out */
+  FR_ERR_UNSUPPORTED = 7, /* option outside the B200 path */
+  FR_ERR_STATE = 8        /* call out of order (e.g. no state set) */
+};
+
+/* Arithmetic of the path. */
+enum {
+  FR_PREC_FP64 = 0, /* plain form: everything in FP64 (the correctness oracle) */
+  FR_PREC_MIXED = 1 /* precision form: FP32 state/fluxes, split-precision operators */
+};
+
+typedef struct fr_case fr_case;
+
+/* Options of a case beyond the reference deck. */
+typedef struct fr_setup_opts {
+  int precision;               /* FR_PREC_* */
+  int perturb;                 /* 1: perturb interior vertices before setup */
+  unsigned long long seed;     /* std::mt19937_64 seed for the perturbation */
+  double perturb_frac;         /* amplitude as a fraction of the cell size */
+  int mu_override;             /* 1: use mu_inf below instead of the deck's */
+  double mu_inf;
+  int visc_flux_quirk;         /* 1 (default): reference 3-D viscous-flux formulas */
+  int debug_arrays;            /* 1: keep F_spts / disFn_fpts of residual calls */
+  int device;                  /* CUDA device ordinal */
+} fr_setup_opts;
+
+/* Mesh supplied by the caller (linear quads or hexes, reference node order).
+ * Boundary faces are listed by their vertices (2 per quad edge, 4 per hex
+ * face) with a BC code of include/global.hpp:116-132 (0 = periodic, 1 = char,
+ * 8 = slip_wall, ...).  Replaces geo::readGmsh + processConnectivity
+ * (src/geo.cpp:1021-1475, 150-219) for callers that own their mesh. */
+typedef struct fr_mesh {
+  int nDims;
+  int nVerts;
+  const double *xv;       /* [nVerts][nDims] */
+  int nEles;
+  int nNodes;             /* 4 (quad) or 8 (hex) */
+  const int *c2v;         /* [nEles][nNodes] */
+  int nBndFaces;
+  const int *bndFaceVerts; /* [nBndFaces][4] (2-D: last two entries ignored) */
+  const int *bndFaceBc;    /* [nBndFaces] */
+  double period[3];        /* periodic translation per axis (>= 1e299: none) */
+} fr_mesh;
+
+typedef struct fr_info {
+  int nDims, nFields, order, nEles, nSpts, nFpts, nFaces, nFacePts, nRKSteps;
+  int precision, dtType, timeType;
+  long long iter;
+  double time, dt;
+  long long launches; /* kernels this case has launched (graph replays counted per kernel) */
+} fr_info;
+
+/* Default fr_setup_opts (FP64, no perturbation, reference quirks on). */
+void fr_setup_opts_default(fr_setup_opts *o);
+
+/* Reads a reference input deck and sets up the case: mesh (meshType 1:
+ * Cartesian generator), connectivity, operators, metrics, device buffers.
+ * Replaces input::readInputFile (src/input.cpp:257-523) followed by
+ * solver::setup(input*, order, geo* = NULL) (src/solver.cpp:60-115). */
+int fr_create_from_deck(const char *deck_path, const fr_setup_opts *opts, fr_case **out);
+
+/* As fr_create_from_deck, with the mesh given by the caller instead of the
+ * deck's meshType (solver::setup with a prepared geo*, solver.cpp:60-75). */
+int fr_create_with_mesh(const char *deck_path, const fr_mesh *mesh, const fr_setup_opts *opts,
+                        fr_case **out);
+
+void fr_destroy(fr_case *c);
+const char *fr_last_error(const fr_case *c);
+int fr_get_info(fr_case *c, fr_info *info);
+
+/* Kernels of the case run on this stream (a cudaStream_t; NULL = default). */
+int fr_set_stream(fr_case *c, void *stream);
+
+/* Initial condition on the device.  kind 0: the deck's icType
+ * (solver::initializeSolution, src/solver.cpp:1892-1943, ele.cpp:733-832);
+ * 1: isentropic vortex (prm: eps, xc, yc, Mach); 2: Taylor-Green vortex
+ * (prm: Mach); 3: uniform boundary state. */
+int fr_init_solution(fr_case *c, int kind, const double *prm, int nprm);
+
+/* Host <-> device state, [nSpts][nEles][nFields] doubles (solver::U_spts,
+ * include/solver.hpp:94). */
+int fr_set_state(fr_case *c, const double *U, size_t count);
+int fr_get_state(fr_case *c, double *U, size_t count);
+
+/* One residual evaluation into divF_spts[step] (solver::calcResidual,
+ * include/solver.hpp:175, src/solver.cpp:366-445). */
+int fr_calc_residual(fr_case *c, int step);
+/* divF_spts[step] to the host, [nSpts][nEles][nFields]. */
+int fr_get_residual(fr_case *c, int step, double *divF, size_t count);
+
+/* One time step, all RK stages (solver::update, include/solver.hpp:172,
+ * src/solver.cpp:319-363); advances time by dt. */
+int fr_update(fr_case *c, int pmg_source);
+/* n steps; the steady-state step is captured once as a CUDA graph. */
+int fr_run(fr_case *c, int nsteps);
+
+/* CFL time step (solver::calcDt, src/solver.cpp:447-468); *dt = global dt. */
+int fr_calc_dt(fr_case *c, double *dt);
+/* Fixed dt for dtType 0 ("dt" in the deck). */
+int fr_set_dt(fr_case *c, double dt);
+
+/* Residual norm per field of divF_spts[0] as writeResidual computes it
+ * (src/output.cpp:1011-1090, ele.cpp:1922-1944); resType 1, 2 or 3. */
+int fr_residual_norm(fr_case *c, int resType, double *out, int nFields);
+
+/* Checks the device state for NaN/Inf or non-positive density
+ * (FR_ERR_NONFINITE), the fail-stop checks of writeResidual. */
+int fr_check_state(fr_case *c);
+
+/* Copies a named array to the host (tests and tools): device arrays
+ * "U_spts", "U0", "U_fpts", "Fn_fpts", "divF_<s>", "waveSp_fpts",
+ * "F_spts", "disFn_fpts" (debug_arrays), "ele_dt"; setup arrays "pos_spts",
+ * "detJac_spts", "JGinv_spts", "norm_fpts", "dA_fpts", "xv",
+ * "opp_spts_to_fpts", "opp_grad_spts_<d>", "opp_extrapolateFn_<d>",
+ * "opp_correction", "opp_correctU_<d>", "opp_prolong", "opp_restrict"
+ * (doubles); "face_eL", "face_locL", "face_eR", "face_locR", "face_bc",
+ * "face_fptR" (ints).  *count on input: capacity in elements; on output: size. */
+int fr_get_array(fr_case *c, const char *name, void *host, size_t *count);
+
+/* Device pointer of a state array ("U_spts", "U_fpts", "divF_0", ...) for
+ * callers that keep data resident (no copy).  Valid until fr_destroy. */
+int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes);
+
+/* Instrumentation: launches one kernel of the steady-state RK stage `reps`
+ * times on the case's stream ("element_stage": the fused element kernel of
+ * an intermediate stage; "faces": the face kernel).  Mutates the state; for
+ * timing only.  No reference counterpart. */
+int fr_bench_kernel(fr_case *c, const char *kernel, int reps);
+
+/* Blocks until the case's stream is idle; returns FR_ERR_CUDA on a sticky error. */
+int fr_synchronize(fr_case *c);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FR_B200_H */

@@ -1,0 +1,141 @@
+"""Parity of the CUDA path with the reference (golden fixtures) and the oracle.
+
+Every case starts the GPU from the fixture's own initial state (the state the
+reference ran from) and compares, through the C ABI:
+  - one residual evaluation: divF, U_fpts, F_spts, Fn_fpts, disFn_fpts;
+  - the state after the fixture's N time steps (reference: 1e-10 relative);
+  - element time steps for the local-CFL case.
+Residual tolerances are relative to the larger of max|divF| and max|F_spts|,
+since the residual is a difference of flux terms of that size (the oracle and
+the reference differ by up to ~2e-12 of max|divF| at Mach 0.1 for that reason).
+"""
+import numpy as np
+import pytest
+
+import flurrypp_b200 as fb
+import fr_oracle as O
+from conftest import deck_path, golden_cases, harness_ic, load_golden, perturb_opts, rel_err
+
+pytestmark = pytest.mark.gpu
+
+RESID_TOL = 1e-12   # per residual evaluation
+STEP_TOL = 1e-10    # state after N steps
+
+
+def gpu_case(meta, **kw):
+    s = fb.Solver(deck_path(meta), debug_arrays=1, **perturb_opts(meta), **kw)
+    if "--cfl-dt" in meta["harness_args"]:
+        s.set_dt(meta["dt"])
+    return s
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_residual_matches_reference(case):
+    a, meta = load_golden(case)
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    s.calc_residual(0)
+    fscale = float(np.max(np.abs(a["F_spts"])))
+    shp = a["divF_0"].shape
+    assert rel_err(s.get_residual(0), a["divF_0"], fscale) < RESID_TOL
+    assert rel_err(s.get_array("U_fpts").reshape(a["U_fpts"].shape), a["U_fpts"]) < 1e-13
+    assert rel_err(s.get_array("F_spts").reshape(a["F_spts"].shape), a["F_spts"]) < 1e-13
+    assert rel_err(s.get_array("Fn_fpts").reshape(a["Fn_fpts"].shape), a["Fn_fpts"]) < 1e-12
+    assert rel_err(s.get_array("disFn_fpts").reshape(a["disFn_fpts"].shape), a["disFn_fpts"], fscale) < RESID_TOL
+    assert shp == s.shape
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_steps_match_reference(case):
+    a, meta = load_golden(case)
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    for _ in range(meta["steps"]):
+        s.update()
+    U = s.get_state()
+    assert rel_err(U, a["U_final"]) < STEP_TOL
+    if "ele_dt" in a:
+        assert rel_err(s.get_array("ele_dt"), a["ele_dt"]) < 1e-12
+    inf = s.info()
+    assert inf.iter == meta["steps"]
+    assert abs(inf.time - a["time_dt"][0]) <= 1e-12 * max(1.0, abs(a["time_dt"][0]))
+
+
+@pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "localdt_jameson2d_p3",
+                                  "channel2d_p2", "euler_fwd2d_p1"])
+def test_graph_run_equals_update_loop(case):
+    """fr_run (CUDA-graph steady state) gives the same bits as fr_update."""
+    a, meta = load_golden(case)
+    s1, s2 = gpu_case(meta), gpu_case(meta)
+    s1.set_state(a["U_init"])
+    s2.set_state(a["U_init"])
+    for _ in range(meta["steps"]):
+        s1.update()
+    s2.run(meta["steps"])
+    assert np.array_equal(s1.get_state(), s2.get_state())
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_initial_condition_matches_reference(case):
+    a, meta = load_golden(case)
+    kind, prm = harness_ic(meta)
+    s = gpu_case(meta)
+    s.initialize_solution(kind, prm)
+    assert rel_err(s.get_state(), a["U_init"]) < 1e-14
+
+
+def test_vortex_32x32_1000_steps():
+    """2-D Euler vortex, 32x32 P3, CFL 0.5 fixed dt, 1000 RK4 steps, from the
+    product's own initial condition: the reference's final state to 1e-10."""
+    a, meta = load_golden("vortex2d_p3_32_1000")
+    s = fb.Solver(deck_path(meta))
+    s.initialize_solution(fb.IC_VORTEX, (5.0, 0.0, 0.0, 0.5))
+    s.set_dt(meta["dt"])
+    s.calc_residual(0)
+    assert rel_err(s.get_residual(0), a["divF_0"]) < RESID_TOL
+    s.run(meta["steps"])
+    assert rel_err(s.get_state(), a["U_final"]) < STEP_TOL
+
+
+def test_residual_norm_matches_oracle():
+    a, meta = load_golden("vortex2d_p3_8")
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    s.calc_residual(0)
+    p = O.params_from_deck(deck_path(meta))
+    c = O.OracleCase(a, p)
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), c.residual_norm(a["divF_0"], rt), rtol=1e-12, atol=0)
+
+
+def test_nonfinite_state_is_reported():
+    """Host-side fault injection: a poisoned state is caught, not trapped."""
+    a, meta = load_golden("vortex2d_p3_8")
+    s = gpu_case(meta)
+    U = a["U_init"].copy()
+    U[3, 5, 1] = np.nan
+    s.set_state(U)
+    with pytest.raises(fb.FrError) as ei:
+        s.check_state()
+    assert ei.value.code == fb.FR_ERR_NONFINITE
+    U[3, 5, 1] = a["U_init"][3, 5, 1]
+    U[0, 0, 0] = -1.0
+    s.set_state(U)
+    with pytest.raises(fb.FrError):
+        s.check_state()
+    s.set_state(a["U_init"])
+    s.check_state()
+
+
+def test_calc_dt_matches_reference_formula():
+    """Global CFL dt on the initial state equals the harness's --cfl-dt value."""
+    a, meta = load_golden("vortex2d_p3_8")
+    src = open(deck_path(meta)).read().replace("dtType        0", "dtType 1\nCFL 0.5")
+    import tempfile, os
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "d.deck")
+        open(p, "w").write(src)
+        s = fb.Solver(p)
+        s.set_state(a["U_init"])
+        dt = s.calc_dt()
+    assert abs(dt - meta["dt"]) <= 1e-14 * meta["dt"]
