@@ -146,7 +146,7 @@ def run_reference_arm(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
@@ -173,7 +173,8 @@ def main():
     import flurrypp_b200 as fb
 
     s = fb.Solver(DECK_GPU, device=local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     s.set_stream(stream.cuda_stream)
     s.initialize_solution(fb.IC_TGV, (0.1,))
     dt = s.calc_dt()  # CFL 0.5 in the deck, evaluated once on the initial state
@@ -190,6 +191,7 @@ def main():
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        time.sleep(0.5)  # let the sampler start before the timed region
         ev0.record(stream)
         s.run(args.steps)
         ev1.record(stream)

@@ -55,6 +55,7 @@ class SetupOpts(ctypes.Structure):
         ("visc_flux_quirk", ctypes.c_int),
         ("debug_arrays", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("generic_kernels", ctypes.c_int),
     ]
 
 
@@ -91,6 +92,7 @@ class Info(ctypes.Structure):
         ("time", ctypes.c_double),
         ("dt", ctypes.c_double),
         ("launches", ctypes.c_longlong),
+        ("tensor_kernels", ctypes.c_int),
     ]
 
 

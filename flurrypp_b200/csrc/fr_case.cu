@@ -56,6 +56,8 @@ struct fr_case {
   unsigned int *bad = nullptr;
   frk::FaceTable ft;
   frk::Csr grad[3], extFn[3], corr, ext;
+  frk::TpTables tp;
+  bool useTp = false;
   int EB = 1;
   frk::Phys ph{};
   cudaGraphExec_t graph = nullptr;
@@ -240,6 +242,8 @@ struct fr_case {
       if ((long long)nS * c > 1024) break;
       EB = c;
     }
+    useTp = build_tp() && !opts.generic_kernels;
+    if (useTp) EB = frk::tp_elems_per_block(nDims, in.order);
     hostDt = in.dt;
     if (cudaMemcpyAsync(dt, &hostDt, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "dt upload");
@@ -261,6 +265,121 @@ struct fr_case {
     nFp = op.nFpts;
     E = mesh.nEles;
     nPF = nDims == 2 ? in.order + 1 : (in.order + 1) * (in.order + 1);
+    return true;
+  }
+
+  // Tensor-product tables of the dense operators, used only if every dense
+  // entry is reproduced bitwise (reference operators: operators.cpp:112-141,
+  // 596-655, 715-824).
+  bool build_tp() {
+    if (!frk::tp_supported(nDims, in.order)) return false;
+    const int n = in.order + 1;
+    auto p1 = fr::pts1d(in.sptsTypeQuad, in.order);
+    auto fp = fr::loc_fpts(nDims, in.order, in.sptsTypeQuad);
+    auto ijk = [&](int sp, int *id) {
+      id[0] = sp % n;
+      id[1] = nDims > 1 ? (sp / n) % n : 0;
+      id[2] = nDims > 2 ? sp / (n * n) : 0;
+    };
+    auto strideOf = [&](int d) { return d == 0 ? 1 : (d == 1 ? n : n * n); };
+    std::vector<double> D((size_t)n * n);
+    for (int i = 0; i < n; i++)
+      for (int m = 0; m < n; m++) D[(size_t)i * n + m] = op.grad[0][(size_t)i * nS + m];
+    for (int d = 0; d < nDims; d++)
+      for (int sp = 0; sp < nS; sp++) {
+        int a[3];
+        ijk(sp, a);
+        int base = sp - a[d] * strideOf(d);
+        for (int c = 0; c < nS; c++) {
+          int b[3];
+          ijk(c, b);
+          bool on = true;
+          for (int q = 0; q < nDims; q++)
+            if (q != d && b[q] != a[q]) on = false;
+          double ex = on ? D[(size_t)a[d] * n + b[d]] : 0.0;
+          if (on && c != base + b[d] * strideOf(d)) return false;
+          if (op.grad[d][(size_t)sp * nS + c] != ex) return false;
+        }
+      }
+    std::vector<int> fBase(nFp), fDn(nFp), fSide(nFp);
+    std::vector<double> E1(2 * n, 0.0), EF(2 * n, 0.0);
+    bool have[2] = {false, false};
+    for (int f = 0; f < nFp; f++) {
+      int dn = -1;
+      for (int d = 0; d < nDims; d++)
+        if (op.tNorm[(size_t)f * nDims + d] != 0.0) dn = d;
+      if (dn < 0) return false;
+      int side = op.tNorm[(size_t)f * nDims + dn] > 0 ? 1 : 0;
+      int id[3] = {0, 0, 0};
+      for (int d = 0; d < nDims; d++) {
+        if (d == dn) continue;
+        int hit = -1;
+        for (int i = 0; i < n; i++)
+          if (fp[f][d] == p1[i]) hit = i;
+        if (hit < 0) return false;
+        id[d] = hit;
+      }
+      int base = id[0] + n * id[1] + n * n * id[2];
+      fBase[f] = base;
+      fDn[f] = dn;
+      fSide[f] = side;
+      if (!have[side]) {
+        for (int m = 0; m < n; m++) {
+          E1[side * n + m] = op.ext[(size_t)f * nS + base + m * strideOf(dn)];
+          EF[side * n + m] = op.extFn[dn][(size_t)f * nS + base + m * strideOf(dn)];
+        }
+        have[side] = true;
+      }
+      for (int c = 0; c < nS; c++) {
+        int b[3];
+        ijk(c, b);
+        bool on = true;
+        for (int d = 0; d < nDims; d++)
+          if (d != dn && b[d] != id[d]) on = false;
+        if (op.ext[(size_t)f * nS + c] != (on ? E1[side * n + b[dn]] : 0.0)) return false;
+        for (int d = 0; d < nDims; d++)
+          if (op.extFn[d][(size_t)f * nS + c] != (on && d == dn ? EF[side * n + b[dn]] : 0.0)) return false;
+      }
+    }
+    const int nFaces = 2 * nDims;
+    std::vector<int> cF((size_t)nS * nFaces);
+    std::vector<double> cV((size_t)nS * nFaces);
+    for (int sp = 0; sp < nS; sp++) {
+      int a[3];
+      ijk(sp, a);
+      for (int fc = 0; fc < nFaces; fc++) {
+        int hit = -1;
+        for (int j = 0; j < nPF; j++) {
+          int f = fc * nPF + j;
+          if (fBase[f] == sp - a[fDn[f]] * strideOf(fDn[f])) hit = f;
+        }
+        if (hit < 0) return false;
+        cF[(size_t)sp * nFaces + fc] = hit;
+        cV[(size_t)sp * nFaces + fc] = op.corr[(size_t)sp * nFp + hit];
+      }
+      for (int c = 0; c < nFp; c++) {
+        bool used = false;
+        for (int fc = 0; fc < nFaces; fc++)
+          if (cF[(size_t)sp * nFaces + fc] == c) used = true;
+        if (!used && op.corr[(size_t)sp * nFp + c] != 0.0) return false;
+      }
+      // ascending flux-point order of the dense row
+      for (int fc = 1; fc < nFaces; fc++)
+        if (cF[(size_t)sp * nFaces + fc] <= cF[(size_t)sp * nFaces + fc - 1]) return false;
+    }
+    double *dD, *dE1, *dEF, *dcV;
+    int *dfB, *dfD, *dfS, *dcF;
+    if (!upload(dD, D) || !upload(dE1, E1) || !upload(dEF, EF) || !upload(dfB, fBase) || !upload(dfD, fDn) ||
+        !upload(dfS, fSide) || !upload(dcF, cF) || !upload(dcV, cV))
+      return false;
+    tp.D = dD;
+    tp.E1 = dE1;
+    tp.EFn1 = dEF;
+    tp.fptBase = dfB;
+    tp.fptDn = dfD;
+    tp.fptSide = dfS;
+    tp.corrFpt = dcF;
+    tp.corrVal = dcV;
     return true;
   }
 
@@ -315,7 +434,10 @@ struct fr_case {
     launches++;
   }
   void element(const frk::ElemArgs &a) {
-    frk::launch_element_stage(nDims, a, stream);
+    if (useTp)
+      frk::launch_element_stage_tp(nDims, in.order, a, tp, stream);
+    else
+      frk::launch_element_stage(nDims, a, stream);
     launches++;
   }
 
@@ -559,6 +681,7 @@ int fr_get_info(fr_case *c, fr_info *info) {
   info->timeType = c->in.timeType;
   info->iter = c->iter;
   info->launches = c->launches;
+  info->tensor_kernels = c->useTp ? 1 : 0;
   if (c->U && !c->hostOnly) {
     if (!c->sync()) return FR_ERR_CUDA;
     cudaMemcpy(&info->time, c->timeAcc, sizeof(double), cudaMemcpyDeviceToHost);

@@ -271,6 +271,7 @@ std::vector<double> spt_weights(int nDims, int order) {
   auto w = qwts1d(order);
   int n = order + 1;
   std::vector<double> out;
+  if (nDims == 1) return w;
   if (nDims == 2) {
     out.resize(n * n);
     for (int i = 0; i < n; i++)

@@ -63,42 +63,53 @@ __device__ __forceinline__ void inviscid_flux(const R *U, R F[ND][ND + 2], R gam
   }
 }
 
+// Primitive state used by the common fluxes: velocity, pressure, energy, with
+// the operations of inviscidFlux (reference: src/flux.cpp:37-76).
+template <int ND, typename R>
+struct Prim {
+  R rho, vel[ND], E, p;
+  __device__ __forceinline__ Prim(const R *U, R gam) {
+    rho = U[0];
+#pragma unroll
+    for (int d = 0; d < ND; d++) vel[d] = U[d + 1] / rho;
+    E = U[ND + 1];
+    R q = vel[0] * vel[0] + vel[1] * vel[1];
+    if (ND == 3) q = vel[0] * vel[0] + vel[1] * vel[1] + vel[ND - 1] * vel[ND - 1];
+    p = (gam - R(1.0)) * (E - R(0.5) * rho * q);
+  }
+  // flux along dimension d, F[d][k] of inviscidFlux
+  __device__ __forceinline__ void flux(int d, R *F) const {
+    F[0] = rho * vel[d];
+#pragma unroll
+    for (int j = 0; j < ND; j++) F[1 + j] = j == d ? rho * vel[j] * vel[d] + p : rho * vel[j] * vel[d];
+    F[ND + 1] = (E + p) * vel[d];
+  }
+};
+
 // Rusanov common flux on the left normal; returns the wave speed stored for
 // the dt estimate (reference: src/face.cpp:314-374).
 template <int ND, typename R>
 __device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R gam, R *Fn) {
   constexpr int NF = ND + 2;
-  R FL[ND][NF], FR[ND][NF];
-  inviscid_flux<ND>(UL, FL, gam);
-  inviscid_flux<ND>(UR, FR, gam);
-  R rhoL = UL[0], rhoR = UR[0];
-  R uL = UL[1] / rhoL, uR = UR[1] / rhoR;
-  R vL = UL[2] / rhoL, vR = UR[2] / rhoR;
-  R pL, pR;
-  if (ND == 2) {
-    pL = (gam - R(1.0)) * (UL[3] - R(0.5) * rhoL * (uL * uL + vL * vL));
-    pR = (gam - R(1.0)) * (UR[3] - R(0.5) * rhoR * (uR * uR + vR * vR));
-  } else {
-    R wL = UL[3] / rhoL, wR = UR[3] / rhoR;
-    pL = (gam - R(1.0)) * (UL[4] - R(0.5) * rhoL * (uL * uL + vL * vL + wL * wL));
-    pR = (gam - R(1.0)) * (UR[4] - R(0.5) * rhoR * (uR * uR + vR * vR + wR * wR));
-  }
+  const Prim<ND, R> L(UL, gam), Rt(UR, gam);
   R vnL = R(0), vnR = R(0);
   R tL[NF], tR[NF];
 #pragma unroll
   for (int i = 0; i < NF; i++) tL[i] = tR[i] = R(0);
 #pragma unroll
   for (int d = 0; d < ND; d++) {
-    vnL += n[d] * UL[d + 1] / rhoL;
-    vnR += n[d] * UR[d + 1] / rhoR;
+    vnL += n[d] * UL[d + 1] / L.rho;
+    vnR += n[d] * UR[d + 1] / Rt.rho;
+    R f[NF];
+    L.flux(d, f);
 #pragma unroll
-    for (int i = 0; i < NF; i++) {
-      tL[i] += n[d] * FL[d][i];
-      tR[i] += n[d] * FR[d][i];
-    }
+    for (int i = 0; i < NF; i++) tL[i] += n[d] * f[i];
+    Rt.flux(d, f);
+#pragma unroll
+    for (int i = 0; i < NF; i++) tR[i] += n[d] * f[i];
   }
-  R csqL = fmax(gam * pL / rhoL, R(0.0));
-  R csqR = fmax(gam * pR / rhoR, R(0.0));
+  R csqL = fmax(gam * L.p / L.rho, R(0.0));
+  R csqR = fmax(gam * Rt.p / Rt.rho, R(0.0));
   R eigL = fabs(vnL) + sqrt(csqL);
   R eigR = fabs(vnR) + sqrt(csqR);
   R eig = fmax(eigL, eigR);

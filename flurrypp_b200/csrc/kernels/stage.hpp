@@ -72,6 +72,27 @@ struct ElemArgs {
 size_t elem_smem_bytes(int nDims, int nS, int nFp, int EB);
 void launch_element_stage(int nDims, const ElemArgs &a, cudaStream_t st);
 
+// Tensor-product form of the same operators (quads/hexes): the dense
+// matrices' nonzeros, verified bitwise on the host, as 1-D tables.
+//   grad_d[s][c] = D[i_d(s)][m]   for c on the line through s along d
+//   ext[f][s]    = E1[side(f)][m] for s on the line of f (normal dim dn(f))
+//   extFn_dn     = (side ? +1 : -1) * ext
+//   corr[s][f]   = corrVal[s][face] at f = corrFpt[s][face], one per face
+struct TpTables {
+  const double *D = nullptr;        // [n][n]
+  const double *E1 = nullptr;       // [2][n]   side 0: xi=-1, side 1: xi=+1
+  const double *EFn1 = nullptr;     // [2][n]   E1 times the reference normal
+  const int *fptBase = nullptr;     // [nFp] first solution point of the line
+  const int *fptDn = nullptr;       // [nFp] normal dimension
+  const int *fptSide = nullptr;     // [nFp]
+  const int *corrFpt = nullptr;     // [nS][2*nDims]
+  const double *corrVal = nullptr;  // [nS][2*nDims]
+};
+bool tp_supported(int nDims, int order);
+int tp_elems_per_block(int nDims, int order);
+void launch_element_stage_tp(int nDims, int order, const ElemArgs &a, const TpTables &t,
+                             cudaStream_t st);
+
 // Wave speed at every flux point from U_fpts (reference: ele.cpp:1076-1125).
 void launch_wavesp_init(int nDims, int nFp, int E, const double *Ufpts, const double *norm,
                         double gamma, double *waveSp, cudaStream_t st);

@@ -1,0 +1,246 @@
+// Tensor-product element kernel, FP64 (quads and hexes, orders 0..5).
+//
+// Same stage as k_element_stage (flux at the solution points, divergence,
+// extrapolated normal flux, correction, RK update, extrapolation of the new
+// state to the flux points; reference: solver.cpp:470-572, 707-736,
+// 906-1058), with compile-time sizes: one thread per (solution point,
+// element), all fields in registers, the 1-D operator tables in shared
+// memory.  Every sum is the one the dense operator would form, over its
+// nonzero terms in ascending column order.
+#include "stage.hpp"
+
+namespace frk {
+
+namespace {
+
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+template <int ND, int P>
+struct Tp {
+  static constexpr int N = P + 1;
+  static constexpr int NF = ND + 2;
+  static constexpr int NS = ipow(N, ND);
+  static constexpr int NPF = ipow(N, ND - 1);
+  static constexpr int NFP = 2 * ND * NPF;
+  static constexpr int EB = NS >= 256 ? 1 : (NS * 2 > 256 ? 1 : (NS * 4 > 256 ? 2 : (NS * 8 > 256 ? 4 : (NS * 16 > 256 ? 8 : (NS * 32 > 256 ? 16 : 32)))));
+  static constexpr int NT = NS * EB;
+  static constexpr int ROW = EB * NF;  // doubles per point row of a tile
+  static constexpr size_t SMEM = sizeof(double) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 4 * N);
+};
+
+template <int ND, int P>
+__global__ void __launch_bounds__(Tp<ND, P>::NT) k_elem_tp(ElemArgs a, TpTables t) {
+  using T = Tp<ND, P>;
+  constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  extern __shared__ double smem[];
+  double *sU = smem;                 // [NS][EB][NF]
+  double *sF = sU + NS * ROW;        // [ND][NS][EB][NF]
+  double *sQ = sF + ND * NS * ROW;   // [NFP][EB][NF]
+  double *sD = sQ + NFP * ROW;       // [N][N]
+  double *sE = sD + N * N;           // [2][N]
+  double *sEF = sE + 2 * N;          // [2][N]
+
+  const int E = a.E;
+  const int e0 = blockIdx.x * EB;
+  const int nValid = min(EB, E - e0);
+  const int tid = threadIdx.x;
+  const int s = tid / EB, el = tid - (tid / EB) * EB;
+  const int e = e0 + el;
+  const bool valid = el < nValid;
+
+  for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
+  for (int i = tid; i < 2 * N; i += NT) {
+    sE[i] = t.E1[i];
+    sEF[i] = t.EFn1[i];
+  }
+  // A: state tile, coalesced along (element, field)
+  for (int idx = tid; idx < NS * ROW; idx += NT) {
+    const int ss = idx / ROW, r = idx - ss * ROW;
+    sU[idx] = (r < nValid * NF) ? a.U[((long long)ss * E + e0) * NF + r] : 1.0;
+  }
+  double J[ND][ND];
+#pragma unroll
+  for (int d1 = 0; d1 < ND; d1++)
+#pragma unroll
+    for (int d2 = 0; d2 < ND; d2++)
+      J[d1][d2] = valid ? a.JGinv[(((long long)d1 * NS + s) * E + e) * ND + d2] : 0.0;
+  __syncthreads();
+
+  // B: reference-space flux at (s, el)
+  {
+    double Fp[ND][NF];
+    const double *u = &sU[s * ROW + el * NF];
+    if (valid) {
+      inviscid_flux<ND, double>(u, Fp, a.gamma);
+    } else {
+#pragma unroll
+      for (int d = 0; d < ND; d++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) Fp[d][k] = 0.0;
+    }
+#pragma unroll
+    for (int d1 = 0; d1 < ND; d1++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        double f = 0.0;
+#pragma unroll
+        for (int d2 = 0; d2 < ND; d2++) f += J[d1][d2] * Fp[d2][k];
+        sF[(d1 * NS + s) * ROW + el * NF + k] = f;
+        if (a.F_dbg && valid) a.F_dbg[(((long long)d1 * NS + s) * E + e) * NF + k] = f;
+      }
+  }
+  __syncthreads();
+
+  // C1: divergence at (s, el): sum over d of D-lines
+  int idx3[3];
+  idx3[0] = s % N;
+  idx3[1] = ND > 1 ? (s / N) % N : 0;
+  idx3[2] = ND > 2 ? s / (N * N) : 0;
+  double div[NF];
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
+    const int base = s - idx3[d] * stride;
+    const double *Dr = &sD[idx3[d] * N];
+    double acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const double dv = Dr[m];
+      const double *x = &sF[(d * NS + base + m * stride) * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) div[k] = d == 0 ? acc[k] : div[k] + acc[k];
+  }
+
+  // C2: Fn - extrapolated normal flux at every (fpt, el)
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    const int ee = e0 + fe;
+    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+    double acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const double ev = sEF[side * N + m];
+      const double *x = &sF[(dn * NS + base + m * stride) * ROW + fe * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+    }
+    const bool v = fe < nValid;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const double q = v ? a.Fn[((long long)f * E + ee) * NF + k] - acc[k] : 0.0;
+      sQ[f * ROW + fe * NF + k] = q;
+      if (a.disFn_dbg && v) a.disFn_dbg[((long long)f * E + ee) * NF + k] = q;
+    }
+  }
+  __syncthreads();
+
+  // D: correction and RK update at (s, el)
+  if (valid) {
+    double cq[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) cq[k] = 0.0;
+#pragma unroll
+    for (int fc = 0; fc < 2 * ND; fc++) {
+      const int fp = __ldg(&t.corrFpt[s * 2 * ND + fc]);
+      const double cv = __ldg(&t.corrVal[s * 2 * ND + fc]);
+      const double *x = &sQ[fp * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
+    }
+    const double dJ = a.detJ[(long long)s * E + e];
+    const double dt = a.eleDt ? a.eleDt[e] : (a.mode != MODE_RESIDUAL ? *a.dt : 0.0);
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const long long gi = ((long long)s * E + e) * NF + k;
+      double dv = cq[k] + div[k];
+      if (a.divF_out) a.divF_out[gi] = dv;
+      if (a.mode == MODE_RESIDUAL) continue;
+      if (a.src) dv = dv + a.src[gi];
+      const double u = sU[s * ROW + el * NF + k];
+      double unew;
+      if (a.mode == MODE_RK_STAGE) {
+        const double u0 = a.stage == 0 ? u : a.U0[gi];
+        if (a.stage == 0) a.U0[gi] = u;
+        unew = u0 - a.rka_next * dv / dJ * dt;
+        const double base = a.stage == 0 ? u0 : a.acc[gi];
+        a.acc[gi] = base - a.rkb * dv / dJ * dt;
+      } else if (a.mode == MODE_RK_FINAL) {
+        const double base = a.nRK == 1 ? u : a.acc[gi];
+        unew = base - a.rkb * dv / dJ * dt;
+      } else {
+        const double u0 = a.stage == 0 ? u : a.U0[gi];
+        if (a.stage == 0) a.U0[gi] = u;
+        unew = u0 - a.rka_next * dv / dJ * dt;
+      }
+      a.Uout[gi] = unew;
+      sU[s * ROW + el * NF + k] = unew;
+    }
+  }
+  if (a.mode == MODE_RESIDUAL || !a.Ufpts_out) return;
+  __syncthreads();
+
+  // E: new state at the flux points
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    if (fe >= nValid) continue;
+    const int ee = e0 + fe;
+    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+    double acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const double ev = sE[side * N + m];
+      const double *x = &sU[(base + m * stride) * ROW + fe * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) a.Ufpts_out[((long long)f * E + ee) * NF + k] = acc[k];
+  }
+}
+
+template <int ND, int P>
+void launch_tp(const ElemArgs &a, const TpTables &t, cudaStream_t st) {
+  using T = Tp<ND, P>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_elem_tp<ND, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    attr = true;
+  }
+  int g = (a.E + T::EB - 1) / T::EB;
+  k_elem_tp<ND, P><<<g, T::NT, T::SMEM, st>>>(a, t);
+}
+
+}  // namespace
+
+bool tp_supported(int nDims, int order) { return (nDims == 2 || nDims == 3) && order >= 0 && order <= 5; }
+
+int tp_elems_per_block(int nDims, int order) {
+#define FR_TP_EB(ND, P) \
+  if (nDims == ND && order == P) return Tp<ND, P>::EB;
+  FR_TP_EB(2, 0) FR_TP_EB(2, 1) FR_TP_EB(2, 2) FR_TP_EB(2, 3) FR_TP_EB(2, 4) FR_TP_EB(2, 5)
+  FR_TP_EB(3, 0) FR_TP_EB(3, 1) FR_TP_EB(3, 2) FR_TP_EB(3, 3) FR_TP_EB(3, 4) FR_TP_EB(3, 5)
+#undef FR_TP_EB
+  return 0;
+}
+
+void launch_element_stage_tp(int nDims, int order, const ElemArgs &a, const TpTables &t, cudaStream_t st) {
+  if (a.E <= 0) return;
+#define FR_TP_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_tp<ND, P>(a, t, st);
+  FR_TP_CASE(2, 0) FR_TP_CASE(2, 1) FR_TP_CASE(2, 2) FR_TP_CASE(2, 3) FR_TP_CASE(2, 4) FR_TP_CASE(2, 5)
+  FR_TP_CASE(3, 0) FR_TP_CASE(3, 1) FR_TP_CASE(3, 2) FR_TP_CASE(3, 3) FR_TP_CASE(3, 4) FR_TP_CASE(3, 5)
+#undef FR_TP_CASE
+}
+
+}  // namespace frk

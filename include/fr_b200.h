@@ -57,7 +57,8 @@ typedef struct fr_setup_opts {
   double mu_inf;
   int visc_flux_quirk;         /* 1 (default): reference 3-D viscous-flux formulas */
   int debug_arrays;            /* 1: keep F_spts / disFn_fpts of residual calls */
-  int device;                  /* CUDA device ordinal */
+  int device;                  /* CUDA device ordinal; -1: host-side setup only */
+  int generic_kernels;         /* 1: use the general sparse-operator element kernel */
 } fr_setup_opts;
 
 /* Mesh supplied by the caller (linear quads or hexes, reference node order).
@@ -84,6 +85,7 @@ typedef struct fr_info {
   long long iter;
   double time, dt;
   long long launches; /* kernels this case has launched (graph replays counted per kernel) */
+  int tensor_kernels; /* 1: the tensor-product element kernel is in use */
 } fr_info;
 
 /* Default fr_setup_opts (FP64, no perturbation, reference quirks on). */
