@@ -56,6 +56,7 @@ class SetupOpts(ctypes.Structure):
         ("debug_arrays", ctypes.c_int),
         ("device", ctypes.c_int),
         ("generic_kernels", ctypes.c_int),
+        ("no_tma", ctypes.c_int),
     ]
 
 

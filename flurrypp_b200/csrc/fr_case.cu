@@ -5,6 +5,8 @@
 // touch lives in device memory for the life of the case.  update() issues the
 // same sequence of steps as solver::update (solver.cpp:319-363), each stage as
 // a face kernel plus a fused element kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -58,6 +60,9 @@ struct fr_case {
   frk::Csr grad[3], extFn[3], corr, ext;
   frk::TpTables tp;
   bool useTp = false;
+  frk::TmaMaps tm;
+  bool useTma = false;
+  unsigned int *devErr = nullptr;
   int EB = 1;
   frk::Phys ph{};
   cudaGraphExec_t graph = nullptr;
@@ -244,6 +249,8 @@ struct fr_case {
     }
     useTp = build_tp() && !opts.generic_kernels;
     if (useTp) EB = frk::tp_elems_per_block(nDims, in.order);
+    if (!alloc(devErr, 1)) return false;
+    useTma = useTp && !opts.no_tma && build_tma();
     hostDt = in.dt;
     if (cudaMemcpyAsync(dt, &hostDt, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "dt upload");
@@ -383,6 +390,45 @@ struct fr_case {
     return true;
   }
 
+  // TMA descriptors for the tile copies of the TMA element kernel.  The row
+  // pitch of every tensor must be a multiple of 16 bytes: E even.
+  bool build_tma() {
+    if (E % 2 != 0 || nS > 256 || nFp > 256) return false;
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+      void *fn = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+          q != cudaDriverEntryPointSuccess || !fn)
+        return false;
+      encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const int eb = frk::tma_elems_per_block(nDims, in.order);
+    auto map2 = [&](CUtensorMap *m, void *p, cuuint64_t inner, cuuint64_t outer, cuuint32_t bi, cuuint32_t bo) {
+      cuuint64_t dims[2] = {inner, outer};
+      cuuint64_t str[1] = {inner * sizeof(double)};
+      cuuint32_t box[2] = {bi, bo};
+      cuuint32_t es[2] = {1, 1};
+      return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const cuuint64_t rowU = (cuuint64_t)E * nF;
+    bool ok = map2(&tm.U, U, rowU, nS, eb * nF, nS) && map2(&tm.U0, U0, rowU, nS, eb * nF, nS) &&
+              map2(&tm.acc, acc, rowU, nS, eb * nF, nS) && map2(&tm.Fn, Fn, rowU, nFp, eb * nF, nFp) &&
+              map2(&tm.Ufpts, Ufpts, rowU, nFp, eb * nF, nFp) && map2(&tm.det, detJ, E, nS, eb, nS);
+    if (!ok) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)E * nDims, (cuuint64_t)nS, (cuuint64_t)nDims};
+    cuuint64_t str[2] = {(cuuint64_t)E * nDims * sizeof(double), (cuuint64_t)nS * E * nDims * sizeof(double)};
+    cuuint32_t box[3] = {(cuuint32_t)(eb * nDims), (cuuint32_t)nS, (cuuint32_t)nDims};
+    cuuint32_t es[3] = {1, 1, 1};
+    if (encode(&tm.J, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, JGinv, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    return true;
+  }
+
   frk::ElemArgs elem_args() {
     frk::ElemArgs a;
     a.E = E;
@@ -405,6 +451,7 @@ struct fr_case {
     a.U0 = U0;
     a.acc = acc;
     a.Uout = U;
+    a.err = devErr;
     a.gamma = in.gamma;
     return a;
   }
@@ -434,7 +481,9 @@ struct fr_case {
     launches++;
   }
   void element(const frk::ElemArgs &a) {
-    if (useTp)
+    if (useTma)
+      frk::launch_element_stage_tma(nDims, in.order, a, tp, tm, stream);
+    else if (useTp)
       frk::launch_element_stage_tp(nDims, in.order, a, tp, stream);
     else
       frk::launch_element_stage(nDims, a, stream);
@@ -537,8 +586,18 @@ struct fr_case {
   bool sync() {
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string("sync: ") + cudaGetErrorString(e));
+    if (devErr) {
+      unsigned int w = 0;
+      if (cudaMemcpy(&w, devErr, sizeof(w), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(FR_ERR_CUDA, "status read failed");
+      if (w) {
+        timedOut = true;
+        return fail(FR_ERR_TIMEOUT, "a bounded device wait ran out (TMA tile load)");
+      }
+    }
     return true;
   }
+  bool timedOut = false;
 };
 
 namespace {
@@ -681,7 +740,7 @@ int fr_get_info(fr_case *c, fr_info *info) {
   info->timeType = c->in.timeType;
   info->iter = c->iter;
   info->launches = c->launches;
-  info->tensor_kernels = c->useTp ? 1 : 0;
+  info->tensor_kernels = c->useTma ? 2 : (c->useTp ? 1 : 0);
   if (c->U && !c->hostOnly) {
     if (!c->sync()) return FR_ERR_CUDA;
     cudaMemcpy(&info->time, c->timeAcc, sizeof(double), cudaMemcpyDeviceToHost);

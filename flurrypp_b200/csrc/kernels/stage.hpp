@@ -2,6 +2,7 @@
 // All arrays are device pointers in the reference layout
 // ([point][element][field], last index fastest).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "fr_physics.cuh"
@@ -66,6 +67,7 @@ struct ElemArgs {
   double *Ufpts_out = nullptr;     // optional: next state at flux points
   double *F_dbg = nullptr;         // optional: F_spts [nDims][nS][E][nF]
   double *disFn_dbg = nullptr;     // optional: Fn - extrapolated flux [nFp][E][nF]
+  unsigned int *err = nullptr;     // device status word (bit 0: a bounded wait ran out)
   double gamma = 1.4;
 };
 
@@ -89,6 +91,22 @@ struct TpTables {
   const double *corrVal = nullptr;  // [nS][2*nDims]
 };
 bool tp_supported(int nDims, int order);
+
+// TMA descriptors of the tiles the TMA element kernel moves (one row block of
+// points x EB elements of the reference layout per copy).
+struct TmaMaps {
+  CUtensorMap U;      // [nS][E*nF]    load + store (in place)
+  CUtensorMap U0;     // [nS][E*nF]
+  CUtensorMap acc;    // [nS][E*nF]
+  CUtensorMap Fn;     // [nFp][E*nF]
+  CUtensorMap Ufpts;  // [nFp][E*nF]   store
+  CUtensorMap J;      // [nDims][nS][E*nDims]
+  CUtensorMap det;    // [nS][E]
+};
+int tma_elems_per_block(int nDims, int order);
+size_t tma_smem_bytes(int nDims, int order);
+void launch_element_stage_tma(int nDims, int order, const ElemArgs &a, const TpTables &t,
+                              const TmaMaps &m, cudaStream_t st);
 int tp_elems_per_block(int nDims, int order);
 void launch_element_stage_tp(int nDims, int order, const ElemArgs &a, const TpTables &t,
                              cudaStream_t st);

@@ -59,6 +59,7 @@ typedef struct fr_setup_opts {
   int debug_arrays;            /* 1: keep F_spts / disFn_fpts of residual calls */
   int device;                  /* CUDA device ordinal; -1: host-side setup only */
   int generic_kernels;         /* 1: use the general sparse-operator element kernel */
+  int no_tma;                  /* 1: tensor-product element kernel without TMA tiles */
 } fr_setup_opts;
 
 /* Mesh supplied by the caller (linear quads or hexes, reference node order).
@@ -85,7 +86,7 @@ typedef struct fr_info {
   long long iter;
   double time, dt;
   long long launches; /* kernels this case has launched (graph replays counted per kernel) */
-  int tensor_kernels; /* 1: the tensor-product element kernel is in use */
+  int tensor_kernels; /* 0 general, 1 tensor-product, 2 tensor-product with TMA tiles */
 } fr_info;
 
 /* Default fr_setup_opts (FP64, no perturbation, reference quirks on). */
