@@ -41,7 +41,7 @@ struct Tm {
   static constexpr int O_F = O_DET + al(NS * EB);
   static constexpr int O_TAB = O_F + al(ND * NS * ROW);
   static constexpr int O_BAR = O_TAB + al(N * N + 4 * N);
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(O_BAR + 2) + 128;
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(O_BAR + 4) + 128;
 };
 
 template <int ND, int P>
@@ -76,32 +76,39 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
   const bool needAcc = (a.mode == MODE_RK_STAGE && a.stage > 0) || (a.mode == MODE_RK_FINAL && a.nRK > 1);
   const bool needDet = a.mode != MODE_RESIDUAL;
 
+  // two transaction barriers: bar[0] for what the flux needs (U, JGinv),
+  // bar[1] for what the correction and update need (Fn, U0, acc, detJ), so
+  // the second batch lands while the flux and divergence are computed
   if (tid == 0) {
-    mbar_init(bar, 1);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     fence_mbar_init();
   }
   __syncthreads();
   if (tid == 0) {
-    uint32_t bytes = sizeof(double) * (NS * ROW + NFP * ROW + ND * NS * EB * ND);
+    mbar_arrive_expect_tx(&bar[0], sizeof(double) * (NS * ROW + ND * NS * EB * ND));
+    tma_load_2d(sU, &mp.U, e0 * NF, 0, &bar[0]);
+    tma_load_3d(sJ, &mp.J, e0 * ND, 0, 0, &bar[0]);
+    uint32_t bytes = sizeof(double) * NFP * ROW;
     if (needU0) bytes += sizeof(double) * NS * ROW;
     if (needAcc) bytes += sizeof(double) * NS * ROW;
     if (needDet) bytes += sizeof(double) * NS * EB;
-    mbar_arrive_expect_tx(bar, bytes);
-    tma_load_2d(sU, &mp.U, e0 * NF, 0, bar);
-    tma_load_2d(sFn, &mp.Fn, e0 * NF, 0, bar);
-    tma_load_3d(sJ, &mp.J, e0 * ND, 0, 0, bar);
-    if (needU0) tma_load_2d(sU0, &mp.U0, e0 * NF, 0, bar);
-    if (needAcc) tma_load_2d(sAcc, &mp.acc, e0 * NF, 0, bar);
-    if (needDet) tma_load_2d(sDet, &mp.det, e0, 0, bar);
+    mbar_arrive_expect_tx(&bar[1], bytes);
+    tma_load_2d(sFn, &mp.Fn, e0 * NF, 0, &bar[1]);
+    if (needU0) tma_load_2d(sU0, &mp.U0, e0 * NF, 0, &bar[1]);
+    if (needAcc) tma_load_2d(sAcc, &mp.acc, e0 * NF, 0, &bar[1]);
+    if (needDet) tma_load_2d(sDet, &mp.det, e0, 0, &bar[1]);
   }
   for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
   for (int i = tid; i < 2 * N; i += NT) {
     sE[i] = t.E1[i];
     sEF[i] = t.EFn1[i];
   }
-  if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
+  if (!mbar_wait_bounded(&bar[0], 0, 1u << 22)) {
+    // give up: flag it, let the copies in flight land (bounded), leave
     if (a.err) atomicOr(a.err, 1);
-    mbar_wait_bounded(bar, 0, 1u << 22);
+    mbar_wait_bounded(&bar[0], 0, 1u << 22);
+    mbar_wait_bounded(&bar[1], 0, 1u << 22);
     return;
   }
   __syncthreads();  // tables
@@ -162,6 +169,13 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
     }
 #pragma unroll
     for (int k = 0; k < NF; k++) div[k] = d == 0 ? acc[k] : div[k] + acc[k];
+  }
+
+  if (!mbar_wait_bounded(&bar[1], 0, 1u << 22)) {
+    if (a.err) atomicOr(a.err, 1);
+    mbar_wait_bounded(&bar[1], 0, 1u << 22);
+    if (tid == 0) tma_wait_read_all();
+    return;
   }
 
   // C2: Fn - extrapolated normal flux, in place in the Fn tile
