@@ -40,7 +40,9 @@ struct Tm {
   static constexpr int O_DET = O_J + al(ND * NS * EB * ND);
   static constexpr int O_F = O_DET + al(NS * EB);
   static constexpr int O_TAB = O_F + al(ND * NS * ROW);
-  static constexpr int O_BAR = O_TAB + al(N * N + 4 * N);
+  static constexpr int O_CV = O_TAB + al(N * N + 4 * N);       // corrVal [NS][2ND] doubles
+  static constexpr int O_IDX = O_CV + al(NS * 2 * ND);          // ints: fpt line [NFP], corrFpt [NS][2ND]
+  static constexpr int O_BAR = O_IDX + al((NFP + NS * 2 * ND + 1) / 2);
   static constexpr size_t SMEM = sizeof(double) * (size_t)(O_BAR + 4) + 128;
 };
 
@@ -62,6 +64,9 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
   double *sD = smem + T::O_TAB;
   double *sE = sD + N * N;
   double *sEF = sE + 2 * N;
+  double *sCV = smem + T::O_CV;
+  int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);  // base | dn << 16 | side << 20
+  int *sCF = sLine + NFP;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::O_BAR);
 
   const int E = a.E;
@@ -103,6 +108,11 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
   for (int i = tid; i < 2 * N; i += NT) {
     sE[i] = t.E1[i];
     sEF[i] = t.EFn1[i];
+  }
+  for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
+  for (int i = tid; i < NS * 2 * ND; i += NT) {
+    sCF[i] = t.corrFpt[i];
+    sCV[i] = t.corrVal[i];
   }
   if (!mbar_wait_bounded(&bar[0], 0, 1u << 22)) {
     // give up: flag it, let the copies in flight land (bounded), leave
@@ -181,7 +191,8 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
   // C2: Fn - extrapolated normal flux, in place in the Fn tile
   for (int it = tid; it < NFP * EB; it += NT) {
     const int f = it / EB, fe = it - (it / EB) * EB;
-    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int ln = sLine[f];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
     double acc[NF];
 #pragma unroll
@@ -210,13 +221,14 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
     for (int k = 0; k < NF; k++) cq[k] = 0.0;
 #pragma unroll
     for (int fc = 0; fc < 2 * ND; fc++) {
-      const int fp = __ldg(&t.corrFpt[s * 2 * ND + fc]);
-      const double cv = __ldg(&t.corrVal[s * 2 * ND + fc]);
+      const int fp = sCF[s * 2 * ND + fc];
+      const double cv = sCV[s * 2 * ND + fc];
       const double *x = &sFn[fp * ROW + el * NF];
 #pragma unroll
       for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
     }
-    const double dJ = needDet ? sDet[s * EB + el] : 1.0;
+    // one reciprocal per point instead of a division per update term
+    const double rdJ = needDet ? 1.0 / sDet[s * EB + el] : 1.0;
     const double dt = a.mode == MODE_RESIDUAL ? 0.0 : (a.eleDt ? (valid ? a.eleDt[e] : 0.0) : *a.dt);
 #pragma unroll
     for (int k = 0; k < NF; k++) {
@@ -230,15 +242,15 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
       double unew;
       if (a.mode == MODE_RK_STAGE) {
         const double u0 = a.stage == 0 ? u : sU0[li];
-        unew = u0 - a.rka_next * dv / dJ * dt;
+        unew = u0 - a.rka_next * dv * rdJ * dt;
         const double base = a.stage == 0 ? u0 : sAcc[li];
-        sAcc[li] = base - a.rkb * dv / dJ * dt;
+        sAcc[li] = base - a.rkb * dv * rdJ * dt;
       } else if (a.mode == MODE_RK_FINAL) {
         const double base = a.nRK == 1 ? u : sAcc[li];
-        unew = base - a.rkb * dv / dJ * dt;
+        unew = base - a.rkb * dv * rdJ * dt;
       } else {
         const double u0 = a.stage == 0 ? u : sU0[li];
-        unew = u0 - a.rka_next * dv / dJ * dt;
+        unew = u0 - a.rka_next * dv * rdJ * dt;
       }
       sU[li] = unew;
     }
@@ -259,7 +271,8 @@ __global__ void __launch_bounds__(Tm<ND, P>::NT) k_elem_tma(ElemArgs a, TpTables
   // E: new state at the flux points, into the Fn tile
   for (int it = tid; it < NFP * EB; it += NT) {
     const int f = it / EB, fe = it - (it / EB) * EB;
-    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int ln = sLine[f];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
     double acc[NF];
 #pragma unroll
