@@ -198,7 +198,13 @@ struct fr_case {
         }
         fps.push_back(p);
       }
-    std::sort(fps.begin(), fps.end(), [](const FP &a, const FP &b) { return a.sL < b.sL; });
+    std::sort(fps.begin(), fps.end(), [](const FP &a, const FP &b) {
+      const bool ia = a.sR >= 0, ib = b.sR >= 0;
+      if (ia != ib) return ia;  // interior points first
+      return a.sL < b.sL;
+    });
+    int nInt = 0;
+    for (auto &p : fps) nInt += p.sR >= 0 ? 1 : 0;
     std::vector<int> sL(fps.size()), sR(fps.size());
     std::vector<double> nrm(fps.size() * nDims), aL(fps.size()), aR(fps.size());
     for (size_t i = 0; i < fps.size(); i++) {
@@ -213,6 +219,7 @@ struct fr_case {
     if (!upload(dsL, sL) || !upload(dsR, sR) || !upload(dn, nrm) || !upload(daL, aL) || !upload(daR, aR))
       return false;
     ft.n = (int)fps.size();
+    ft.nInterior = nInt;
     ft.slotL = dsL;
     ft.slotR = dsR;
     ft.nrm = dn;
@@ -478,7 +485,7 @@ struct fr_case {
 
   void faces_pass() {
     frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
-    launches++;
+    launches += (ft.nInterior > 0 ? 1 : 0) + (ft.n > ft.nInterior ? 1 : 0);
   }
   void element(const frk::ElemArgs &a) {
     if (useTma)

@@ -40,8 +40,9 @@ template <int ND, typename R>
 __device__ __forceinline__ void inviscid_flux(const R *U, R F[ND][ND + 2], R gam) {
   if (ND == 2) {
     R rho = U[0];
-    R u = U[1] / rho;
-    R v = U[2] / rho;
+    R ri = R(1.0) / rho;
+    R u = U[1] * ri;
+    R v = U[2] * ri;
     R E = U[3];
     R p = (gam - R(1.0)) * (E - R(0.5) * rho * (u * u + v * v));
     F[0][0] = rho * u;          F[1][0] = rho * v;
@@ -50,9 +51,10 @@ __device__ __forceinline__ void inviscid_flux(const R *U, R F[ND][ND + 2], R gam
     F[0][3] = (E + p) * u;      F[1][3] = (E + p) * v;
   } else {
     R rho = U[0];
-    R u = U[1] / rho;
-    R v = U[2] / rho;
-    R w = U[3] / rho;
+    R ri = R(1.0) / rho;
+    R u = U[1] * ri;
+    R v = U[2] * ri;
+    R w = U[3] * ri;
     R E = U[4];
     R p = (gam - R(1.0)) * (E - R(0.5) * rho * (u * u + v * v + w * w));
     F[0][0] = rho * u;          F[1][0] = rho * v;          F[ND - 1][0] = rho * w;
@@ -68,10 +70,12 @@ __device__ __forceinline__ void inviscid_flux(const R *U, R F[ND][ND + 2], R gam
 template <int ND, typename R>
 struct Prim {
   R rho, vel[ND], E, p;
+  R rinv;
   __device__ __forceinline__ Prim(const R *U, R gam) {
     rho = U[0];
+    rinv = R(1.0) / rho;  // one reciprocal per state instead of a division per term
 #pragma unroll
-    for (int d = 0; d < ND; d++) vel[d] = U[d + 1] / rho;
+    for (int d = 0; d < ND; d++) vel[d] = U[d + 1] * rinv;
     E = U[ND + 1];
     R q = vel[0] * vel[0] + vel[1] * vel[1];
     if (ND == 3) q = vel[0] * vel[0] + vel[1] * vel[1] + vel[ND - 1] * vel[ND - 1];
@@ -98,8 +102,8 @@ __device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R gam
   for (int i = 0; i < NF; i++) tL[i] = tR[i] = R(0);
 #pragma unroll
   for (int d = 0; d < ND; d++) {
-    vnL += n[d] * UL[d + 1] / L.rho;
-    vnR += n[d] * UR[d + 1] / Rt.rho;
+    vnL += n[d] * L.vel[d];
+    vnR += n[d] * Rt.vel[d];
     R f[NF];
     L.flux(d, f);
 #pragma unroll
@@ -108,8 +112,8 @@ __device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R gam
 #pragma unroll
     for (int i = 0; i < NF; i++) tR[i] += n[d] * f[i];
   }
-  R csqL = fmax(gam * L.p / L.rho, R(0.0));
-  R csqR = fmax(gam * Rt.p / Rt.rho, R(0.0));
+  R csqL = fmax(gam * L.p * L.rinv, R(0.0));
+  R csqR = fmax(gam * Rt.p * Rt.rinv, R(0.0));
   R eigL = fabs(vnL) + sqrt(csqL);
   R eigR = fabs(vnR) + sqrt(csqR);
   R eig = fmax(eigL, eigR);

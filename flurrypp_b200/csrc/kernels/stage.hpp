@@ -27,6 +27,7 @@ void launch_apply_op(const Csr &A, const double *in, double *out, long long N, d
 // Face-point table, one entry per flux point of each face, sorted by left slot.
 struct FaceTable {
   int n = 0;
+  int nInterior = 0;            // interior points first, then boundary points
   const int *slotL = nullptr;   // fpt*E + e of the left side
   const int *slotR = nullptr;   // fpt*E + e of the right side, or -(bc+2) on a boundary
   const double *nrm = nullptr;  // [n][nDims] left unit normal
@@ -36,6 +37,8 @@ struct FaceTable {
 
 // Common inviscid flux on every face point: Fn_fpts at both sides and the
 // left-side wave speed (reference: solver.cpp:752-758, face.cpp:163-208).
+// Interior and boundary points run as two kernels (no BC code in the
+// interior one).
 void launch_faces_inviscid(int nDims, const FaceTable &ft, const double *Ufpts, double *Fn,
                            double *waveSp, const Phys &ph, cudaStream_t st);
 

@@ -33,11 +33,16 @@ __global__ void k_apply_op(int nRows, const int *__restrict__ rp, const int *__r
   out[(long long)r * N + n] = o;
 }
 
+// Interior face points: Rusanov (or 2-D Roe) on the left normal, written to
+// both sides (reference: face.cpp:163-208, intFace.cpp:147-154).
 template <int ND>
-__global__ void k_faces_inviscid(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
-                                 const double *__restrict__ nrm, const double *__restrict__ dAL,
-                                 const double *__restrict__ dAR, const double *__restrict__ Uf,
-                                 double *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
+__global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__restrict__ slotL,
+                                                        const int *__restrict__ slotR,
+                                                        const double *__restrict__ nrm,
+                                                        const double *__restrict__ dAL,
+                                                        const double *__restrict__ dAR,
+                                                        const double *__restrict__ Uf, double *__restrict__ Fn,
+                                                        double *__restrict__ waveSp, double gam, int roe) {
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -47,31 +52,44 @@ __global__ void k_faces_inviscid(int n, const int *__restrict__ slotL, const int
 #pragma unroll
   for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
 #pragma unroll
+  for (int k = 0; k < NF; k++) UR[k] = Uf[(long long)sR * NF + k];
+#pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
-  const double gam = ph.gamma;
-  if (sR >= 0) {
-#pragma unroll
-    for (int k = 0; k < NF; k++) UR[k] = Uf[(long long)sR * NF + k];
-    if (ND == 2 && ph.riemannType == 1) {
-      roe2d<double>(UL, UR, nv, gam, F);
-    } else {
-      waveSp[sL] = rusanov<ND, double>(UL, UR, nv, gam, F);
-    }
-    const double aL = dAL[i], aR = dAR[i];
-#pragma unroll
-    for (int k = 0; k < NF; k++) {
-      Fn[(long long)sL * NF + k] = F[k] * aL;
-      Fn[(long long)sR * NF + k] = -F[k] * aR;
-    }
+  if (ND == 2 && roe) {
+    roe2d<double>(UL, UR, nv, gam, F);
   } else {
-    const int bc = -sR - 2;
-    boundary_state<ND, double>(bc, UL, nv, ph, UR);
-    // boundaries always use Rusanov (reference: face.cpp:174-176)
     waveSp[sL] = rusanov<ND, double>(UL, UR, nv, gam, F);
-    const double aL = dAL[i];
-#pragma unroll
-    for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
   }
+  const double aL = dAL[i], aR = dAR[i];
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    Fn[(long long)sL * NF + k] = F[k] * aL;
+    Fn[(long long)sR * NF + k] = -F[k] * aR;
+  }
+}
+
+// Boundary face points: ghost state from the BC, then Rusanov (boundaries
+// always use Rusanov, face.cpp:174-176; ghost states boundFace.cpp:65-314).
+template <int ND>
+__global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
+                                 const double *__restrict__ nrm, const double *__restrict__ dAL,
+                                 const double *__restrict__ Uf, double *__restrict__ Fn,
+                                 double *__restrict__ waveSp, Phys ph) {
+  constexpr int NF = ND + 2;
+  int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int sL = slotL[i];
+  const int bc = -slotR[i] - 2;
+  double UL[NF], UR[NF], nv[ND], F[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
+#pragma unroll
+  for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
+  boundary_state<ND, double>(bc, UL, nv, ph, UR);
+  waveSp[sL] = rusanov<ND, double>(UL, UR, nv, ph.gamma, F);
+  const double aL = dAL[i];
+#pragma unroll
+  for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
 }
 
 __device__ __forceinline__ double csr_dot(const Csr &A, int row, const double *__restrict__ x,
@@ -306,12 +324,24 @@ void launch_apply_op(const Csr &A, const double *in, double *out, long long N, d
 
 void launch_faces_inviscid(int nDims, const FaceTable &ft, const double *Ufpts, double *Fn,
                            double *waveSp, const Phys &ph, cudaStream_t st) {
-  if (ft.n <= 0) return;
-  int b = 256, g = (ft.n + b - 1) / b;
-  if (nDims == 2)
-    k_faces_inviscid<2><<<g, b, 0, st>>>(ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp, ph);
-  else
-    k_faces_inviscid<3><<<g, b, 0, st>>>(ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp, ph);
+  const int b = 256;
+  const int nI = ft.nInterior, nB = ft.n - ft.nInterior;
+  if (nI > 0) {
+    const int g = (nI + b - 1) / b;
+    if (nDims == 2)
+      k_faces_interior<2><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
+                                           ph.gamma, ph.riemannType == 1);
+    else
+      k_faces_interior<3><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
+                                           ph.gamma, 0);
+  }
+  if (nB > 0) {
+    const int g = (nB + b - 1) / b;
+    if (nDims == 2)
+      k_faces_boundary<2><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
+    else
+      k_faces_boundary<3><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
+  }
 }
 
 size_t elem_smem_bytes(int nDims, int nS, int nFp, int EB) {
