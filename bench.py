@@ -33,6 +33,18 @@ METRIC = "DOF·RK-stage/s"
 WORKLOAD = "3D Euler Taylor-Green vortex, 32^3 hexes, P=3, RK4, Rusanov, FP64 plain form"
 
 
+def profiled_traffic(kernel_tag: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "fp64_stage_tgv32_p3.md")
+    try:
+        for line in open(p):
+            if line.startswith(kernel_tag + ":"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def measured_peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -264,7 +276,9 @@ def main():
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "traffic": None, "kernel": "k_element_stage<3>",
+                         "traffic": profiled_traffic("traffic_bytes_per_launch"),
+                         "traffic_source": "profiles/fp64_stage_tgv32_p3.md (ncu, one launch)",
+                         "kernel": "k_elem_tma<3, 3>" if inf.tensor_kernels == 2 else "k_elem_tp<3, 3>",
                          "kernel_ms": kt["element_stage"], "algorithmic_bytes": elem_bytes,
                          "peak_source": peak_kind},
             "kernels_ms": {"element_stage": kt["element_stage"], "faces": kt["faces"],

@@ -1,0 +1,39 @@
+// Minimal FlurryPP-style driver on the B200 path (reference: src/flurry.cpp:71-188):
+// read a deck, set up, apply the deck's initial condition, take N steps of
+// update(), printing the residual norm every `freq` steps and at the end.
+//
+//   flurry_b200 DECK NSTEPS [FREQ]
+#include <cstdio>
+#include <cstdlib>
+
+#include "../../include/fr_solver.hpp"
+
+int main(int argc, char **argv) {
+  if (argc < 3) {
+    std::fprintf(stderr, "usage: %s DECK NSTEPS [FREQ]\n", argv[0]);
+    return 2;
+  }
+  const int nsteps = std::atoi(argv[2]);
+  const int freq = argc > 3 ? std::atoi(argv[3]) : 10;
+  try {
+    fr::b200::Solver S;
+    S.setup(argv[1]);
+    S.initializeSolution();
+    const fr_info &inf = S.info();
+    std::printf("case: nDims %d order %d nEles %d nSpts %d nFields %d\n", inf.nDims, inf.order, inf.nEles,
+                inf.nSpts, inf.nFields);
+    for (int iter = 1; iter <= nsteps; iter++) {
+      S.update();
+      if (iter % freq == 0 || iter == nsteps) {
+        auto r = S.residualNorm(2);
+        std::printf("iter %6d  time %.10e  res", iter, S.info().time);
+        for (double v : r) std::printf(" %.10e", v);
+        std::printf("\n");
+      }
+    }
+  } catch (const fr::b200::Error &e) {
+    std::fprintf(stderr, "fr_b200 error %d: %s\n", e.code, e.what());
+    return 1;
+  }
+  return 0;
+}

@@ -161,3 +161,23 @@ def test_element_kernel_variants_agree(case, variant):
     for _ in range(meta["steps"]):
         s.update()
     assert rel_err(s.get_state(), a["U_final"]) < STEP_TOL
+
+
+def test_cpp_driver_matches_python_binding():
+    """The C++ solver adapter (include/fr_solver.hpp) driven like the
+    reference's main loop gives the same residual history as the binding."""
+    import os
+    import subprocess
+    from conftest import ROOT, DECKS
+    exe = os.path.join(ROOT, "flurrypp_b200", "examples", "flurry_b200")
+    deck = os.path.join(DECKS, "ic1_2d_p3.deck")
+    out = subprocess.run([exe, deck, "10", "5"], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    last = [l for l in out.stdout.splitlines() if l.startswith("iter")][-1].split()
+    res_cpp = np.array([float(x) for x in last[5:]])
+    s = fb.Solver(deck)
+    s.initialize_solution(fb.IC_DECK)
+    for _ in range(10):
+        s.update()
+    res_py = s.residual_norm(2)
+    assert np.allclose(res_cpp, res_py, rtol=1e-9, atol=0)
