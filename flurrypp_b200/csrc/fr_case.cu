@@ -54,6 +54,7 @@ struct fr_case {
   double *wSpt = nullptr, *wSurf = nullptr, *eleDt = nullptr, *dt = nullptr, *timeAcc = nullptr;
   double *eleRes = nullptr, *src = nullptr;
   double *Fdbg = nullptr, *disFnDbg = nullptr;
+  double *dUc = nullptr, *dUs = nullptr, *dUf = nullptr;  // viscous: LDG jumps, gradients
   unsigned long long *dtBits = nullptr;
   unsigned int *bad = nullptr;
   frk::FaceTable ft;
@@ -150,7 +151,6 @@ struct fr_case {
     ownedStream = stream;
     if (o.precision != FR_PREC_FP64)
       return fail(FR_ERR_UNSUPPORTED, "mixed precision is served by the batch API");
-    if (in.viscous) return fail(FR_ERR_UNSUPPORTED, "viscous path not built into this case type");
     if (!setup_host()) return false;
 
     size_t nU = (size_t)nS * E * nF, nUf = (size_t)nFp * E * nF;
@@ -256,8 +256,12 @@ struct fr_case {
     }
     useTp = build_tp() && !opts.generic_kernels;
     if (useTp) EB = frk::tp_elems_per_block(nDims, in.order);
+    if (in.viscous) {
+      if (!useTp) return fail(FR_ERR_UNSUPPORTED, "viscous stages need the tensor-product operators");
+      if (!alloc(dUc, nUf) || !alloc(dUs, (size_t)nDims * nU) || !alloc(dUf, (size_t)nDims * nUf)) return false;
+    }
     if (!alloc(devErr, 1)) return false;
-    useTma = useTp && !opts.no_tma && build_tma();
+    useTma = useTp && !in.viscous && !opts.no_tma && build_tma();
     hostDt = in.dt;
     if (cudaMemcpyAsync(dt, &hostDt, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "dt upload");
@@ -460,6 +464,11 @@ struct fr_case {
     a.Uout = U;
     a.err = devErr;
     a.gamma = in.gamma;
+    a.ph = ph;
+    if (in.viscous) {
+      a.dUs = dUs;
+      a.dUsStride = (long long)nS * E * nF;
+    }
     return a;
   }
 
@@ -483,12 +492,34 @@ struct fr_case {
     frk::launch_store_min(dtBits, dt, timeAcc, stream);
   }
 
+  // Everything of a stage before the element kernel: the common flux Fn (and,
+  // viscous, the LDG jumps and the corrected gradients it needs).
   void faces_pass() {
-    frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
-    launches += (ft.nInterior > 0 ? 1 : 0) + (ft.n > ft.nInterior ? 1 : 0);
+    const int nk = (ft.nInterior > 0 ? 1 : 0) + (ft.n > ft.nInterior ? 1 : 0);
+    if (!in.viscous) {
+      frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
+      launches += nk;
+      return;
+    }
+    frk::launch_faces_ldg(nDims, ft, Ufpts, dUc, ph, stream);
+    frk::GradArgs g;
+    g.E = E;
+    g.U = U;
+    g.dUc = dUc;
+    g.JGinv = JGinv;
+    g.detJ = detJ;
+    g.dUs = dUs;
+    g.dUf = dUf;
+    g.sStride = (long long)nS * E * nF;
+    g.fStride = (long long)nFp * E * nF;
+    frk::launch_elem_grad(nDims, in.order, g, tp, stream);
+    frk::launch_faces_visc(nDims, ft, Ufpts, dUf, g.fStride, Fn, waveSp, ph, stream);
+    launches += 2 * nk + 1;
   }
   void element(const frk::ElemArgs &a) {
-    if (useTma)
+    if (in.viscous)
+      frk::launch_element_stage_tp_visc(nDims, in.order, a, tp, stream);
+    else if (useTma)
       frk::launch_element_stage_tma(nDims, in.order, a, tp, tm, stream);
     else if (useTp)
       frk::launch_element_stage_tp(nDims, in.order, a, tp, stream);
@@ -667,7 +698,8 @@ int create_common(const char *deck, const fr_mesh *mesh, const fr_setup_opts *op
   bool ok = c->setup(o);
   int st = FR_OK;
   if (!ok) {
-    st = c->err.find("mixed") != std::string::npos || c->err.find("viscous") != std::string::npos
+    st = c->err.find("mixed") != std::string::npos || c->err.find("viscous") != std::string::npos ||
+                 c->err.find("tensor-product") != std::string::npos
              ? FR_ERR_UNSUPPORTED
              : (c->err.find("cuda") != std::string::npos ? FR_ERR_CUDA : FR_ERR_SETUP);
   }
@@ -948,6 +980,7 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
   std::string n = name;
   size_t nU = (size_t)c->nS * c->E * c->nF, nUf = (size_t)c->nFp * c->E * c->nF;
   if (c->hostOnly && (n == "U_spts" || n == "U0" || n == "U_fpts" || n == "Fn_fpts" || n == "waveSp_fpts" ||
+                      n == "dUc_fpts" || n == "dU_spts" || n == "dU_fpts" ||
                       n == "ele_dt" || n == "F_spts" || n == "disFn_fpts" || n.rfind("divF_", 0) == 0)) {
     c->err = "host-only case: no device state";
     return FR_ERR_STATE;
@@ -960,6 +993,9 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
   if (n == "ele_dt") return copy_dev(c, c->eleDt, (size_t)c->E, host, count);
   if (n == "F_spts") return copy_dev(c, c->Fdbg, (size_t)c->nDims * nU, host, count);
   if (n == "disFn_fpts") return copy_dev(c, c->disFnDbg, nUf, host, count);
+  if (n == "dUc_fpts") return copy_dev(c, c->dUc, nUf, host, count);
+  if (n == "dU_spts") return copy_dev(c, c->dUs, (size_t)c->nDims * nU, host, count);
+  if (n == "dU_fpts") return copy_dev(c, c->dUf, (size_t)c->nDims * nUf, host, count);
   if (n.rfind("divF_", 0) == 0) {
     int s = std::atoi(n.c_str() + 5);
     if (s < 0 || s >= c->nRK) return FR_ERR_ARG;

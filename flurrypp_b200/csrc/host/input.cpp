@@ -112,6 +112,12 @@ bool read_deck(const std::string &path, Input &in, std::string &err) {
   d.get("riemannType", in.riemannType);
   d.get("testCase", in.testCase);
   if (in.viscous) {
+    // options the reference requires (no default) for viscous runs
+    for (const char *k : {"Re", "MachBound", "MachWall"})
+      if (!d.has(k)) {
+        err = std::string("Required option not found: ") + k;
+        return false;
+      }
     in.penFact = 0.0;
     in.tau = 1.0;
     d.get("LDG_penFact", in.penFact);

@@ -72,6 +72,11 @@ struct ElemArgs {
   double *disFn_dbg = nullptr;     // optional: Fn - extrapolated flux [nFp][E][nF]
   unsigned int *err = nullptr;     // device status word (bit 0: a bounded wait ran out)
   double gamma = 1.4;
+  // viscous stages: physical gradient at the solution points
+  // [nDims][nS][E][nF] (stride between dimensions dUsStride), and constants
+  const double *dUs = nullptr;
+  long long dUsStride = 0;
+  Phys ph{};
 };
 
 size_t elem_smem_bytes(int nDims, int nS, int nFp, int EB);
@@ -113,6 +118,25 @@ void launch_element_stage_tma(int nDims, int order, const ElemArgs &a, const TpT
 int tp_elems_per_block(int nDims, int order);
 void launch_element_stage_tp(int nDims, int order, const ElemArgs &a, const TpTables &t,
                              cudaStream_t st);
+
+// Viscous (LDG) stage pieces (kernels/stage_visc_fp64.cu).
+struct GradArgs {
+  int E = 0;
+  const double *U = nullptr;      // [nS][E][nF]
+  const double *dUc = nullptr;    // [nFp][E][nF] LDG jumps
+  const double *JGinv = nullptr;
+  const double *detJ = nullptr;
+  double *dUs = nullptr;          // [nDims][nS][E][nF]
+  double *dUf = nullptr;          // [nDims][nFp][E][nF]
+  long long sStride = 0, fStride = 0;
+};
+void launch_faces_ldg(int nDims, const FaceTable &ft, const double *Ufpts, double *dUc, const Phys &ph,
+                      cudaStream_t st);
+void launch_elem_grad(int nDims, int order, const GradArgs &g, const TpTables &t, cudaStream_t st);
+void launch_faces_visc(int nDims, const FaceTable &ft, const double *Ufpts, const double *dUf, long long fStride,
+                       double *Fn, double *waveSp, const Phys &ph, cudaStream_t st);
+// tensor-product element stage with the viscous flux added at the solution points
+void launch_element_stage_tp_visc(int nDims, int order, const ElemArgs &a, const TpTables &t, cudaStream_t st);
 
 // Wave speed at every flux point from U_fpts (reference: ele.cpp:1076-1125).
 void launch_wavesp_init(int nDims, int nFp, int E, const double *Ufpts, const double *norm,

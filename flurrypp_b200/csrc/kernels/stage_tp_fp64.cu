@@ -28,7 +28,7 @@ struct Tp {
   static constexpr size_t SMEM = sizeof(double) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 4 * N);
 };
 
-template <int ND, int P>
+template <int ND, int P, bool VISC>
 __global__ void __launch_bounds__(Tp<ND, P>::NT) k_elem_tp(ElemArgs a, TpTables t) {
   using T = Tp<ND, P>;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
@@ -72,6 +72,20 @@ __global__ void __launch_bounds__(Tp<ND, P>::NT) k_elem_tp(ElemArgs a, TpTables 
     const double *u = &sU[s * ROW + el * NF];
     if (valid) {
       inviscid_flux<ND, double>(u, Fp, a.gamma);
+      if (VISC) {
+        // physical viscous flux added to the physical inviscid flux
+        // (reference: solver.cpp:777-811)
+        double gU[ND][NF], Fv[ND][NF];
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+#pragma unroll
+          for (int k = 0; k < NF; k++) gU[d][k] = a.dUs[d * a.dUsStride + ((long long)s * E + e) * NF + k];
+        viscous_flux<ND, double>(u, gU, a.ph, Fv);
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+#pragma unroll
+          for (int k = 0; k < NF; k++) Fp[d][k] = Fv[d][k] + Fp[d][k];
+      }
     } else {
 #pragma unroll
       for (int d = 0; d < ND; d++)
@@ -209,16 +223,16 @@ __global__ void __launch_bounds__(Tp<ND, P>::NT) k_elem_tp(ElemArgs a, TpTables 
   }
 }
 
-template <int ND, int P>
+template <int ND, int P, bool VISC = false>
 void launch_tp(const ElemArgs &a, const TpTables &t, cudaStream_t st) {
   using T = Tp<ND, P>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_elem_tp<ND, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    cudaFuncSetAttribute(k_elem_tp<ND, P, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
   int g = (a.E + T::EB - 1) / T::EB;
-  k_elem_tp<ND, P><<<g, T::NT, T::SMEM, st>>>(a, t);
+  k_elem_tp<ND, P, VISC><<<g, T::NT, T::SMEM, st>>>(a, t);
 }
 
 }  // namespace
@@ -241,6 +255,15 @@ void launch_element_stage_tp(int nDims, int order, const ElemArgs &a, const TpTa
   FR_TP_CASE(2, 0) FR_TP_CASE(2, 1) FR_TP_CASE(2, 2) FR_TP_CASE(2, 3) FR_TP_CASE(2, 4) FR_TP_CASE(2, 5)
   FR_TP_CASE(3, 0) FR_TP_CASE(3, 1) FR_TP_CASE(3, 2) FR_TP_CASE(3, 3) FR_TP_CASE(3, 4) FR_TP_CASE(3, 5)
 #undef FR_TP_CASE
+}
+
+void launch_element_stage_tp_visc(int nDims, int order, const ElemArgs &a, const TpTables &t, cudaStream_t st) {
+  if (a.E <= 0) return;
+#define FR_TPV_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_tp<ND, P, true>(a, t, st);
+  FR_TPV_CASE(2, 0) FR_TPV_CASE(2, 1) FR_TPV_CASE(2, 2) FR_TPV_CASE(2, 3) FR_TPV_CASE(2, 4) FR_TPV_CASE(2, 5)
+  FR_TPV_CASE(3, 0) FR_TPV_CASE(3, 1) FR_TPV_CASE(3, 2) FR_TPV_CASE(3, 3) FR_TPV_CASE(3, 4) FR_TPV_CASE(3, 5)
+#undef FR_TPV_CASE
 }
 
 }  // namespace frk

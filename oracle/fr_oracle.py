@@ -240,6 +240,114 @@ def boundary_state(bc, UL, n, ph):
     return UR
 
 
+def viscous_flux(U, gU, ph, quirk=True):
+    """Navier-Stokes viscous flux Fv[d, ..., k] (src/flux.cpp:79-210).
+
+    U[..., k], gU[d, ..., k] physical gradient.  With quirk, the reference's
+    3-D tauxz/tauyz and the z-momentum entries of the x/y fluxes are kept."""
+    nd = gU.shape[0]
+    rho = U[..., 0]
+    u = U[..., 1] / rho
+    v = U[..., 2] / rho
+    e = U[..., nd + 1] / rho - 0.5 * (u * u + v * v)
+    if nd == 3:
+        w = U[..., 3] / rho
+        e = e - 0.5 * (w * w)
+    else:
+        w = np.zeros_like(rho)
+    g = lambda d, k: gU[d][..., k]
+    dRho_dx, dRhoU_dx, dRhoV_dx, dE_dx = g(0, 0), g(0, 1), g(0, 2), g(0, nd + 1)
+    dRho_dy, dRhoU_dy, dRhoV_dy, dE_dy = g(1, 0), g(1, 1), g(1, 2), g(1, nd + 1)
+    z = np.zeros_like(rho)
+    dRho_dz = dRhoU_dz = dRhoV_dz = dRhoW_dx = dRhoW_dy = dRhoW_dz = dE_dz = z
+    if nd == 3:
+        dRho_dz, dRhoU_dz, dRhoV_dz = g(2, 0), g(2, 1), g(2, 2)
+        dRhoW_dx, dRhoW_dy, dRhoW_dz, dE_dz = g(0, 3), g(1, 3), g(2, 3), g(2, 4)
+    mu = np.full_like(rho, ph["mu_inf"])
+    if not ph.get("fixVis", 0):
+        rt = (ph["gamma"] - 1.0) * e / ph["rt_inf"]
+        mu = mu * (rt ** 1.5 * (1. + ph["c_sth"]) / (rt + ph["c_sth"]))
+    du_dx = (dRhoU_dx - dRho_dx * u) / rho
+    du_dy = (dRhoU_dy - dRho_dy * u) / rho
+    dv_dx = (dRhoV_dx - dRho_dx * v) / rho
+    dv_dy = (dRhoV_dy - dRho_dy * v) / rho
+    du_dz = dv_dz = dw_dx = dw_dy = dw_dz = z
+    if nd == 3:
+        du_dz = (dRhoU_dz - dRho_dz * u) / rho
+        dv_dz = (dRhoV_dz - dRho_dz * v) / rho
+        dw_dx = (dRhoW_dx - dRho_dx * w) / rho
+        dw_dy = (dRhoW_dy - dRho_dy * w) / rho
+        dw_dz = (dRhoW_dz - dRho_dz * w) / rho
+    if nd == 2:
+        dK_dx = 0.5 * (u * u + v * v) * dRho_dx + rho * (u * du_dx + v * dv_dx)
+        dK_dy = 0.5 * (u * u + v * v) * dRho_dy + rho * (u * du_dy + v * dv_dy)
+        dK_dz = z
+    else:
+        q = u * u + v * v + w * w
+        dK_dx = 0.5 * q * dRho_dx + rho * (u * du_dx + v * dv_dx + w * dw_dx)
+        dK_dy = 0.5 * q * dRho_dy + rho * (u * du_dy + v * dv_dy + w * dw_dy)
+        dK_dz = 0.5 * q * dRho_dz + rho * (u * du_dz + v * dv_dz + w * dw_dz)
+    de_dx = (dE_dx - dK_dx - dRho_dx * e) / rho
+    de_dy = (dE_dy - dK_dy - dRho_dy * e) / rho
+    de_dz = (dE_dz - dK_dz - dRho_dz * e) / rho if nd == 3 else z
+    diag = (du_dx + dv_dy + dw_dz) / 3.0
+    tauxx = 2.0 * mu * (du_dx - diag)
+    tauyy = 2.0 * mu * (dv_dy - diag)
+    tauxy = mu * (du_dy + dv_dx)
+    tauxz = tauyz = tauzz = z
+    if nd == 3:
+        if quirk:
+            tauxz = mu * (du_dz + dv_dx)
+            tauyz = mu * (du_dz + dv_dy)
+        else:
+            tauxz = mu * (du_dz + dw_dx)
+            tauyz = mu * (dv_dz + dw_dy)
+        tauzz = 2.0 * mu * (dw_dz - diag)
+    kq = (mu / ph["prandtl"]) * ph["gamma"]
+    F = np.zeros((nd,) + U.shape)
+    F[0, ..., 1] = -tauxx
+    F[0, ..., 2] = -tauxy
+    F[0, ..., nd + 1] = -(u * tauxx + v * tauxy + w * tauxz + kq * de_dx)
+    F[1, ..., 1] = -tauxy
+    F[1, ..., 2] = -tauyy
+    F[1, ..., nd + 1] = -(u * tauxy + v * tauyy + w * tauyz + kq * de_dy)
+    if nd == 3:
+        F[0, ..., 3] = -tauzz if quirk else -tauxz
+        F[1, ..., 3] = -tauyz
+        F[2, ..., 1] = -tauxz
+        F[2, ..., 2] = -tauyz
+        F[2, ..., 3] = -tauzz
+        F[2, ..., 4] = -(u * tauxz + v * tauyz + w * tauzz + kq * de_dz)
+    return F
+
+
+def ldg_pen(n, penFact):
+    """Penalty direction switch (src/face.cpp:596-604)."""
+    nd = n.shape[-1]
+    s = n[:, 0] + n[:, 1] if nd == 2 else n[:, 0] + n[:, 1] + np.sqrt(2.) * n[:, 2]
+    return np.where(s < 0, -penFact, penFact)
+
+
+def adiabatic_gradient(UL, UR, gL, gamma):
+    """Right gradient at an adiabatic wall (src/boundFace.cpp:316-350)."""
+    nd = gL.shape[0]
+    g = gL.copy()
+    rhovSq = np.sum(UL[:, 1:nd + 1] ** 2, axis=1)
+    pL = (gamma - 1.) * (UL[:, nd + 1] - 0.5 * rhovSq / UL[:, 0])
+    e = pL / ((gamma - 1.) * UR[:, 0])
+    gradVel = np.empty((nd, nd, UL.shape[0]))
+    for d1 in range(nd):
+        for d2 in range(nd):
+            gradVel[d1, d2] = (gL[d1][:, d2 + 1] - gL[d1][:, 0] * UR[:, d2 + 1] / UR[:, 0]) / UR[:, 0]
+    vSq = np.sum(UR[:, 1:nd + 1] ** 2 / (UR[:, :1] ** 2), axis=1)
+    for d1 in range(nd):
+        v = (e + 0.5 * vSq) * gL[d1][:, 0]
+        for d2 in range(nd):
+            v = v + UR[:, d2 + 1] * gradVel[d2, d1]
+        g[d1][:, nd + 1] = v
+    return g
+
+
 class OracleCase:
     """A case described by its setup arrays (reference layout)."""
 
@@ -252,6 +360,9 @@ class OracleCase:
         self.grad = [arrays[f"opp_grad_spts_{d}"] for d in range(nd)]
         self.extFn = [arrays[f"opp_extrapolateFn_{d}"] for d in range(nd)]
         self.corr = arrays["opp_correction"]
+        self.viscous = int(params.get("viscous", 0))
+        if self.viscous:
+            self.corrU = [arrays[f"opp_correctU_{d}"] for d in range(nd)]
         self.detJ = arrays["detJac_spts"]
         self.JGinv = arrays["JGinv_spts"]
         self.norm = arrays["norm_fpts"]
@@ -272,6 +383,7 @@ class OracleCase:
         self.wSurf = spt_weights(nd - 1, self.order) if nd == 3 else gauss_weights(self.order)
         self.waveSp = np.zeros(self.nFp * self.E)
         self.nRK, self.RKa, self.RKb = rk_table(int(params.get("timeType", 4)), self.order)
+        self.quirk = bool(params.get("visc_flux_quirk", 1))
         self.iter = 0
         self.dt = float(params.get("dt", 0.0))
         self.eleDt = np.zeros(self.E)
@@ -315,11 +427,104 @@ class OracleCase:
             Fn[self.slotL[b]] = Fb * dA[self.slotL[b]][:, None]
         return Fn.reshape(Uf.shape)
 
+    def faces_viscous(self, U, Uf):
+        """Viscous calcResidual up to Fn and F_spts (solver.cpp:366-445 with
+        viscous = 1): LDG solution, corrected gradient, viscous fluxes."""
+        nd, nF = self.nd, self.nF
+        ph = self.p
+        gam = ph["gamma"]
+        Ufl = Uf.reshape(-1, nF)
+        n = self.norm.reshape(-1, nd)[self.slotL]
+        dA = self.dA.ravel()
+        m = self.interior
+        b = ~m
+        UL = Ufl[self.slotL]
+        # 1. gradient in reference space (solver.cpp:1060-1078)
+        dUr = [np.einsum("ts,sek->tek", self.grad[d], U) for d in range(nd)]
+        # 2. inviscid common flux (kept per face point, before *dA) and LDG solution
+        Fn_raw = np.zeros_like(UL)
+        URall = np.empty_like(UL)
+        URall[m] = Ufl[self.slotR[m]]
+        if b.any():
+            URall[b] = boundary_state(self.fbc[b], UL[b], n[b], ph)
+        if nd == 2 and int(ph.get("riemannType", 0)) == 1:
+            Fn_raw[m] = roe2d(UL[m], URall[m], n[m], gam)
+        else:
+            Fn_raw[m], ws = rusanov(UL[m], URall[m], n[m], gam)
+            self.waveSp[self.slotL[m]] = ws
+        if b.any():
+            Fn_raw[b], wsb = rusanov(UL[b], URall[b], n[b], gam)
+            self.waveSp[self.slotL[b]] = wsb
+        dUc = np.zeros_like(Ufl)
+        pen = ldg_pen(n[m], ph["penFact"])[:, None]
+        UC = 0.5 * (UL[m] + URall[m]) - pen * (UL[m] - URall[m])
+        dUc[self.slotL[m]] = UC - UL[m]
+        dUc[self.slotR[m]] = UC - URall[m]
+        if b.any():
+            dUc[self.slotL[b]] = 0.5 * (UL[b] + URall[b]) - UL[b]
+        dUc = dUc.reshape(Uf.shape)
+        # 3. correction and physical transform (solver.cpp:1080-1137)
+        for d in range(nd):
+            dUr[d] = dUr[d] + np.einsum("sf,fek->sek", self.corrU[d], dUc)
+        invDet = (1. / self.detJ)[..., None]
+        dU = []
+        for d2 in range(nd):
+            v = dUr[0] * self.JGinv[0, :, :, d2][..., None] + dUr[1] * self.JGinv[1, :, :, d2][..., None]
+            if nd == 3:
+                v = v + dUr[2] * self.JGinv[2, :, :, d2][..., None]
+            dU.append(invDet * v)
+        dU = np.array(dU)
+        dUf = np.array([self.extrapolate(dU[d]) for d in range(nd)])  # solver.cpp:1139-1158
+        # 4. flux at the solution points (solver.cpp:777-811)
+        Fv = viscous_flux(U, dU, ph, self.quirk) + inviscid_flux(U, gam)
+        F = np.zeros_like(Fv)
+        for d1 in range(nd):
+            for d2 in range(nd):
+                F[d1] = F[d1] + self.JGinv[d1, :, :, d2][..., None] * Fv[d2]
+        # 5. viscous common flux (face.cpp:210-311)
+        gflat = dUf.reshape(nd, -1, nF)
+        gL = gflat[:, self.slotL]
+        Fn_tot = Fn_raw.copy()
+        if m.any():
+            gR = gflat[:, self.slotR[m]]
+            FL = viscous_flux(UL[m], gL[:, m], ph, self.quirk)
+            FR = viscous_flux(URall[m], gR, ph, self.quirk)
+            nn = n[m]
+            pen = ldg_pen(nn, ph["penFact"])[:, None]
+            dUj = UL[m] - URall[m]
+            dF = [FL[0] - FR[0], FL[1] - FR[1]]
+            if nd == 3:
+                dF.append(FL[1] - FR[2] if self.quirk else FL[2] - FR[2])
+            sdot = sum(nn[:, d:d + 1] * dF[d] for d in range(nd)) if nd == 3 else \
+                nn[:, 0:1] * dF[0] + nn[:, 1:2] * dF[1]
+            for d in range(nd):
+                Fc = 0.5 * (FL[d] + FR[d]) + pen * nn[:, d:d + 1] * sdot + ph["tau"] * nn[:, d:d + 1] * dUj
+                Fn_tot[m] = Fn_tot[m] + Fc * nn[:, d:d + 1]
+        if b.any():
+            adi = self.fbc[b] == BC_ADI_NOSLIP
+            Fv_b = viscous_flux(UL[b], gL[:, b], ph, self.quirk)
+            if adi.any():
+                bi = np.nonzero(b)[0][adi]
+                gA = adiabatic_gradient(UL[bi], URall[bi], gflat[:, self.slotL[bi]], gam)
+                Fv_b[:, adi] = viscous_flux(URall[bi], gA, ph, self.quirk)
+            nb = n[b]
+            for d in range(nd):
+                Fc = Fv_b[d] + ph["tau"] * nb[:, d:d + 1] * (UL[b] - URall[b])
+                Fn_tot[b] = Fn_tot[b] + Fc * nb[:, d:d + 1]
+        Fn = np.zeros_like(Ufl)
+        Fn[self.slotL] = Fn_tot * dA[self.slotL][:, None]
+        Fn[self.slotR[m]] = -Fn_tot[m] * dA[self.slotR[m]][:, None]
+        self.last_visc = {"dU_spts": dU, "dU_fpts": dUf, "dUc_fpts": dUc}
+        return F, Fn.reshape(Uf.shape)
+
     def residual(self, U, keep: dict | None = None):
         """divF of solver::calcResidual (solver.cpp:366-445)."""
         Uf = self.extrapolate(U)
-        F = self.flux_spts(U)
-        Fn = self.faces(Uf)
+        if self.viscous:
+            F, Fn = self.faces_viscous(U, Uf)
+        else:
+            F = self.flux_spts(U)
+            Fn = self.faces(Uf)
         disFn = np.einsum("fs,sek->fek", self.extFn[0], F[0])
         for d in range(1, self.nd):
             disFn = disFn + np.einsum("fs,sek->fek", self.extFn[d], F[d])
@@ -415,11 +620,33 @@ def params_from_deck(path: str) -> dict:
     f = lambda k, d: float(vals.get(k, d))
     i = lambda k, d: int(float(vals.get(k, d)))
     nd = i("nDims", 2)
-    return {
+    p = {
         "nDims": nd, "order": i("order", 3), "gamma": f("gamma", 1.4),
         "rhoBound": f("rhoBound", 1.0), "uBound": f("uBound", 0.2), "vBound": f("vBound", 0.0),
         "wBound": f("wBound", 0.0) if nd == 3 else 0.0, "pBound": f("pBound", 0.7142857143),
         "riemannType": i("riemannType", 0), "timeType": i("timeType", 4), "dtType": i("dtType", 0),
         "CFL": f("CFL", 0.0), "dt": f("dt", 0.0), "RGas": f("RGas", 286.9), "TWall": f("TWall", 300.0),
-        "uWall": 0.0, "vWall": 0.0, "wWall": 0.0,
+        "uWall": 0.0, "vWall": 0.0, "wWall": 0.0, "viscous": i("viscous", 0),
     }
+    if p["viscous"]:
+        # input::nonDimensionalize (src/input.cpp:526-596)
+        g = p["gamma"]
+        Re, Lref, muGas = f("Re", 0.0), f("Lref", 1.0), f("muGas", 1.827e-5)
+        SGas, TGas, RGas = f("SGas", 120.0), f("TGas", 291.15), f("RGas", 286.9)
+        TBound, TWall, M = f("TBound", 300.0), f("TWall", 300.0), f("MachBound", 0.0)
+        nxB, nyB, nzB = f("nxBound", 1.0), f("nyBound", 0.0), f("nzBound", 0.0) if nd == 3 else 0.0
+        nm = np.sqrt(nxB * nxB + nyB * nyB + nzB * nzB)
+        nxB, nyB, nzB = nxB / nm, nyB / nm, nzB / nm
+        UB = M * np.sqrt(g * RGas * TBound)
+        muB = muGas * (TBound / TGas) ** 1.5 * ((TGas + SGas) / (TBound + SGas))
+        rhoB = muB * Re / (UB * Lref)
+        pB = rhoB * RGas * TBound
+        rhoRef = rhoB
+        pRef = rhoRef * UB * UB
+        muRef = rhoRef * UB * Lref
+        p.update(c_sth=SGas / TGas, mu_inf=muGas / muRef, rt_inf=TGas * RGas / (UB * UB),
+                 RGas=RGas * TBound / (UB * UB), rhoBound=1.0, uBound=UB * nxB / UB, vBound=UB * nyB / UB,
+                 wBound=UB * nzB / UB, pBound=pB / pRef, TWall=TWall / TBound,
+                 prandtl=f("prandtl", 0.72), fixVis=i("fixVis", 0), penFact=f("LDG_penFact", 0.0),
+                 tau=f("LDG_tau", 1.0))
+    return p

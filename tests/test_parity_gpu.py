@@ -43,6 +43,14 @@ def test_residual_matches_reference(case):
     assert rel_err(s.get_array("Fn_fpts").reshape(a["Fn_fpts"].shape), a["Fn_fpts"]) < 1e-12
     assert rel_err(s.get_array("disFn_fpts").reshape(a["disFn_fpts"].shape), a["disFn_fpts"], fscale) < RESID_TOL
     assert shp == s.shape
+    if "dU_spts" in a:  # viscous: LDG jumps and corrected gradients
+        # dUc = UC - U is a difference of nearly equal traces: measured
+        # against the size of the traces
+        uscale = float(np.max(np.abs(a["U_fpts"])))
+        assert rel_err(s.get_array("dUc_fpts").reshape(a["dUc_fpts"].shape), a["dUc_fpts"], uscale) < 1e-13
+        gscale = float(np.max(np.abs(a["dU_spts"])))
+        assert rel_err(s.get_array("dU_spts").reshape(a["dU_spts"].shape), a["dU_spts"], gscale) < 1e-11
+        assert rel_err(s.get_array("dU_fpts").reshape(a["dU_fpts"].shape), a["dU_fpts"], gscale) < 1e-11
 
 
 @pytest.mark.parametrize("case", golden_cases())
