@@ -122,6 +122,7 @@ def _load() -> ctypes.CDLL:
         "fr_get_residual": (i, [P, i, dp, sz]),
         "fr_update": (i, [P, i]),
         "fr_run": (i, [P, i]),
+        "fr_pmg_cycle": (i, [P]),
         "fr_calc_dt": (i, [P, dp]),
         "fr_set_dt": (i, [P, ctypes.c_double]),
         "fr_residual_norm": (i, [P, i, dp, i]),
@@ -217,7 +218,11 @@ class Solver:
         self._check(lib.fr_update(self._c, int(pmg_source)))
 
     def run(self, nsteps: int):
+        """nsteps of update() (+ the P-multigrid cycle with PMG 1)."""
         self._check(lib.fr_run(self._c, nsteps))
+
+    def pmg_cycle(self):
+        self._check(lib.fr_pmg_cycle(self._c))
 
     def calc_dt(self) -> float:
         d = ctypes.c_double()

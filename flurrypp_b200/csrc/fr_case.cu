@@ -69,10 +69,17 @@ struct fr_case {
   cudaGraphExec_t graph = nullptr;
   bool ownStream = false;
   bool hostOnly = false;  // set up without a device: setup arrays only
+  // P-multigrid (reference: multigrid.cpp:47-384): coarse levels share the
+  // mesh and the stream; index = order, null below lowOrder
+  std::vector<std::unique_ptr<fr_case>> levels;
+  bool pmgCoarse = false;
+  double *sol = nullptr, *corrPmg = nullptr;
+  frk::Csr restrictOp, prolongOp;
 
   ~fr_case() {
-    if (graph) cudaGraphExecDestroy(graph);
     if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    levels.clear();  // coarse levels use this case's stream: release them first
     for (auto &b : allocs) cudaFree(b.p);
     if (ownStream && ownedStream) cudaStreamDestroy(ownedStream);
   }
@@ -145,10 +152,12 @@ struct fr_case {
     hostOnly = o.device < 0;
     if (hostOnly) return setup_host();
     if (cudaSetDevice(o.device) != cudaSuccess) return fail(FR_ERR_CUDA, "cudaSetDevice failed");
-    if (!stream && cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
-      return fail(FR_ERR_CUDA, "stream create");
-    ownStream = true;
-    ownedStream = stream;
+    if (!stream) {
+      if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(FR_ERR_CUDA, "stream create");
+      ownStream = true;
+      ownedStream = stream;
+    }
     if (o.precision != FR_PREC_FP64)
       return fail(FR_ERR_UNSUPPORTED, "mixed precision is served by the batch API");
     if (!setup_host()) return false;
@@ -265,8 +274,115 @@ struct fr_case {
     hostDt = in.dt;
     if (cudaMemcpyAsync(dt, &hostDt, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "dt upload");
+    if (in.PMG) {
+      if (!alloc(src, nU) || !alloc(sol, nU) || !alloc(corrPmg, nU)) return false;
+      if (in.order > 0 && !make_csr(op.restrict_, op.nSptsRes, nS, restrictOp)) return false;
+      if (!make_csr(op.prolong, op.nSptsPro, nS, prolongOp)) return false;
+      if (!pmgCoarse && !build_levels()) return false;
+    }
     if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(FR_ERR_CUDA, "setup sync");
     return cuda_ok("setup");
+  }
+
+  // Coarse P levels (multiGrid::setup, multigrid.cpp:111-139): each a solver
+  // of order P on the same mesh, with the deck's initial condition applied
+  // (solver::initializeSolution(true)), which also fixes their initial wave
+  // speeds for CFL-based stepping.
+  bool build_levels() {
+    if (in.lowOrder < 0 || in.lowOrder >= in.order) return in.order == 0 || fail(FR_ERR_ARG, "bad lowOrder");
+    levels.clear();
+    levels.resize(in.order);
+    for (int P = in.lowOrder; P < in.order; P++) {
+      std::unique_ptr<fr_case> L(new fr_case());
+      L->in = in;
+      L->in.order = P;
+      L->mesh = mesh;
+      L->pmgCoarse = true;
+      L->stream = stream;
+      if (!L->setup(opts)) return fail(FR_ERR_SETUP, "P-multigrid level " + std::to_string(P) + ": " + L->err);
+      std::vector<double> Uic;
+      std::string e;
+      if (!fr::initial_condition(L->in, L->geo, L->nS, L->E, fr::IC_DECK, nullptr, 0, Uic, e))
+        return fail(FR_ERR_SETUP, e);
+      if (!L->set_state_host(Uic.data())) return fail(FR_ERR_CUDA, L->err);
+      levels[P] = std::move(L);
+    }
+    return true;
+  }
+
+  bool set_state_host(const double *Uh) {
+    size_t count = (size_t)nS * E * nF;
+    if (cudaMemcpyAsync(U, Uh, count * sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "cudaMemcpy H2D failed");
+    extrapolate();
+    if (in.dtType != 0) {  // solver::initializeSolution, solver.cpp:1932-1938
+      frk::launch_wavesp_init(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
+      launches++;
+    }
+    stateSet = true;
+    return cuda_ok("set_state");
+  }
+
+  // restrict_pmg (multigrid.cpp:315-345): U and divF[0] to the next coarser level
+  void restrict_to(fr_case &C) {
+    const long long N = (long long)C.E * C.nF;
+    frk::launch_apply_op(restrictOp, U, C.U, N, 1.0, 0.0, stream);
+    frk::launch_apply_op(restrictOp, divF[0], C.divF[0], N, 1.0, 0.0, stream);
+    C.fptsFresh = false;
+    launches += 2;
+  }
+  // prolong_err (multigrid.cpp:347-364): finer U += prolong(corr)
+  void prolong_to(fr_case &F) {
+    frk::launch_apply_op(prolongOp, corrPmg, F.U, (long long)E * nF, 1.0, 1.0, stream);
+    F.fptsFresh = false;
+    launches++;
+  }
+
+  // multiGrid::cycle (multigrid.cpp:169-313) for this (finest) level
+  bool pmg_cycle() {
+    if (!in.PMG || levels.empty()) return fail(FR_ERR_STATE, "no P-multigrid levels (PMG 0)");
+    const long long nU = (long long)nS * E * nF;
+    if (!calc_residual(0)) return false;
+    restrict_to(*levels[in.order - 1]);
+    for (int P = in.order - 1; P >= in.lowOrder; P--) {
+      fr_case &L = *levels[P];
+      const long long n = (long long)L.nS * L.E * L.nF;
+      // compute_source_term (multigrid.cpp:366-384)
+      cudaMemcpyAsync(L.src, L.divF[0], n * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+      if (!L.calc_residual(0)) return fail(FR_ERR_CUDA, L.err);
+      frk::launch_add(n, L.src, L.src, L.divF[0], -1.0, stream);
+      cudaMemcpyAsync(L.sol, L.U, n * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+      L.launches++;
+      for (int st = 0; st < in.smoothSteps; st++)
+        if (!L.update(true)) return fail(FR_ERR_CUDA, L.err);
+      if (P - 1 >= in.lowOrder) {
+        if (!L.calc_residual(0)) return fail(FR_ERR_CUDA, L.err);
+        frk::launch_add(n, L.divF[0], L.divF[0], L.src, 1.0, stream);
+        L.launches++;
+        L.restrict_to(*levels[P - 1]);
+      }
+    }
+    for (int P = in.lowOrder; P <= in.order - 1; P++) {
+      fr_case &L = *levels[P];
+      const long long n = (long long)L.nS * L.E * L.nF;
+      for (int st = 0; st < in.smoothSteps; st++)
+        if (!L.update(true)) return fail(FR_ERR_CUDA, L.err);
+      frk::launch_add(n, L.corrPmg, L.U, L.sol, -1.0, stream);
+      L.launches++;
+      if (P < in.order - 1)
+        L.prolong_to(*levels[P + 1]);
+      else
+        L.prolong_to(*this);
+    }
+    (void)nU;
+    return cuda_ok("pmg_cycle");
+  }
+
+  long long total_launches() const {
+    long long n = launches;
+    for (auto &L : levels)
+      if (L) n += L->total_launches();
+    return n;
   }
 
   // Mesh, faces, metrics and operators on the host (no device needed).
@@ -481,7 +597,9 @@ struct fr_case {
   // solver::calcDt (solver.cpp:447-468): the first iteration recomputes the
   // wave speeds from U_fpts; afterwards the face kernel's (left-only) values.
   void calc_dt_dev() {
-    if (iter == 1) {
+    // coarse P levels never re-initialise (their iteration counter stays at
+    // the initial one in the reference, multigrid.cpp:94-98 copies params)
+    if (iter == 1 && !pmgCoarse) {
       frk::launch_wavesp_init(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
       launches++;
     }
@@ -585,12 +703,21 @@ struct fr_case {
     return update_once(pmgSource);
   }
 
+  // one step of the driver loop: update, then the P-multigrid cycle when on
+  // (reference: flurry.cpp:162-170)
+  bool step_once() {
+    if (!update_once(false)) return false;
+    if (in.PMG && !pmgCoarse && !levels.empty()) return pmg_cycle();
+    return true;
+  }
+
   bool run(int n) {
     if (!stateSet) return fail(FR_ERR_STATE, "no state set");
     if (n <= 0) return true;
     // the first iteration differs (wave-speed initialisation); run it eagerly
-    while (n > 0 && (iter < 1 || !fptsFresh)) {
-      if (!update(false)) return false;
+    while (n > 0 && iter < 1) {
+      iter++;
+      if (!step_once()) return false;
       n--;
     }
     if (n <= 0) return true;
@@ -601,10 +728,10 @@ struct fr_case {
       iter = 2;  // steady-state branch
       if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return fail(FR_ERR_CUDA, "begin capture");
-      long long before = launches;
-      update_once(false);
-      graphKernels = (int)(launches - before);
-      launches = before;
+      long long before = total_launches();
+      step_once();
+      graphKernels = (int)(total_launches() - before);
+      launches -= graphKernels;  // counted again at every replay
       if (cudaStreamEndCapture(stream, &g) != cudaSuccess) return fail(FR_ERR_CUDA, "end capture");
       iter = saveIter;
       if (cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) {
@@ -778,7 +905,7 @@ int fr_get_info(fr_case *c, fr_info *info) {
   info->dtType = c->in.dtType;
   info->timeType = c->in.timeType;
   info->iter = c->iter;
-  info->launches = c->launches;
+  info->launches = c->total_launches();
   info->tensor_kernels = c->useTma ? 2 : (c->useTp ? 1 : 0);
   if (c->U && !c->hostOnly) {
     if (!c->sync()) return FR_ERR_CUDA;
@@ -880,6 +1007,16 @@ int fr_update(fr_case *c, int pmg_source) {
   }
   bool ok = c->update(pmg_source != 0);
   return ok ? FR_OK : (c->err == "no state set" ? FR_ERR_STATE : FR_ERR_CUDA);
+}
+
+int fr_pmg_cycle(fr_case *c) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = "no device state";
+    return FR_ERR_STATE;
+  }
+  bool ok = c->pmg_cycle();
+  return ok ? FR_OK : (c->err.find("no P-multigrid") != std::string::npos ? FR_ERR_STATE : FR_ERR_CUDA);
 }
 
 int fr_run(fr_case *c, int nsteps) {

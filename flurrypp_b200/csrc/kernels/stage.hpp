@@ -152,6 +152,10 @@ void launch_store_min(const unsigned long long *bits, double *dt, double *time_a
                       cudaStream_t st);
 void launch_add_time(const double *dt, double *time_acc, cudaStream_t st);
 
+// out[i] = x[i] + sgn * y[i] (sgn = +1 or -1), the elementwise updates of the
+// P-multigrid cycle (reference: multigrid.cpp:199-205, 282-290, 366-384).
+void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st);
+
 // Per-element residual norm contributions (reference: ele.cpp:1922-1944).
 void launch_residual_norm(int nS, int E, int nF, const double *divF, const double *detJ,
                           const double *wSpt, int resType, double *eleRes, cudaStream_t st);

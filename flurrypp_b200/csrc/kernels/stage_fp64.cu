@@ -304,6 +304,13 @@ __global__ void k_residual_norm(int nS, int E, int nF, const double *__restrict_
   }
 }
 
+__global__ void k_add(long long n, double *__restrict__ out, const double *__restrict__ x,
+                      const double *__restrict__ y, double sgn) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = sgn > 0 ? x[i] + y[i] : x[i] - y[i];
+}
+
 __global__ void k_check_state(long long n, int nF, const double *__restrict__ U, unsigned int *bad) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -397,6 +404,11 @@ void launch_residual_norm(int nS, int E, int nF, const double *divF, const doubl
                           const double *wSpt, int resType, double *eleRes, cudaStream_t st) {
   if (E <= 0) return;
   k_residual_norm<<<(E + 127) / 128, 128, 0, st>>>(nS, E, nF, divF, detJ, wSpt, resType, eleRes);
+}
+
+void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st) {
+  if (n <= 0) return;
+  k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, out, x, y, sgn);
 }
 
 void launch_check_state(int nS, int E, int nF, const double *U, unsigned int *bad, cudaStream_t st) {

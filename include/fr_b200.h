@@ -130,7 +130,14 @@ int fr_get_residual(fr_case *c, int step, double *divF, size_t count);
 /* One time step, all RK stages (solver::update, include/solver.hpp:172,
  * src/solver.cpp:319-363); advances time by dt. */
 int fr_update(fr_case *c, int pmg_source);
-/* n steps; the steady-state step is captured once as a CUDA graph. */
+/* One P-multigrid V-cycle on the case's coarse levels (multiGrid::cycle,
+ * src/multigrid.cpp:169-313); the deck must have PMG 1.  The levels
+ * (orders lowOrder .. order-1, same mesh) are built by fr_create_*. */
+int fr_pmg_cycle(fr_case *c);
+
+/* n steps of the reference's driver loop: update(), then, with PMG 1, the
+ * V-cycle (src/flurry.cpp:162-170).  The steady-state step is captured once
+ * as a CUDA graph and replayed. */
 int fr_run(fr_case *c, int nsteps);
 
 /* CFL time step (solver::calcDt, src/solver.cpp:447-468); *dt = global dt. */

@@ -38,6 +38,19 @@ def deck_path(meta):
     return os.path.join(DECKS, meta["deck"] + ".deck")
 
 
+def deck_option(meta, key, default=None):
+    """First value of `key` in the fixture's deck (the reference's rule)."""
+    for line in open(deck_path(meta)):
+        t = line.split()
+        if len(t) > 1 and t[0] == key:
+            return t[1]
+    return default
+
+
+def has_pmg(meta):
+    return int(float(deck_option(meta, "PMG", 0))) == 1
+
+
 def harness_ic(meta):
     """(kind, params) of the product's fr_init_solution matching the fixture."""
     a = meta["harness_args"]

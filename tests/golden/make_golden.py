@@ -70,6 +70,8 @@ CASES = {
     "ns_vortex2d_p3_6": ("ns_vortex2d_p3_6", ["--ic", "vortex", "--vortex", "3,0,0,0.5", "--cfl-dt", "0.3"], 10, "all"),
     "ns_walls2d_p2": ("ns_walls2d_p2", ["--ic", "uniform", "--cfl-dt", "0.2"], 10, "all"),
     "ns_sutherland2d_p3": ("ns_sutherland2d_p3", ["--ic", "vortex", "--vortex", "2,0,0,0.3"], 10, "all"),
+    "pmg_vortex2d_p3_8": ("pmg_vortex2d_p3_8", ["--ic", "vortex", "--vortex", "5,0,0,0.5"], 5, "all"),
+    "pmg_tgv3d_p3_3": ("pmg_tgv3d_p3_3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.4"], 3, "all"),
     "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5"], 5, "all"),
 }
 

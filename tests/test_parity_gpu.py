@@ -14,7 +14,7 @@ import pytest
 
 import flurrypp_b200 as fb
 import fr_oracle as O
-from conftest import deck_path, golden_cases, harness_ic, load_golden, perturb_opts, rel_err
+from conftest import deck_path, golden_cases, harness_ic, has_pmg, load_golden, perturb_opts, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -60,6 +60,8 @@ def test_steps_match_reference(case):
     s.set_state(a["U_init"])
     for _ in range(meta["steps"]):
         s.update()
+        if has_pmg(meta):  # the driver's loop: update, then the V-cycle
+            s.pmg_cycle()
     U = s.get_state()
     assert rel_err(U, a["U_final"]) < STEP_TOL
     if "ele_dt" in a:
@@ -70,7 +72,7 @@ def test_steps_match_reference(case):
 
 
 @pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "localdt_jameson2d_p3",
-                                  "channel2d_p2", "euler_fwd2d_p1"])
+                                  "channel2d_p2", "euler_fwd2d_p1", "pmg_vortex2d_p3_8", "ns_walls2d_p2"])
 def test_graph_run_equals_update_loop(case):
     """fr_run (CUDA-graph steady state) gives the same bits as fr_update."""
     a, meta = load_golden(case)
@@ -79,6 +81,8 @@ def test_graph_run_equals_update_loop(case):
     s2.set_state(a["U_init"])
     for _ in range(meta["steps"]):
         s1.update()
+        if has_pmg(meta):
+            s1.pmg_cycle()
     s2.run(meta["steps"])
     assert np.array_equal(s1.get_state(), s2.get_state())
 
