@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -810,17 +811,41 @@ int create_common(const char *deck, const fr_mesh *mesh, const fr_setup_opts *op
     for (int d = 0; d < 3; d++) m.period[d] = mesh->period[d];
     m.periodicTol = c->in.periodicTol;
   } else {
-    if (c->in.meshType != 1) {
-      c->err = "deck reads a mesh file: pass the mesh with fr_create_with_mesh";
+    if (c->in.meshType == 0) {
+      // mesh file named in the deck, relative to the deck's directory first
+      std::string mf = c->in.meshFileName;
+      std::string dk = deck;
+      size_t sl = dk.find_last_of('/');
+      if (!mf.empty() && mf[0] != '/' && sl != std::string::npos) {
+        std::string cand = dk.substr(0, sl + 1) + mf;
+        if (FILE *fp = std::fopen(cand.c_str(), "r")) {
+          std::fclose(fp);
+          mf = cand;
+        }
+      }
+      if (!fr::read_gmsh(mf, c->in, c->mesh, e)) {
+        c->err = e;
+        *out = c.release();
+        return e.find("open") != std::string::npos ? FR_ERR_ARG
+                                                   : (e.find("not on the B200") != std::string::npos ? FR_ERR_UNSUPPORTED
+                                                                                                     : FR_ERR_SETUP);
+      }
+      std::string e2;
+      if (!fr::finalize_input(c->in, e2)) {
+        c->err = e2;
+        *out = c.release();
+        return FR_ERR_UNSUPPORTED;
+      }
+    } else if (c->in.meshType != 1) {
+      c->err = "meshType 2 (overset) is not on the B200 path";
       *out = c.release();
       return FR_ERR_UNSUPPORTED;
-    }
-    if (!fr::create_cartesian_mesh(c->in, c->mesh, e)) {
+    } else if (!fr::create_cartesian_mesh(c->in, c->mesh, e)) {
       c->err = e;
       *out = c.release();
       return FR_ERR_SETUP;
     }
-    if (o.perturb) fr::perturb_interior_vertices(c->in, c->mesh, o.seed, o.perturb_frac);
+    if (o.perturb && c->in.meshType == 1) fr::perturb_interior_vertices(c->in, c->mesh, o.seed, o.perturb_frac);
   }
   bool ok = c->setup(o);
   int st = FR_OK;

@@ -149,7 +149,18 @@ struct Mesh {
   std::vector<int> bndFaceBc;
   double period[3] = {1e300, 1e300, 1e300};
   double periodicTol = 1e-6;
+  // Alternatively, boundaries as vertex sets (Gmsh input): a boundary face
+  // takes the BC of the first set holding all its vertices
+  // (reference: src/geo.cpp:290-305, 476-497).
+  std::vector<std::vector<int>> bndPointSets;  // sorted vertex ids per boundary
+  std::vector<int> bndPointBc;
 };
+
+// Gmsh 2.x ASCII reader for linear quads (type 3) and hexes (type 5), with
+// $PhysicalNames boundaries mapped through the deck's mesh_bound entries
+// (reference: src/geo.cpp:1021-1475).  Higher-order (curved) elements are
+// rejected.
+bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err);
 
 // Cartesian generator (reference: src/geo.cpp:1477-1762): same vertex and
 // element numbering, BCs from the create_bc* options.

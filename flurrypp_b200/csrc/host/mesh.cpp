@@ -2,8 +2,11 @@
 // periodic pairing, flux-point orientation and metric terms.
 #include <algorithm>
 #include <cmath>
+#include <fstream>
 #include <map>
 #include <random>
+#include <set>
+#include <sstream>
 #include <unordered_map>
 
 #include "fr_host.hpp"
@@ -138,6 +141,137 @@ void perturb_interior_vertices(const Input &in, Mesh &m, uint64_t seed, double f
   }
 }
 
+bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err) {
+  std::ifstream f(path);
+  if (!f.is_open()) {
+    err = "Unable to open mesh file " + path;
+    return false;
+  }
+  std::string line;
+  auto seek = [&](const char *tag) {
+    f.clear();
+    f.seekg(0, std::ios::beg);
+    while (std::getline(f, line))
+      if (line.find(tag) != std::string::npos) return true;
+    return false;
+  };
+  // $PhysicalNames: boundary tag -> boundary index (in file order) and BC
+  if (!seek("$PhysicalNames")) {
+    err = "$PhysicalNames tag not found in Gmsh file!";
+    return false;
+  }
+  int nNames = 0;
+  f >> nNames;
+  std::getline(f, line);
+  std::map<int, int> tag2bnd;  // -1: fluid
+  std::vector<int> bndBc;
+  int nd = in.nDims;
+  for (int i = 0; i < nNames; i++) {
+    std::getline(f, line);
+    std::stringstream ss(line);
+    int dim, id;
+    std::string name;
+    ss >> dim >> id >> name;
+    name.erase(std::remove(name.begin(), name.end(), '"'), name.end());
+    std::transform(name.begin(), name.end(), name.begin(), ::tolower);
+    std::string bcName;
+    for (auto &kv : in.meshBounds)
+      if (kv.first == name) bcName = kv.second;
+    if (bcName.empty()) {
+      err = "Unrecognized mesh boundary: \"" + name + "\"";
+      return false;
+    }
+    if (bcName == "fluid") {
+      nd = dim;
+      tag2bnd[id] = -1;
+      continue;
+    }
+    int bc = bc_from_string(bcName);
+    if (bc == -100 || bc == BC_NONE) {
+      err = "Unrecognized boundary condition: \"" + bcName + "\"";
+      return false;
+    }
+    tag2bnd[id] = (int)bndBc.size();
+    bndBc.push_back(bc);
+  }
+  in.nDims = nd;
+  m.nDims = nd;
+  // $Nodes: positions in file order (node ids are assumed 1..n in order)
+  if (!seek("$Nodes")) {
+    err = "$Nodes tag not found in Gmsh file!";
+    return false;
+  }
+  f >> m.nVerts;
+  std::getline(f, line);
+  m.xv.assign((size_t)m.nVerts * nd, 0.0);
+  for (int i = 0; i < m.nVerts; i++) {
+    std::getline(f, line);
+    std::stringstream ss(line);
+    long long id;
+    ss >> id;
+    for (int d = 0; d < nd; d++) ss >> m.xv[(size_t)i * nd + d];
+  }
+  if (!seek("$Elements")) {
+    err = "$Elements tag not found in Gmsh file!";
+    return false;
+  }
+  long long nEl = 0;
+  f >> nEl;
+  std::getline(f, line);
+  std::vector<std::set<int>> pts(bndBc.size());
+  m.nNodes = nd == 2 ? 4 : 8;
+  m.c2v.clear();
+  m.nEles = 0;
+  for (long long k = 0; k < nEl; k++) {
+    std::getline(f, line);
+    std::stringstream ss(line);
+    int id, type, nTags, tag0 = 0, tmp;
+    ss >> id >> type >> nTags;
+    if (nTags > 0) ss >> tag0;
+    for (int t = 1; t < nTags; t++) ss >> tmp;
+    auto it = tag2bnd.find(tag0);
+    if (it == tag2bnd.end()) {
+      err = "element with an unknown physical tag";
+      return false;
+    }
+    if (it->second == -1) {
+      int nv = type == 3 ? 4 : (type == 5 ? 8 : -1);
+      if (nv < 0 || nv != m.nNodes) {
+        err = "Gmsh element type " + std::to_string(type) +
+              " not on the B200 path (linear quads and hexes only)";
+        return false;
+      }
+      for (int v = 0; v < nv; v++) {
+        int g;
+        ss >> g;
+        m.c2v.push_back(g - 1);
+      }
+      m.nEles++;
+    } else {
+      int np = type == 1 ? 2 : (type == 3 ? 4 : (type == 8 ? 3 : (type == 10 || type == 16 ? 4 : -1)));
+      if (np < 0) {
+        err = "Boundary Element (Face) Type Not Recognized!";
+        return false;
+      }
+      for (int v = 0; v < np; v++) {
+        int g;
+        ss >> g;
+        pts[it->second].insert(g - 1);
+      }
+    }
+  }
+  m.bndFaceVerts.clear();
+  m.bndFaceBc.clear();
+  m.bndPointSets.clear();
+  m.bndPointBc = bndBc;
+  for (auto &p : pts) m.bndPointSets.emplace_back(p.begin(), p.end());
+  m.period[0] = in.periodicDX;
+  m.period[1] = in.periodicDY;
+  m.period[2] = in.periodicDZ;
+  m.periodicTol = in.periodicTol;
+  return true;
+}
+
 namespace {
 
 // Local face -> element vertices, in the order that the element's flux
@@ -263,6 +397,20 @@ bool build_faces(const Mesh &m, int order, int ptsType, std::vector<Face> &faces
       if (pr.first.e != e || pr.first.f != f) continue;  // emitted once, at first side
       if (pr.second.e >= 0) {
         interior.push_back(pr);
+      } else if (!m.bndPointSets.empty()) {
+        // first boundary holding every vertex of the face
+        int nfv = nd == 2 ? 2 : 4, bc = -100;
+        for (size_t bi = 0; bi < m.bndPointSets.size() && bc == -100; bi++) {
+          bool all = true;
+          for (int q = 0; q < nfv && all; q++)
+            all = std::binary_search(m.bndPointSets[bi].begin(), m.bndPointSets[bi].end(), k.v[q]);
+          if (all) bc = m.bndPointBc[bi];
+        }
+        if (bc == -100) {
+          err = "boundary face without a boundary condition";
+          return false;
+        }
+        boundary.push_back({pr.first, bc});
       } else {
         auto b = bndBc.find(k);
         if (b == bndBc.end()) {

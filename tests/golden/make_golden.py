@@ -72,6 +72,8 @@ CASES = {
     "ns_sutherland2d_p3": ("ns_sutherland2d_p3", ["--ic", "vortex", "--vortex", "2,0,0,0.3"], 10, "all"),
     "pmg_vortex2d_p3_8": ("pmg_vortex2d_p3_8", ["--ic", "vortex", "--vortex", "5,0,0,0.5"], 5, "all"),
     "pmg_tgv3d_p3_3": ("pmg_tgv3d_p3_3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.4"], 3, "all"),
+    "chbump_p2_pmg": ("chbump_p2_pmg", [], 5, "all"),
+    "chbump_p3": ("chbump_p3", [], 10, "all"),
     "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5"], 5, "all"),
 }
 
@@ -99,7 +101,8 @@ def run_case(name: str) -> None:
     deck_path = os.path.join(HERE, "decks", deck + ".deck")
     with tempfile.TemporaryDirectory() as td:
         cmd = [HARNESS, deck_path, td] + args + ["--steps", str(steps)]
-        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+        # mesh files named in a deck are relative to the deck's directory
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=os.path.join(HERE, "decks"))
         arrays, meta = read_dump(td)
     names = SETUP + RESID + FINAL if keep == "all" else keep
     out = {k: arrays[k] for k in names if k in arrays}
