@@ -131,6 +131,13 @@ def _load() -> ctypes.CDLL:
         "fr_device_ptr": (i, [P, ctypes.c_char_p, ctypes.POINTER(P), ctypes.POINTER(sz)]),
         "fr_synchronize": (i, [P]),
         "fr_bench_kernel": (i, [P, ctypes.c_char_p, i]),
+        "fr_batch_create": (i, [ctypes.POINTER(P), i, ctypes.POINTER(P)]),
+        "fr_batch_run": (i, [P, i]),
+        "fr_batch_gather": (i, [P]),
+        "fr_batch_residual_norms": (i, [P, i, dp, i]),
+        "fr_batch_info": (i, [P, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]),
+        "fr_batch_last_error": (ctypes.c_char_p, [P]),
+        "fr_batch_destroy": (None, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -263,6 +270,50 @@ class Solver:
         b = ctypes.c_size_t()
         self._check(lib.fr_device_ptr(self._c, name.encode(), ctypes.byref(p), ctypes.byref(b)))
         return p.value, b.value
+
+
+class Batch:
+    """Many independent cases advanced together (fr_batch_*): same-order cases
+    merged into one group, one face + one element launch per stage per order."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s._c.value for s in self.solvers])
+        self._b = ctypes.c_void_p()
+        st = lib.fr_batch_create(arr, len(self.solvers), ctypes.byref(self._b))
+        if st != FR_OK:
+            msg = lib.fr_batch_last_error(self._b).decode() if self._b else "batch create failed"
+            lib.fr_batch_destroy(self._b)
+            self._b = None
+            raise FrError(st, msg)
+
+    def __del__(self):
+        if getattr(self, "_b", None):
+            lib.fr_batch_destroy(self._b)
+            self._b = None
+
+    def _check(self, st):
+        if st != FR_OK:
+            raise FrError(st, lib.fr_batch_last_error(self._b).decode())
+
+    def run(self, nsteps: int):
+        self._check(lib.fr_batch_run(self._b, nsteps))
+
+    def gather(self):
+        """Copy every member's state (and last stage-0 residual) back to its case."""
+        self._check(lib.fr_batch_gather(self._b))
+
+    def residual_norms(self, res_type: int = 2) -> np.ndarray:
+        nf = self.solvers[0].nFields
+        out = np.empty((len(self.solvers), nf), dtype=np.float64)
+        self._check(lib.fr_batch_residual_norms(self._b, res_type, _dptr(out), nf))
+        return out
+
+    def info(self):
+        g = ctypes.c_int()
+        n = ctypes.c_longlong()
+        self._check(lib.fr_batch_info(self._b, ctypes.byref(g), ctypes.byref(n)))
+        return {"groups": g.value, "launches": n.value}
 
 
 def _make_mesh(m: dict):

@@ -74,6 +74,9 @@ struct fr_case {
   // mesh and the stream; index = order, null below lowOrder
   std::vector<std::unique_ptr<fr_case>> levels;
   bool pmgCoarse = false;
+  // batch group: several cases merged along the element axis, each with its
+  // own fixed dt held per element
+  bool perElementDt = false;
   double *sol = nullptr, *corrPmg = nullptr;
   frk::Csr restrictOp, prolongOp;
 
@@ -162,7 +165,13 @@ struct fr_case {
     if (o.precision != FR_PREC_FP64)
       return fail(FR_ERR_UNSUPPORTED, "mixed precision is served by the batch API");
     if (!setup_host()) return false;
+    return setup_device();
+  }
 
+  // Device buffers, uploads, face table, operator tables (after setup_host or
+  // after a merge of several cases' host data).
+  bool setup_device() {
+    const fr_setup_opts &o = opts;
     size_t nU = (size_t)nS * E * nF, nUf = (size_t)nFp * E * nF;
     if (!alloc(U, nU) || !alloc(U0, nU) || !alloc(acc, nU) || !alloc(Ufpts, nUf) || !alloc(Fn, nUf))
       return false;
@@ -557,6 +566,92 @@ struct fr_case {
     return true;
   }
 
+  // Merge the host data of several same-order cases along the element axis
+  // (face element indices shifted, metric arrays concatenated), then set up
+  // the device side and copy the members' states and time steps in.
+  bool merge_from(const std::vector<fr_case *> &ms, const fr_setup_opts &o) {
+    opts = o;
+    opts.debug_arrays = 0;
+    const fr_case &f = *ms[0];
+    in = f.in;
+    nDims = f.nDims;
+    nF = f.nF;
+    nRK = f.nRK;
+    nS = f.nS;
+    nFp = f.nFp;
+    nPF = f.nPF;
+    op = f.op;
+    perElementDt = true;
+    E = 0;
+    std::vector<int> off;
+    for (auto *m : ms) {
+      off.push_back(E);
+      E += m->E;
+    }
+    mesh.nDims = nDims;
+    mesh.nEles = E;
+    auto cat = [&](std::vector<double> fr::Geometry::*field, size_t A, size_t B) {
+      std::vector<double> out(A * (size_t)E * B);
+      for (size_t a = 0; a < A; a++)
+        for (size_t k = 0; k < ms.size(); k++) {
+          const auto &src = ms[k]->geo.*field;
+          const size_t Em = ms[k]->E;
+          std::copy(src.begin() + a * Em * B, src.begin() + (a + 1) * Em * B,
+                    out.begin() + (a * (size_t)E + off[k]) * B);
+        }
+      geo.*field = std::move(out);
+    };
+    cat(&fr::Geometry::pos_spts, nS, nDims);
+    cat(&fr::Geometry::pos_fpts, nFp, nDims);
+    cat(&fr::Geometry::detJac_spts, nS, 1);
+    cat(&fr::Geometry::detJac_fpts, nFp, 1);
+    cat(&fr::Geometry::JGinv_spts, (size_t)nDims * nS, nDims);
+    cat(&fr::Geometry::norm_fpts, nFp, nDims);
+    cat(&fr::Geometry::dA_fpts, nFp, 1);
+    faces.clear();
+    for (size_t k = 0; k < ms.size(); k++)
+      for (auto fc : ms[k]->faces) {
+        fc.eL += off[k];
+        if (fc.eR >= 0) fc.eR += off[k];
+        faces.push_back(std::move(fc));
+      }
+    if (cudaSetDevice(o.device) != cudaSuccess) return fail(FR_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "stream create");
+    ownStream = true;
+    ownedStream = stream;
+    if (!setup_device()) return false;
+    std::vector<double> edt(E);
+    for (size_t k = 0; k < ms.size(); k++) {
+      fr_case &m = *ms[k];
+      if (!m.sync()) return fail(FR_ERR_CUDA, m.err);
+      for (int e = 0; e < m.E; e++) edt[off[k] + e] = m.hostDt;
+      if (cudaMemcpy2DAsync(U + (size_t)off[k] * nF, (size_t)E * nF * sizeof(double), m.U,
+                            (size_t)m.E * nF * sizeof(double), (size_t)m.E * nF * sizeof(double), nS,
+                            cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+        return fail(FR_ERR_CUDA, "state gather failed");
+    }
+    if (cudaMemcpyAsync(eleDt, edt.data(), E * sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "dt upload failed");
+    extrapolate();
+    stateSet = true;
+    return sync();
+  }
+
+  // Copy a member's slice of this merged state back into the member case.
+  bool scatter_to(fr_case &m, int offset) {
+    if (cudaMemcpy2DAsync(m.U, (size_t)m.E * nF * sizeof(double), U + (size_t)offset * nF,
+                          (size_t)E * nF * sizeof(double), (size_t)m.E * nF * sizeof(double), nS,
+                          cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "state scatter failed");
+    if (cudaMemcpy2DAsync(m.divF[0], (size_t)m.E * nF * sizeof(double), divF[0] + (size_t)offset * nF,
+                          (size_t)E * nF * sizeof(double), (size_t)m.E * nF * sizeof(double), nS,
+                          cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "residual scatter failed");
+    m.fptsFresh = false;
+    return true;
+  }
+
   frk::ElemArgs elem_args() {
     frk::ElemArgs a;
     a.E = E;
@@ -575,7 +670,7 @@ struct fr_case {
     a.ext = ext;
     a.nRK = nRK;
     a.dt = dt;
-    a.eleDt = in.dtType == 2 ? eleDt : nullptr;
+    a.eleDt = (in.dtType == 2 || perElementDt) ? eleDt : nullptr;
     a.U0 = U0;
     a.acc = acc;
     a.Uout = U;
@@ -764,6 +859,20 @@ struct fr_case {
     return true;
   }
   bool timedOut = false;
+};
+
+// Many independent cases advanced together: same-order cases are merged into
+// one group case (elements concatenated, faces offset), so each RK stage is
+// one face launch and one element launch per order present, and a whole step
+// of a group replays as one CUDA graph; groups of different orders run on
+// their own streams concurrently.
+struct fr_batch {
+  std::string err;
+  std::vector<fr_case *> members;                 // not owned
+  std::vector<std::unique_ptr<fr_case>> groups;   // one per order present
+  std::vector<std::vector<int>> groupMembers;     // member indices per group
+  std::vector<std::vector<int>> groupOffsets;     // element offset of each member
+  long long steps = 0;
 };
 
 namespace {
@@ -1253,6 +1362,121 @@ int fr_bench_kernel(fr_case *c, const char *kernel, int reps) {
   }
   return c->cuda_ok("bench_kernel") ? FR_OK : FR_ERR_CUDA;
 }
+
+int fr_batch_create(fr_case *const *cases, int n, fr_batch **out) {
+  if (!cases || n <= 0 || !out) return FR_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<fr_batch> b(new fr_batch());
+  for (int i = 0; i < n; i++) {
+    fr_case *c = cases[i];
+    if (!c || c->hostOnly || !c->stateSet) return FR_ERR_STATE;
+    if (c->in.viscous || c->in.PMG || c->in.dtType != 0 || c->in.nDims != cases[0]->in.nDims ||
+        c->in.timeType != cases[0]->in.timeType) {
+      return FR_ERR_UNSUPPORTED;  // batches hold inviscid, fixed-dt cases of one RK scheme
+    }
+    b->members.push_back(c);
+  }
+  std::vector<int> orders;
+  for (auto *c : b->members)
+    if (std::find(orders.begin(), orders.end(), c->in.order) == orders.end()) orders.push_back(c->in.order);
+  std::sort(orders.begin(), orders.end());
+  for (int P : orders) {
+    std::vector<fr_case *> ms;
+    std::vector<int> idx, offs;
+    int off = 0;
+    for (int i = 0; i < n; i++)
+      if (b->members[i]->in.order == P) {
+        ms.push_back(b->members[i]);
+        idx.push_back(i);
+        offs.push_back(off);
+        off += b->members[i]->E;
+      }
+    std::unique_ptr<fr_case> g(new fr_case());
+    fr_setup_opts o = ms[0]->opts;
+    if (!g->merge_from(ms, o)) {
+      *out = b.release();
+      (*out)->err = g->err;
+      return FR_ERR_CUDA;
+    }
+    b->groups.push_back(std::move(g));
+    b->groupMembers.push_back(idx);
+    b->groupOffsets.push_back(offs);
+  }
+  *out = b.release();
+  return FR_OK;
+}
+
+int fr_batch_run(fr_batch *b, int nsteps) {
+  if (!b || nsteps < 0) return FR_ERR_ARG;
+  for (auto &g : b->groups)
+    if (!g->run(nsteps)) {
+      b->err = g->err;
+      return FR_ERR_CUDA;
+    }
+  for (auto &g : b->groups)
+    if (!g->sync()) {
+      b->err = g->err;
+      return g->timedOut ? FR_ERR_TIMEOUT : FR_ERR_CUDA;
+    }
+  b->steps += nsteps;
+  return FR_OK;
+}
+
+int fr_batch_gather(fr_batch *b) {
+  if (!b) return FR_ERR_ARG;
+  for (size_t gi = 0; gi < b->groups.size(); gi++) {
+    fr_case &g = *b->groups[gi];
+    for (size_t k = 0; k < b->groupMembers[gi].size(); k++)
+      if (!g.scatter_to(*b->members[b->groupMembers[gi][k]], b->groupOffsets[gi][k])) {
+        b->err = g.err;
+        return FR_ERR_CUDA;
+      }
+    if (!g.sync()) {
+      b->err = g.err;
+      return FR_ERR_CUDA;
+    }
+  }
+  return FR_OK;
+}
+
+int fr_batch_residual_norms(fr_batch *b, int resType, double *out, int nFields) {
+  if (!b || !out || resType < 1 || resType > 3 || b->groups.empty() || nFields != b->groups[0]->nF)
+    return FR_ERR_ARG;
+  for (size_t gi = 0; gi < b->groups.size(); gi++) {
+    fr_case &g = *b->groups[gi];
+    frk::launch_residual_norm(g.nS, g.E, g.nF, g.divF[0], g.detJ, g.wSpt, resType, g.eleRes, g.stream);
+    std::vector<double> er((size_t)g.E * g.nF);
+    if (!g.sync()) return FR_ERR_CUDA;
+    cudaMemcpy(er.data(), g.eleRes, er.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    for (size_t k = 0; k < b->groupMembers[gi].size(); k++) {
+      const int mi = b->groupMembers[gi][k], e0 = b->groupOffsets[gi][k], Em = b->members[mi]->E;
+      for (int f = 0; f < g.nF; f++) {
+        double r = 0;
+        for (int e = e0; e < e0 + Em; e++) {
+          double v = er[(size_t)e * g.nF + f];
+          r = resType == 3 ? std::max(r, v) : r + v;
+        }
+        out[(size_t)mi * nFields + f] = resType == 2 ? std::sqrt(r) : r;
+      }
+    }
+  }
+  return FR_OK;
+}
+
+int fr_batch_info(fr_batch *b, int *nGroups, long long *launches) {
+  if (!b) return FR_ERR_ARG;
+  if (nGroups) *nGroups = (int)b->groups.size();
+  if (launches) {
+    long long n = 0;
+    for (auto &g : b->groups) n += g->total_launches();
+    *launches = n;
+  }
+  return FR_OK;
+}
+
+const char *fr_batch_last_error(const fr_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+void fr_batch_destroy(fr_batch *b) { delete b; }
 
 int fr_synchronize(fr_case *c) {
   if (!c) return FR_ERR_ARG;

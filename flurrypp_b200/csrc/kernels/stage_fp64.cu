@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256) k_element_stage(ElemArgs a) {
     const int s = it / EB, el = it - s * EB;
     const int e = e0 + el;
     if (el >= nValid) continue;
-    const double dJ = a.detJ[(long long)s * E + e];
+    const double rdJ = 1.0 / a.detJ[(long long)s * E + e];  // one reciprocal per point
     const double dt = a.eleDt ? a.eleDt[e] : dtg;
 #pragma unroll
     for (int k = 0; k < NF; k++) {
@@ -204,16 +204,16 @@ __global__ void __launch_bounds__(256) k_element_stage(ElemArgs a) {
       if (a.mode == MODE_RK_STAGE) {
         const double u0 = a.stage == 0 ? u : a.U0[gi];
         if (a.stage == 0) a.U0[gi] = u;
-        unew = u0 - a.rka_next * div / dJ * dt;
+        unew = u0 - a.rka_next * div * rdJ * dt;
         const double base = a.stage == 0 ? u0 : a.acc[gi];
-        a.acc[gi] = base - a.rkb * div / dJ * dt;
+        a.acc[gi] = base - a.rkb * div * rdJ * dt;
       } else if (a.mode == MODE_RK_FINAL) {
         const double base = a.nRK == 1 ? u : a.acc[gi];
-        unew = base - a.rkb * div / dJ * dt;
+        unew = base - a.rkb * div * rdJ * dt;
       } else {  // MODE_JAMESON
         const double u0 = a.stage == 0 ? u : a.U0[gi];
         if (a.stage == 0) a.U0[gi] = u;
-        unew = u0 - a.rka_next * div / dJ * dt;
+        unew = u0 - a.rka_next * div * rdJ * dt;
       }
       a.Uout[gi] = unew;
       sU[li] = unew;

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(Tp<ND, P>::NT) k_elem_tp(ElemArgs a, TpTables 
 #pragma unroll
       for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
     }
-    const double dJ = a.detJ[(long long)s * E + e];
+    const double rdJ = 1.0 / a.detJ[(long long)s * E + e];  // one reciprocal per point
     const double dt = a.eleDt ? a.eleDt[e] : (a.mode != MODE_RESIDUAL ? *a.dt : 0.0);
 #pragma unroll
     for (int k = 0; k < NF; k++) {
@@ -183,16 +183,16 @@ __global__ void __launch_bounds__(Tp<ND, P>::NT) k_elem_tp(ElemArgs a, TpTables 
       if (a.mode == MODE_RK_STAGE) {
         const double u0 = a.stage == 0 ? u : a.U0[gi];
         if (a.stage == 0) a.U0[gi] = u;
-        unew = u0 - a.rka_next * dv / dJ * dt;
+        unew = u0 - a.rka_next * dv * rdJ * dt;
         const double base = a.stage == 0 ? u0 : a.acc[gi];
-        a.acc[gi] = base - a.rkb * dv / dJ * dt;
+        a.acc[gi] = base - a.rkb * dv * rdJ * dt;
       } else if (a.mode == MODE_RK_FINAL) {
         const double base = a.nRK == 1 ? u : a.acc[gi];
-        unew = base - a.rkb * dv / dJ * dt;
+        unew = base - a.rkb * dv * rdJ * dt;
       } else {
         const double u0 = a.stage == 0 ? u : a.U0[gi];
         if (a.stage == 0) a.U0[gi] = u;
-        unew = u0 - a.rka_next * dv / dJ * dt;
+        unew = u0 - a.rka_next * dv * rdJ * dt;
       }
       a.Uout[gi] = unew;
       sU[s * ROW + el * NF + k] = unew;

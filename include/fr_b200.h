@@ -173,6 +173,25 @@ int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes);
  * timing only.  No reference counterpart. */
 int fr_bench_kernel(fr_case *c, const char *kernel, int reps);
 
+/* ---- Batching: many independent cases advanced together ----------------
+ * Same-order cases are merged along the element axis into one group, so each
+ * RK stage is one face launch and one element launch per order present and a
+ * group's whole step replays as one CUDA graph; groups of different orders run
+ * concurrently on their own streams.  Members must be inviscid, fixed-dt
+ * (dtType 0, per-case dt kept), one RK scheme, state set.  No reference
+ * counterpart (the reference runs one case per process). */
+typedef struct fr_batch fr_batch;
+int fr_batch_create(fr_case *const *cases, int n, fr_batch **out);
+/* nsteps of every member (each with its own dt), then a device sync. */
+int fr_batch_run(fr_batch *b, int nsteps);
+/* Copies each member's state and last stage-0 residual back into its case. */
+int fr_batch_gather(fr_batch *b);
+/* writeResidual norms of every member: out[n][nFields]. */
+int fr_batch_residual_norms(fr_batch *b, int resType, double *out, int nFields);
+int fr_batch_info(fr_batch *b, int *nGroups, long long *launches);
+const char *fr_batch_last_error(const fr_batch *b);
+void fr_batch_destroy(fr_batch *b);
+
 /* Blocks until the case's stream is idle; returns FR_ERR_CUDA on a sticky error. */
 int fr_synchronize(fr_case *c);
 
