@@ -138,6 +138,15 @@ def _load() -> ctypes.CDLL:
         "fr_batch_info": (i, [P, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]),
         "fr_batch_last_error": (ctypes.c_char_p, [P]),
         "fr_batch_destroy": (None, [P]),
+        "fr_server_create": (i, [sz, i, i, i, ctypes.POINTER(P)]),
+        "fr_server_submit": (i, [P, ctypes.c_char_p, ctypes.POINTER(Mesh), i, dp, i, ctypes.c_double, i,
+                                 ctypes.POINTER(ctypes.c_longlong)]),
+        "fr_server_poll": (i, [P, ctypes.c_longlong, ctypes.POINTER(i), dp, ctypes.POINTER(i), dp]),
+        "fr_server_wait": (i, [P, ctypes.c_longlong, ctypes.c_double]),
+        "fr_server_result": (i, [P, ctypes.c_longlong, dp, sz]),
+        "fr_server_cancel": (i, [P, ctypes.c_longlong]),
+        "fr_server_stats": (i, [P, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(sz)]),
+        "fr_server_destroy": (None, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -314,6 +323,65 @@ class Batch:
         n = ctypes.c_longlong()
         self._check(lib.fr_batch_info(self._b, ctypes.byref(g), ctypes.byref(n)))
         return {"groups": g.value, "launches": n.value}
+
+
+class Server:
+    """Continuous-batching solve server (fr_server_*)."""
+
+    def __init__(self, budget_bytes: int, max_inflight: int = 8, check_every: int = 10, device: int = 0):
+        self._s = ctypes.c_void_p()
+        st = lib.fr_server_create(int(budget_bytes), max_inflight, check_every, device, ctypes.byref(self._s))
+        if st != FR_OK:
+            raise FrError(st, "server create failed")
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib.fr_server_destroy(self._s)
+            self._s = None
+
+    __del__ = close
+
+    def submit(self, deck: str, mesh: dict | None = None, ic=(IC_DECK, ()), tol: float = 1e-8,
+               max_steps: int = 100000) -> int:
+        kind, prm = ic
+        p = np.ascontiguousarray(prm, dtype=np.float64)
+        m = _make_mesh(mesh) if mesh is not None else None
+        rid = ctypes.c_longlong()
+        st = lib.fr_server_submit(self._s, deck.encode(), ctypes.byref(m[0]) if m else None, kind,
+                                  _dptr(p) if p.size else None, int(p.size), tol, max_steps, ctypes.byref(rid))
+        if st != FR_OK:
+            raise FrError(st, "submit failed")
+        return rid.value
+
+    def poll(self, rid: int) -> dict:
+        stt, steps = ctypes.c_int(), ctypes.c_int()
+        lat, ratio = ctypes.c_double(), ctypes.c_double()
+        code = lib.fr_server_poll(self._s, rid, ctypes.byref(stt), ctypes.byref(lat), ctypes.byref(steps),
+                                  ctypes.byref(ratio))
+        return {"status": stt.value, "latency_s": lat.value, "steps": steps.value, "res_ratio": ratio.value,
+                "code": code}
+
+    def wait(self, rid: int, timeout_s: float = 600.0):
+        st = lib.fr_server_wait(self._s, rid, timeout_s)
+        if st != FR_OK:
+            raise FrError(st, f"request {rid} did not finish cleanly")
+
+    def result(self, rid: int, shape) -> np.ndarray:
+        U = np.empty(shape, dtype=np.float64)
+        st = lib.fr_server_result(self._s, rid, _dptr(U), U.size)
+        if st != FR_OK:
+            raise FrError(st, "no result")
+        return U
+
+    def cancel(self, rid: int):
+        lib.fr_server_cancel(self._s, rid)
+
+    def stats(self) -> dict:
+        q, f = ctypes.c_int(), ctypes.c_int()
+        b = ctypes.c_size_t()
+        lib.fr_server_stats(self._s, ctypes.byref(q), ctypes.byref(f), ctypes.byref(b))
+        return {"queued": q.value, "inflight": f.value, "inflight_bytes": b.value}
 
 
 def _make_mesh(m: dict):

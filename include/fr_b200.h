@@ -192,6 +192,27 @@ int fr_batch_info(fr_batch *b, int *nGroups, long long *launches);
 const char *fr_batch_last_error(const fr_batch *b);
 void fr_batch_destroy(fr_batch *b);
 
+/* ---- Serving: a request loop with continuous batching --------------------
+ * Requests (deck, optional mesh, initial condition, residual-drop target)
+ * are admitted while the device-memory budget and the slot count allow; all
+ * admitted cases stay on the device and advance together (own streams, graph
+ * replays, overlapping on the GPU); a case retires when max over fields of
+ * res/res0 (writeResidual norm, resType 2) <= tol or after max_steps, and
+ * waiting requests take its place.  No reference counterpart. */
+typedef struct fr_server fr_server;
+int fr_server_create(size_t budget_bytes, int max_inflight, int check_every, int device, fr_server **out);
+int fr_server_submit(fr_server *s, const char *deck, const fr_mesh *mesh, int ic_kind, const double *ic_prm,
+                     int n_prm, double tol, int max_steps, long long *id);
+/* status: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled; latency from submission. */
+int fr_server_poll(fr_server *s, long long id, int *status, double *latency_s, int *steps, double *res_ratio);
+/* Waits (bounded) for a request to finish; FR_ERR_TIMEOUT if it has not. */
+int fr_server_wait(fr_server *s, long long id, double timeout_s);
+/* Final state of a finished request, [nSpts][nEles][nFields]. */
+int fr_server_result(fr_server *s, long long id, double *U, size_t count);
+int fr_server_cancel(fr_server *s, long long id);
+int fr_server_stats(fr_server *s, int *queued, int *inflight, size_t *inflight_bytes);
+void fr_server_destroy(fr_server *s);
+
 /* Blocks until the case's stream is idle; returns FR_ERR_CUDA on a sticky error. */
 int fr_synchronize(fr_case *c);
 

@@ -1,4 +1,5 @@
 """The C-ABI library loads and exports every entry point include/*.h declares."""
+import pytest
 import ctypes
 import glob
 import os
@@ -33,3 +34,14 @@ def test_library_exports_every_declared_symbol():
 def test_default_opts():
     o = fb.default_opts()
     assert o.precision == fb.FR_PREC_FP64 and o.visc_flux_quirk == 1 and o.perturb == 0
+
+
+def test_server_reports_setup_failure_without_gpu_work(tmp_path):
+    """A request whose deck cannot be read fails with FR_ERR_ARG (host path)."""
+    srv = fb.Server(budget_bytes=1 << 20, max_inflight=1, check_every=1, device=0)
+    r = srv.submit(str(tmp_path / "missing.deck"), tol=1e-3, max_steps=1)
+    with pytest.raises(fb.FrError) as ei:
+        srv.wait(r, 30)
+    assert ei.value.code == fb.FR_ERR_ARG
+    assert srv.poll(r)["status"] == 3
+    srv.close()
