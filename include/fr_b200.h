@@ -216,6 +216,29 @@ void fr_server_destroy(fr_server *s);
 /* Blocks until the case's stream is idle; returns FR_ERR_CUDA on a sticky error. */
 int fr_synchronize(fr_case *c);
 
+/* Residual norm that allocates no device memory.  No counterpart in the
+ * reference; it computes what fr_residual_norm computes (writeResidual,
+ * src/output.cpp:1011-1090, ele.cpp:1922-1944), for callers that may not
+ * allocate device memory: applications that hand out every device byte from
+ * their own pool, and loops that may not take the synchronisation a
+ * cudaMalloc/cudaFree brings.  divF and detJ are device arrays in the
+ * library's layout ([nSpts][nEles][nFields] and [nSpts][nEles]), nFields =
+ * nDims + 2, order <= 5, nEles <= FR_NOALLOC_MAX_ELES; out is a host array of
+ * nFields.  Partial sums live in one fixed static device array of
+ * FR_NOALLOC_SCRATCH_BYTES per GPU, so:
+ *   - the first call on a device (with that device current) looks up the
+ *     array's address; make it before any stream capture;
+ *   - calls that overlap in time (other streams, other host threads) race
+ *     on the array: issue them one after another;
+ *   - nothing needs zeroing: each call writes every partial it reads.
+ * Returns when the result is in out (the stream is synchronised);
+ * FR_ERR_ARG for sizes beyond the limits, FR_ERR_NONFINITE on a NaN norm. */
+#define FR_NOALLOC_MAX_SPTS 216
+#define FR_NOALLOC_MAX_ELES 2147483647
+#define FR_NOALLOC_SCRATCH_BYTES ((1024 * 5 + 5 + FR_NOALLOC_MAX_SPTS) * 8)
+int fr_residual_norm_noalloc(const double *divF, const double *detJ, int nDims, int order, int nEles, int nFields,
+                             int resType, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
