@@ -57,6 +57,7 @@ class SetupOpts(ctypes.Structure):
         ("device", ctypes.c_int),
         ("generic_kernels", ctypes.c_int),
         ("no_tma", ctypes.c_int),
+        ("tile_variant", ctypes.c_int),
     ]
 
 
@@ -94,6 +95,8 @@ class Info(ctypes.Structure):
         ("dt", ctypes.c_double),
         ("launches", ctypes.c_longlong),
         ("tensor_kernels", ctypes.c_int),
+        ("tile_variant", ctypes.c_int),
+        ("elems_per_block", ctypes.c_int),
     ]
 
 

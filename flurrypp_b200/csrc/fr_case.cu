@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/fr_b200.h"
@@ -79,6 +80,22 @@ struct fr_case {
   bool perElementDt = false;
   double *sol = nullptr, *corrPmg = nullptr;
   frk::Csr restrictOp, prolongOp;
+  // precision form (FR_PREC_MIXED): the stage arrays in FP32; U (FP64) is
+  // the boundary copy, and detJ, norm, dA, waveSp, the time step and the
+  // norm reductions stay FP64
+  bool mixed = false;
+  struct Fp32 {
+    float *U = nullptr, *U0 = nullptr, *acc = nullptr, *comp = nullptr, *Ufpts = nullptr, *Fn = nullptr;
+    float *JGinv = nullptr, *detJ = nullptr;
+    std::vector<float *> divF;
+    float *dUc = nullptr, *dUs = nullptr, *dUf = nullptr, *Fdbg = nullptr, *disFnDbg = nullptr;
+    frk::FaceTableT<float> ft;
+    frk::TpTablesT<float> tp;
+    frk::TmaMaps tm;
+    bool useTma = false;
+    int variant = 0;
+    std::vector<float> tuneMs;  // element-stage time per tile variant (autotuner)
+  } f32;
 
   ~fr_case() {
     if (stream) cudaStreamSynchronize(stream);
@@ -162,9 +179,11 @@ struct fr_case {
       ownStream = true;
       ownedStream = stream;
     }
-    if (o.precision != FR_PREC_FP64)
-      return fail(FR_ERR_UNSUPPORTED, "mixed precision is served by the batch API");
+    if (o.precision != FR_PREC_FP64 && o.precision != FR_PREC_MIXED)
+      return fail(FR_ERR_UNSUPPORTED, "unknown precision");
+    mixed = o.precision == FR_PREC_MIXED;
     if (!setup_host()) return false;
+    if (mixed && in.PMG) return fail(FR_ERR_UNSUPPORTED, "P-multigrid runs in the plain form, not the precision form");
     return setup_device();
   }
 
@@ -173,19 +192,30 @@ struct fr_case {
   bool setup_device() {
     const fr_setup_opts &o = opts;
     size_t nU = (size_t)nS * E * nF, nUf = (size_t)nFp * E * nF;
-    if (!alloc(U, nU) || !alloc(U0, nU) || !alloc(acc, nU) || !alloc(Ufpts, nUf) || !alloc(Fn, nUf))
-      return false;
-    divF.assign(nRK, nullptr);
-    for (int s = 0; s < nRK; s++)
-      if (!alloc(divF[s], nU)) return false;
+    if (!alloc(U, nU)) return false;
+    if (!mixed) {
+      if (!alloc(U0, nU) || !alloc(acc, nU) || !alloc(Ufpts, nUf) || !alloc(Fn, nUf)) return false;
+      divF.assign(nRK, nullptr);
+      for (int s = 0; s < nRK; s++)
+        if (!alloc(divF[s], nU)) return false;
+      if (o.debug_arrays)
+        if (!alloc(Fdbg, (size_t)nDims * nU) || !alloc(disFnDbg, nUf)) return false;
+      if (!upload(JGinv, geo.JGinv_spts)) return false;
+    } else {
+      if (!alloc(f32.U, nU) || !alloc(f32.U0, nU) || !alloc(f32.acc, nU) || !alloc(f32.comp, nU) ||
+          !alloc(f32.Ufpts, nUf) || !alloc(f32.Fn, nUf))
+        return false;
+      f32.divF.assign(nRK, nullptr);
+      for (int s = 0; s < nRK; s++)
+        if (!alloc(f32.divF[s], nU)) return false;
+      if (o.debug_arrays)
+        if (!alloc(f32.Fdbg, (size_t)nDims * nU) || !alloc(f32.disFnDbg, nUf)) return false;
+      if (!upload(f32.JGinv, narrow(geo.JGinv_spts)) || !upload(f32.detJ, narrow(geo.detJac_spts))) return false;
+    }
     if (!alloc(waveSp, (size_t)nFp * E) || !alloc(eleDt, E) || !alloc(dt, 1) || !alloc(timeAcc, 1) ||
         !alloc(eleRes, (size_t)E * nF) || !alloc(dtBits, 1) || !alloc(bad, 1))
       return false;
-    if (o.debug_arrays)
-      if (!alloc(Fdbg, (size_t)nDims * nU) || !alloc(disFnDbg, nUf)) return false;
-    if (!upload(detJ, geo.detJac_spts) || !upload(JGinv, geo.JGinv_spts) ||
-        !upload(norm, geo.norm_fpts) || !upload(dA, geo.dA_fpts))
-      return false;
+    if (!upload(detJ, geo.detJac_spts) || !upload(norm, geo.norm_fpts) || !upload(dA, geo.dA_fpts)) return false;
     if (!upload(wSpt, fr::spt_weights(nDims, in.order)) || !upload(wSurf, fr::face_weights(nDims, in.order)))
       return false;
     for (int d = 0; d < nDims; d++) {
@@ -234,16 +264,24 @@ struct fr_case {
       aR[i] = fps[i].aR;
     }
     int *dsL, *dsR;
-    double *dn, *daL, *daR;
-    if (!upload(dsL, sL) || !upload(dsR, sR) || !upload(dn, nrm) || !upload(daL, aL) || !upload(daR, aR))
-      return false;
-    ft.n = (int)fps.size();
-    ft.nInterior = nInt;
-    ft.slotL = dsL;
-    ft.slotR = dsR;
-    ft.nrm = dn;
-    ft.dAL = daL;
-    ft.dAR = daR;
+    if (!upload(dsL, sL) || !upload(dsR, sR)) return false;
+    ft.n = f32.ft.n = (int)fps.size();
+    ft.nInterior = f32.ft.nInterior = nInt;
+    ft.slotL = f32.ft.slotL = dsL;
+    ft.slotR = f32.ft.slotR = dsR;
+    if (!mixed) {
+      double *dn, *daL, *daR;
+      if (!upload(dn, nrm) || !upload(daL, aL) || !upload(daR, aR)) return false;
+      ft.nrm = dn;
+      ft.dAL = daL;
+      ft.dAR = daR;
+    } else {
+      float *dn, *daL, *daR;
+      if (!upload(dn, narrow(nrm)) || !upload(daL, narrow(aL)) || !upload(daR, narrow(aR))) return false;
+      f32.ft.nrm = dn;
+      f32.ft.dAL = daL;
+      f32.ft.dAR = daR;
+    }
 
     ph.gamma = in.gamma;
     ph.rhoBound = in.rhoBound;
@@ -274,13 +312,23 @@ struct fr_case {
       EB = c;
     }
     useTp = build_tp() && !opts.generic_kernels;
-    if (useTp) EB = frk::tp_elems_per_block(nDims, in.order);
+    if (useTp) EB = mixed ? frk::tp_elems_per_block<float>(nDims, in.order) : frk::tp_elems_per_block<double>(nDims, in.order);
+    if (mixed && !useTp) return fail(FR_ERR_UNSUPPORTED, "the precision form needs the tensor-product operators");
     if (in.viscous) {
       if (!useTp) return fail(FR_ERR_UNSUPPORTED, "viscous stages need the tensor-product operators");
-      if (!alloc(dUc, nUf) || !alloc(dUs, (size_t)nDims * nU) || !alloc(dUf, (size_t)nDims * nUf)) return false;
+      if (!mixed) {
+        if (!alloc(dUc, nUf) || !alloc(dUs, (size_t)nDims * nU) || !alloc(dUf, (size_t)nDims * nUf)) return false;
+      } else {
+        if (!alloc(f32.dUc, nUf) || !alloc(f32.dUs, (size_t)nDims * nU) || !alloc(f32.dUf, (size_t)nDims * nUf))
+          return false;
+      }
     }
     if (!alloc(devErr, 1)) return false;
-    useTma = useTp && !in.viscous && !opts.no_tma && build_tma();
+    if (!mixed) {
+      useTma = useTp && !in.viscous && !opts.no_tma && build_tma();
+    } else if (useTp && !in.viscous && !opts.no_tma && E % 4 == 0) {
+      if (!autotune_tiles()) return false;
+    }
     hostDt = in.dt;
     if (cudaMemcpyAsync(dt, &hostDt, sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "dt upload");
@@ -324,9 +372,10 @@ struct fr_case {
     size_t count = (size_t)nS * E * nF;
     if (cudaMemcpyAsync(U, Uh, count * sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "cudaMemcpy H2D failed");
+    if (mixed) split_state();
     extrapolate();
     if (in.dtType != 0) {  // solver::initializeSolution, solver.cpp:1932-1938
-      frk::launch_wavesp_init(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
+      wavesp_init();
       launches++;
     }
     stateSet = true;
@@ -519,28 +568,149 @@ struct fr_case {
     tp.D = dD;
     tp.E1 = dE1;
     tp.EFn1 = dEF;
-    tp.fptBase = dfB;
-    tp.fptDn = dfD;
-    tp.fptSide = dfS;
-    tp.corrFpt = dcF;
+    tp.fptBase = f32.tp.fptBase = dfB;
+    tp.fptDn = f32.tp.fptDn = dfD;
+    tp.fptSide = f32.tp.fptSide = dfS;
+    tp.corrFpt = f32.tp.corrFpt = dcF;
     tp.corrVal = dcV;
+    if (mixed) {
+      float *fD, *fE1, *fEF, *fcV;
+      if (!upload(fD, narrow(D)) || !upload(fE1, narrow(E1)) || !upload(fEF, narrow(EF)) || !upload(fcV, narrow(cV)))
+        return false;
+      f32.tp.D = fD;
+      f32.tp.E1 = fE1;
+      f32.tp.EFn1 = fEF;
+      f32.tp.corrVal = fcV;
+    }
     return true;
   }
 
-  // TMA descriptors for the tile copies of the TMA element kernel.  The row
-  // pitch of every tensor must be a multiple of 16 bytes: E even.
-  bool build_tma() {
-    if (E % 2 != 0 || nS > 256 || nFp > 256) return false;
+  static std::vector<float> narrow(const std::vector<double> &v) {
+    std::vector<float> o(v.size());
+    for (size_t i = 0; i < v.size(); i++) o[i] = (float)v[i];
+    return o;
+  }
+
+  // TMA descriptors of the precision form's tiles for tile variant v (the
+  // box width is that variant's element block); rows are 16-byte multiples
+  // when E is a multiple of 4.
+  bool build_tma32(int v) {
+    if (E % 4 != 0 || nS > 256 || nFp > 256) return false;
+    auto encode = tensor_map_encoder();
+    if (!encode) return false;
+    const int eb = frk::tma_elems_per_block<float>(nDims, in.order, v);
+    if (eb <= 0 || eb % 4 != 0) return false;
+    auto map2 = [&](CUtensorMap *m, void *p, cuuint64_t inner, cuuint64_t outer, cuuint32_t bi, cuuint32_t bo) {
+      cuuint64_t dims[2] = {inner, outer};
+      cuuint64_t str[1] = {inner * sizeof(float)};
+      cuuint32_t box[2] = {bi, bo};
+      cuuint32_t es[2] = {1, 1};
+      return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, p, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const cuuint64_t rowU = (cuuint64_t)E * nF;
+    frk::TmaMaps &t = f32.tm;
+    bool ok = map2(&t.U, f32.U, rowU, nS, eb * nF, nS) && map2(&t.U0, f32.U0, rowU, nS, eb * nF, nS) &&
+              map2(&t.acc, f32.acc, rowU, nS, eb * nF, nS) && map2(&t.comp, f32.comp, rowU, nS, eb * nF, nS) &&
+              map2(&t.Fn, f32.Fn, rowU, nFp, eb * nF, nFp) && map2(&t.Ufpts, f32.Ufpts, rowU, nFp, eb * nF, nFp) &&
+              map2(&t.det, f32.detJ, E, nS, eb, nS);
+    if (!ok) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)E * nDims, (cuuint64_t)nS, (cuuint64_t)nDims};
+    cuuint64_t str[2] = {(cuuint64_t)E * nDims * sizeof(float), (cuuint64_t)nS * E * nDims * sizeof(float)};
+    cuuint32_t box[3] = {(cuuint32_t)(eb * nDims), (cuuint32_t)nS, (cuuint32_t)nDims};
+    cuuint32_t es[3] = {1, 1, 1};
+    return encode(&t.J, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, f32.JGinv, dims, str, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+
+  static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
       void *fn = nullptr;
       cudaDriverEntryPointQueryResult q;
       if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
           q != cudaDriverEntryPointSuccess || !fn)
-        return false;
+        return nullptr;
       encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
     }
-    const int eb = frk::tma_elems_per_block(nDims, in.order);
+    return encode;
+  }
+
+  // Tile-shape autotuner of the precision form: times the TMA element stage
+  // (an intermediate RK stage, the common case) for every tile variant on
+  // this case's own arrays and keeps the fastest.  Runs at setup, before any
+  // state exists; the arrays it touched are cleared afterwards.  Every
+  // variant computes each point with the same operations, so the choice
+  // changes the speed only, never the result.
+  bool autotune_tiles() {
+    const int nv = frk::tma_variants(true);
+    int forced = opts.tile_variant;
+    f32.tuneMs.assign(nv, -1.0f);
+    if (forced >= nv) return fail(FR_ERR_ARG, "tile_variant out of range");
+    int best = -1;
+    float bestMs = 0.0f;
+    const int tpEB = EB;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "event create");
+    for (int v = 0; v < nv; v++) {
+      if (forced >= 0 && v != forced) continue;
+      bool dup = false;  // variants that clamp to the same tile are timed once
+      for (int w = 0; w < v; w++)
+        if (frk::tma_elems_per_block<float>(nDims, in.order, w) == frk::tma_elems_per_block<float>(nDims, in.order, v))
+          dup = true;
+      if (dup && forced < 0) continue;
+      if (!build_tma32(v)) continue;
+      f32.variant = v;
+      EB = frk::tma_elems_per_block<float>(nDims, in.order, v);
+      frk::ElemArgsT<float> a = elem_args32();
+      a.mode = frk::MODE_RK_STAGE;
+      a.stage = 1;
+      a.Ufpts_out = f32.Ufpts;
+      for (int i = 0; i < 2; i++) frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
+      cudaEventRecord(e0, stream);
+      const int reps = 5;
+      for (int i = 0; i < reps; i++)
+        frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
+      cudaEventRecord(e1, stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= reps;
+      f32.tuneMs[v] = ms;
+      if (best < 0 || ms < bestMs) {
+        best = v;
+        bestMs = ms;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!cuda_ok("tile autotune")) return false;
+    if (!sync()) return false;
+    if (best < 0) {  // no TMA variant applies: tensor-product kernel
+      EB = tpEB;
+      return true;
+    }
+    if (!build_tma32(best)) return fail(FR_ERR_CUDA, "tensor map");
+    f32.variant = best;
+    f32.useTma = true;
+    EB = frk::tma_elems_per_block<float>(nDims, in.order, best);
+    const size_t nU = (size_t)nS * E * nF, nUf = (size_t)nFp * E * nF;
+    for (float *p : {f32.U, f32.U0, f32.acc, f32.comp}) cudaMemsetAsync(p, 0, nU * sizeof(float), stream);
+    cudaMemsetAsync(f32.Ufpts, 0, nUf * sizeof(float), stream);
+    cudaMemsetAsync(devErr, 0, sizeof(unsigned), stream);
+    return sync();
+  }
+
+  // TMA descriptors for the tile copies of the TMA element kernel.  The row
+  // pitch of every tensor must be a multiple of 16 bytes: E even.
+  bool build_tma() {
+    if (E % 2 != 0 || nS > 256 || nFp > 256) return false;
+    auto encode = tensor_map_encoder();
+    if (!encode) return false;
+    const int eb = frk::tma_elems_per_block<double>(nDims, in.order);
     auto map2 = [&](CUtensorMap *m, void *p, cuuint64_t inner, cuuint64_t outer, cuuint32_t bi, cuuint32_t bo) {
       cuuint64_t dims[2] = {inner, outer};
       cuuint64_t str[1] = {inner * sizeof(double)};
@@ -572,6 +742,7 @@ struct fr_case {
   bool merge_from(const std::vector<fr_case *> &ms, const fr_setup_opts &o) {
     opts = o;
     opts.debug_arrays = 0;
+    mixed = o.precision == FR_PREC_MIXED;
     const fr_case &f = *ms[0];
     in = f.in;
     nDims = f.nDims;
@@ -626,10 +797,11 @@ struct fr_case {
       fr_case &m = *ms[k];
       if (!m.sync()) return fail(FR_ERR_CUDA, m.err);
       for (int e = 0; e < m.E; e++) edt[off[k] + e] = m.hostDt;
-      if (cudaMemcpy2DAsync(U + (size_t)off[k] * nF, (size_t)E * nF * sizeof(double), m.U,
-                            (size_t)m.E * nF * sizeof(double), (size_t)m.E * nF * sizeof(double), nS,
-                            cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      if (!mixed) {
+        if (!copy_rows(U, E, off[k], m.U, m.E, 0)) return fail(FR_ERR_CUDA, "state gather failed");
+      } else if (!copy_rows(f32.U, E, off[k], m.f32.U, m.E, 0) || !copy_rows(f32.comp, E, off[k], m.f32.comp, m.E, 0)) {
         return fail(FR_ERR_CUDA, "state gather failed");
+      }
     }
     if (cudaMemcpyAsync(eleDt, edt.data(), E * sizeof(double), cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return fail(FR_ERR_CUDA, "dt upload failed");
@@ -640,16 +812,27 @@ struct fr_case {
 
   // Copy a member's slice of this merged state back into the member case.
   bool scatter_to(fr_case &m, int offset) {
-    if (cudaMemcpy2DAsync(m.U, (size_t)m.E * nF * sizeof(double), U + (size_t)offset * nF,
-                          (size_t)E * nF * sizeof(double), (size_t)m.E * nF * sizeof(double), nS,
-                          cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
-      return fail(FR_ERR_CUDA, "state scatter failed");
-    if (cudaMemcpy2DAsync(m.divF[0], (size_t)m.E * nF * sizeof(double), divF[0] + (size_t)offset * nF,
-                          (size_t)E * nF * sizeof(double), (size_t)m.E * nF * sizeof(double), nS,
-                          cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
-      return fail(FR_ERR_CUDA, "residual scatter failed");
+    if (!mixed) {
+      if (!copy_rows(m.U, m.E, 0, U, E, offset)) return fail(FR_ERR_CUDA, "state scatter failed");
+      if (!copy_rows(m.divF[0], m.E, 0, divF[0], E, offset)) return fail(FR_ERR_CUDA, "residual scatter failed");
+    } else {
+      if (!copy_rows(m.f32.U, m.E, 0, f32.U, E, offset) || !copy_rows(m.f32.comp, m.E, 0, f32.comp, E, offset))
+        return fail(FR_ERR_CUDA, "state scatter failed");
+      if (!copy_rows(m.f32.divF[0], m.E, 0, f32.divF[0], E, offset))
+        return fail(FR_ERR_CUDA, "residual scatter failed");
+    }
     m.fptsFresh = false;
     return true;
+  }
+
+  // rows [nS] of m elements: dst[s][dOff..dOff+m) = src[s][sOff..sOff+m), all
+  // fields, arrays of dE / sE elements per row
+  template <typename T>
+  bool copy_rows(T *dst, int dE, int dOff, const T *src, int sE, int sOff) {
+    const int m = std::min(dE - dOff, sE - sOff);
+    return cudaMemcpy2DAsync(dst + (size_t)dOff * nF, (size_t)dE * nF * sizeof(T), src + (size_t)sOff * nF,
+                             (size_t)sE * nF * sizeof(T), (size_t)m * nF * sizeof(T), nS, cudaMemcpyDeviceToDevice,
+                             stream) == cudaSuccess;
   }
 
   frk::ElemArgs elem_args() {
@@ -684,11 +867,45 @@ struct fr_case {
     return a;
   }
 
+  frk::ElemArgsT<float> elem_args32() {
+    frk::ElemArgsT<float> a;
+    a.E = E;
+    a.nS = nS;
+    a.nFp = nFp;
+    a.EB = EB;
+    a.U = f32.U;
+    a.JGinv = f32.JGinv;
+    a.detJ = f32.detJ;
+    a.Fn = f32.Fn;
+    a.nRK = nRK;
+    a.dt = dt;
+    a.eleDt = (in.dtType == 2 || perElementDt) ? eleDt : nullptr;
+    a.U0 = f32.U0;
+    a.acc = f32.acc;
+    a.comp = f32.comp;
+    a.Uout = f32.U;
+    a.err = devErr;
+    a.gamma = in.gamma;
+    a.ph = ph;
+    if (in.viscous) {
+      a.dUs = f32.dUs;
+      a.dUsStride = (long long)nS * E * nF;
+    }
+    return a;
+  }
+
   void extrapolate() {
-    frk::launch_apply_op(ext, U, Ufpts, (long long)E * nF, 1.0, 0.0, stream);
+    if (mixed)
+      frk::launch_apply_op_t<float>(ext, f32.U, f32.Ufpts, (long long)E * nF, stream);
+    else
+      frk::launch_apply_op(ext, U, Ufpts, (long long)E * nF, 1.0, 0.0, stream);
     launches++;
     fptsFresh = true;
   }
+
+  // precision form: (U32, comp) from the FP64 boundary copy U, and back
+  void split_state() { frk::launch_split((long long)nS * E * nF, U, f32.U, f32.comp, stream); }
+  void join_state() { frk::launch_join((long long)nS * E * nF, f32.U, f32.comp, U, stream); }
 
   // solver::calcDt (solver.cpp:447-468): the first iteration recomputes the
   // wave speeds from U_fpts; afterwards the face kernel's (left-only) values.
@@ -696,7 +913,7 @@ struct fr_case {
     // coarse P levels never re-initialise (their iteration counter stays at
     // the initial one in the reference, multigrid.cpp:94-98 copies params)
     if (iter == 1 && !pmgCoarse) {
-      frk::launch_wavesp_init(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
+      wavesp_init();
       launches++;
     }
     launches += 3;
@@ -708,8 +925,19 @@ struct fr_case {
 
   // Everything of a stage before the element kernel: the common flux Fn (and,
   // viscous, the LDG jumps and the corrected gradients it needs).
+  void wavesp_init() {
+    if (mixed)
+      frk::launch_wavesp_init<float>(nDims, nFp, E, f32.Ufpts, norm, in.gamma, waveSp, stream);
+    else
+      frk::launch_wavesp_init<double>(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
+  }
+
   void faces_pass() {
     const int nk = (ft.nInterior > 0 ? 1 : 0) + (ft.n > ft.nInterior ? 1 : 0);
+    if (mixed) {
+      faces_pass32(nk);
+      return;
+    }
     if (!in.viscous) {
       frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
       launches += nk;
@@ -730,28 +958,91 @@ struct fr_case {
     frk::launch_faces_visc(nDims, ft, Ufpts, dUf, g.fStride, Fn, waveSp, ph, stream);
     launches += 2 * nk + 1;
   }
+  void faces_pass32(int nk) {
+    if (!in.viscous) {
+      frk::launch_faces_inviscid<float>(nDims, f32.ft, f32.Ufpts, f32.Fn, waveSp, ph, stream);
+      launches += nk;
+      return;
+    }
+    frk::launch_faces_ldg<float>(nDims, f32.ft, f32.Ufpts, f32.dUc, ph, stream);
+    frk::GradArgsT<float> g;
+    g.E = E;
+    g.U = f32.U;
+    g.dUc = f32.dUc;
+    g.JGinv = f32.JGinv;
+    g.detJ = f32.detJ;
+    g.dUs = f32.dUs;
+    g.dUf = f32.dUf;
+    g.sStride = (long long)nS * E * nF;
+    g.fStride = (long long)nFp * E * nF;
+    frk::launch_elem_grad<float>(nDims, in.order, g, f32.tp, stream);
+    frk::launch_faces_visc<float>(nDims, f32.ft, f32.Ufpts, f32.dUf, g.fStride, f32.Fn, waveSp, ph, stream);
+    launches += 2 * nk + 1;
+  }
   void element(const frk::ElemArgs &a) {
     if (in.viscous)
-      frk::launch_element_stage_tp_visc(nDims, in.order, a, tp, stream);
+      frk::launch_element_stage_tp_visc<double>(nDims, in.order, a, tp, stream);
     else if (useTma)
-      frk::launch_element_stage_tma(nDims, in.order, a, tp, tm, stream);
+      frk::launch_element_stage_tma<double>(nDims, in.order, a, tp, tm, stream);
     else if (useTp)
-      frk::launch_element_stage_tp(nDims, in.order, a, tp, stream);
+      frk::launch_element_stage_tp<double>(nDims, in.order, a, tp, stream);
     else
       frk::launch_element_stage(nDims, a, stream);
     launches++;
+  }
+  void element32(const frk::ElemArgsT<float> &a) {
+    if (in.viscous)
+      frk::launch_element_stage_tp_visc<float>(nDims, in.order, a, f32.tp, stream);
+    else if (f32.useTma)
+      frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, f32.variant);
+    else
+      frk::launch_element_stage_tp<float>(nDims, in.order, a, f32.tp, stream);
+    launches++;
+  }
+  // one element-kernel launch of an RK stage in the working precision;
+  // divF of the stage is kept when keepDivF (into divF[0])
+  void element_stage(int mode, int stage, double rka, double rkb, bool keepDivF, bool pmgSource) {
+    if (!mixed) {
+      frk::ElemArgs a = elem_args();
+      a.mode = mode;
+      a.stage = stage;
+      a.rka_next = rka;
+      a.rkb = rkb;
+      a.divF_out = keepDivF ? divF[0] : nullptr;
+      a.src = pmgSource ? src : nullptr;
+      a.Ufpts_out = Ufpts;
+      element(a);
+    } else {
+      frk::ElemArgsT<float> a = elem_args32();
+      a.mode = mode;
+      a.stage = stage;
+      a.rka_next = rka;
+      a.rkb = rkb;
+      a.divF_out = keepDivF ? f32.divF[0] : nullptr;
+      a.Ufpts_out = f32.Ufpts;
+      element32(a);
+    }
   }
 
   bool calc_residual(int step) {
     if (step < 0 || step >= nRK) return fail(FR_ERR_ARG, "step out of range");
     extrapolate();
     faces_pass();
-    frk::ElemArgs a = elem_args();
-    a.mode = frk::MODE_RESIDUAL;
-    a.divF_out = divF[step];
-    a.F_dbg = Fdbg;
-    a.disFn_dbg = disFnDbg;
-    element(a);
+    if (!mixed) {
+      frk::ElemArgs a = elem_args();
+      a.mode = frk::MODE_RESIDUAL;
+      a.divF_out = divF[step];
+      a.F_dbg = Fdbg;
+      a.disFn_dbg = disFnDbg;
+      element(a);
+    } else {
+      frk::ElemArgsT<float> a = elem_args32();
+      a.mode = frk::MODE_RESIDUAL;
+      a.divF_out = f32.divF[step];
+      a.F_dbg = f32.Fdbg;
+      a.disFn_dbg = f32.disFnDbg;
+      element32(a);
+    }
     return cuda_ok("calc_residual");
   }
 
@@ -762,31 +1053,15 @@ struct fr_case {
     for (int step = 0; step < nRK - 1; step++) {
       if (step == 0 && in.dtType != 0) calc_dt_dev();
       faces_pass();
-      frk::ElemArgs a = elem_args();
-      a.mode = jameson ? frk::MODE_JAMESON : frk::MODE_RK_STAGE;
-      a.stage = step;
-      a.rka_next = in.RKa[step + 1];
-      a.rkb = jameson ? 0.0 : in.RKb[step];
-      a.divF_out = step == 0 ? divF[0] : nullptr;
-      a.src = pmgSource ? src : nullptr;
-      a.Ufpts_out = Ufpts;
-      element(a);
+      element_stage(jameson ? frk::MODE_JAMESON : frk::MODE_RK_STAGE, step, in.RKa[step + 1],
+                    jameson ? 0.0 : in.RKb[step], step == 0, pmgSource);
     }
     faces_pass();
     if (nRK == 1 && in.dtType != 0) calc_dt_dev();
-    frk::ElemArgs a = elem_args();
-    a.stage = nRK - 1;
-    a.src = pmgSource ? src : nullptr;
-    a.divF_out = nRK == 1 ? divF[0] : nullptr;
-    a.Ufpts_out = Ufpts;
-    if (jameson) {
-      a.mode = frk::MODE_JAMESON;
-      a.rka_next = in.RKa[nRK];
-    } else {
-      a.mode = frk::MODE_RK_FINAL;
-      a.rkb = in.RKb[nRK - 1];
-    }
-    element(a);
+    if (jameson)
+      element_stage(frk::MODE_JAMESON, nRK - 1, in.RKa[nRK], 0.0, nRK == 1, pmgSource);
+    else
+      element_stage(frk::MODE_RK_FINAL, nRK - 1, 0.0, in.RKb[nRK - 1], nRK == 1, pmgSource);
     frk::launch_add_time(dt, timeAcc, stream);
     launches++;
     fptsFresh = true;
@@ -980,7 +1255,10 @@ int copy_out(fr_case *c, const std::vector<T> &h, void *host, size_t *count) {
   return FR_OK;
 }
 
-int copy_dev(fr_case *c, const double *d, size_t n, void *host, size_t *count) {
+// Copies a device array out as FP64 (FP32 arrays of the precision form are
+// widened on the host).
+template <typename T>
+int copy_dev(fr_case *c, const T *d, size_t n, void *host, size_t *count) {
   if (!count) return FR_ERR_ARG;
   if (!d) {
     c->err = "array not kept (enable debug_arrays)";
@@ -991,10 +1269,18 @@ int copy_dev(fr_case *c, const double *d, size_t n, void *host, size_t *count) {
   if (!host) return FR_OK;
   if (cap < n) return FR_ERR_ARG;
   if (!c->sync()) return FR_ERR_CUDA;
-  if (cudaMemcpy(host, d, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+  std::vector<T> tmp;
+  void *dst = host;
+  if (!std::is_same<T, double>::value) {
+    tmp.resize(n);
+    dst = tmp.data();
+  }
+  if (cudaMemcpy(dst, d, n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess) {
     c->err = "cudaMemcpy D2H failed";
     return FR_ERR_CUDA;
   }
+  if (!std::is_same<T, double>::value)
+    for (size_t i = 0; i < n; i++) static_cast<double *>(host)[i] = (double)tmp[i];
   return FR_OK;
 }
 
@@ -1007,6 +1293,7 @@ void fr_setup_opts_default(fr_setup_opts *o) {
   std::memset(o, 0, sizeof(*o));
   o->precision = FR_PREC_FP64;
   o->visc_flux_quirk = 1;
+  o->tile_variant = -1;
 }
 
 int fr_create_from_deck(const char *deck_path, const fr_setup_opts *opts, fr_case **out) {
@@ -1040,7 +1327,9 @@ int fr_get_info(fr_case *c, fr_info *info) {
   info->timeType = c->in.timeType;
   info->iter = c->iter;
   info->launches = c->total_launches();
-  info->tensor_kernels = c->useTma ? 2 : (c->useTp ? 1 : 0);
+  info->tensor_kernels = (c->mixed ? c->f32.useTma : c->useTma) ? 2 : (c->useTp ? 1 : 0);
+  info->tile_variant = c->mixed && c->f32.useTma ? c->f32.variant : -1;
+  info->elems_per_block = c->EB;
   if (c->U && !c->hostOnly) {
     if (!c->sync()) return FR_ERR_CUDA;
     cudaMemcpy(&info->time, c->timeAcc, sizeof(double), cudaMemcpyDeviceToHost);
@@ -1088,9 +1377,10 @@ int fr_set_state(fr_case *c, const double *U, size_t count) {
     c->err = "cudaMemcpy H2D failed";
     return FR_ERR_CUDA;
   }
+  if (c->mixed) c->split_state();
   c->extrapolate();
   if (c->in.dtType != 0)  // solver::initializeSolution, solver.cpp:1932-1938
-    frk::launch_wavesp_init(c->nDims, c->nFp, c->E, c->Ufpts, c->norm, c->in.gamma, c->waveSp, c->stream);
+    c->wavesp_init();
   c->stateSet = true;
   return c->cuda_ok("set_state") ? FR_OK : FR_ERR_CUDA;
 }
@@ -1102,6 +1392,7 @@ int fr_get_state(fr_case *c, double *U, size_t count) {
     c->err = "state size mismatch";
     return FR_ERR_ARG;
   }
+  if (c->mixed && c->stateSet) c->join_state();
   return copy_dev(c, c->U, n, U, &count);
 }
 
@@ -1126,6 +1417,7 @@ int fr_get_residual(fr_case *c, int step, double *divF, size_t count) {
   }
   size_t n = (size_t)c->nS * c->E * c->nF;
   if (count != n) return FR_ERR_ARG;
+  if (c->mixed) return copy_dev(c, c->f32.divF[step], n, divF, &count);
   return copy_dev(c, c->divF[step], n, divF, &count);
 }
 
@@ -1209,7 +1501,12 @@ int fr_residual_norm(fr_case *c, int resType, double *out, int nFields) {
     c->err = "host-only case: no device state";
     return FR_ERR_STATE;
   }
-  frk::launch_residual_norm(c->nS, c->E, c->nF, c->divF[0], c->detJ, c->wSpt, resType, c->eleRes, c->stream);
+  if (c->mixed)
+    frk::launch_residual_norm<float>(c->nS, c->E, c->nF, c->f32.divF[0], c->detJ, c->wSpt, resType, c->eleRes,
+                                     c->stream);
+  else
+    frk::launch_residual_norm<double>(c->nS, c->E, c->nF, c->divF[0], c->detJ, c->wSpt, resType, c->eleRes,
+                                      c->stream);
   std::vector<double> er((size_t)c->E * c->nF);
   if (!c->sync()) return FR_ERR_CUDA;
   cudaMemcpy(er.data(), c->eleRes, er.size() * sizeof(double), cudaMemcpyDeviceToHost);
@@ -1235,7 +1532,10 @@ int fr_check_state(fr_case *c) {
     return FR_ERR_STATE;
   }
   cudaMemsetAsync(c->bad, 0, sizeof(unsigned), c->stream);
-  frk::launch_check_state(c->nS, c->E, c->nF, c->U, c->bad, c->stream);
+  if (c->mixed)
+    frk::launch_check_state<float>(c->nS, c->E, c->nF, c->f32.U, c->bad, c->stream);
+  else
+    frk::launch_check_state<double>(c->nS, c->E, c->nF, c->U, c->bad, c->stream);
   unsigned b = 0;
   if (!c->sync()) return FR_ERR_CUDA;
   cudaMemcpy(&b, c->bad, sizeof(unsigned), cudaMemcpyDeviceToHost);
@@ -1255,6 +1555,27 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
                       n == "ele_dt" || n == "F_spts" || n == "disFn_fpts" || n.rfind("divF_", 0) == 0)) {
     c->err = "host-only case: no device state";
     return FR_ERR_STATE;
+  }
+  if (c->mixed) {
+    auto &m = c->f32;
+    if (n == "U_spts") {
+      if (c->stateSet) c->join_state();
+      return copy_dev(c, c->U, nU, host, count);
+    }
+    if (n == "U_comp") return copy_dev(c, m.comp, nU, host, count);
+    if (n == "U0") return copy_dev(c, m.U0, nU, host, count);
+    if (n == "U_fpts") return copy_dev(c, m.Ufpts, nUf, host, count);
+    if (n == "Fn_fpts") return copy_dev(c, m.Fn, nUf, host, count);
+    if (n == "F_spts") return copy_dev(c, m.Fdbg, (size_t)c->nDims * nU, host, count);
+    if (n == "disFn_fpts") return copy_dev(c, m.disFnDbg, nUf, host, count);
+    if (n == "dUc_fpts") return copy_dev(c, m.dUc, nUf, host, count);
+    if (n == "dU_spts") return copy_dev(c, m.dUs, (size_t)c->nDims * nU, host, count);
+    if (n == "dU_fpts") return copy_dev(c, m.dUf, (size_t)c->nDims * nUf, host, count);
+    if (n.rfind("divF_", 0) == 0) {
+      int s = std::atoi(n.c_str() + 5);
+      if (s < 0 || s >= c->nRK) return FR_ERR_ARG;
+      return copy_dev(c, m.divF[s], nU, host, count);
+    }
   }
   if (n == "U_spts") return copy_dev(c, c->U, nU, host, count);
   if (n == "U0") return copy_dev(c, c->U0, nU, host, count);
@@ -1317,6 +1638,28 @@ int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes) {
   size_t nU = (size_t)c->nS * c->E * c->nF, nUf = (size_t)c->nFp * c->E * c->nF;
   void *p = nullptr;
   size_t b = 0;
+  if (c->mixed) {  // the precision form's FP32 working arrays
+    if (n == "U_spts") {
+      p = c->f32.U;
+      b = nU * 4;
+    } else if (n == "U_fpts") {
+      p = c->f32.Ufpts;
+      b = nUf * 4;
+    } else if (n == "Fn_fpts") {
+      p = c->f32.Fn;
+      b = nUf * 4;
+    } else if (n.rfind("divF_", 0) == 0) {
+      int s = std::atoi(n.c_str() + 5);
+      if (s < 0 || s >= c->nRK) return FR_ERR_ARG;
+      p = c->f32.divF[s];
+      b = nU * 4;
+    } else {
+      return FR_ERR_ARG;
+    }
+    *ptr = p;
+    if (bytes) *bytes = b;
+    return FR_OK;
+  }
   if (n == "U_spts") {
     p = c->U;
     b = nU * 8;
@@ -1349,13 +1692,11 @@ int fr_bench_kernel(fr_case *c, const char *kernel, int reps) {
   if (k == "faces") {
     for (int i = 0; i < reps; i++) c->faces_pass();
   } else if (k == "element_stage") {
-    frk::ElemArgs a = c->elem_args();
-    a.mode = c->in.timeType >= 5 ? frk::MODE_JAMESON : frk::MODE_RK_STAGE;
-    a.stage = c->nRK > 1 ? 1 : 0;
-    a.rka_next = c->in.RKa.size() > 2 ? c->in.RKa[2] : 0.0;
-    a.rkb = c->in.RKb.size() > 1 ? c->in.RKb[1] : 0.0;
-    a.Ufpts_out = c->Ufpts;
-    for (int i = 0; i < reps; i++) c->element(a);
+    const int mode = c->in.timeType >= 5 ? frk::MODE_JAMESON : frk::MODE_RK_STAGE;
+    const int stage = c->nRK > 1 ? 1 : 0;
+    const double rka = c->in.RKa.size() > 2 ? c->in.RKa[2] : 0.0;
+    const double rkb = c->in.RKb.size() > 1 ? c->in.RKb[1] : 0.0;
+    for (int i = 0; i < reps; i++) c->element_stage(mode, stage, rka, rkb, false, false);
   } else {
     c->err = "unknown kernel " + k;
     return FR_ERR_ARG;
@@ -1371,8 +1712,8 @@ int fr_batch_create(fr_case *const *cases, int n, fr_batch **out) {
     fr_case *c = cases[i];
     if (!c || c->hostOnly || !c->stateSet) return FR_ERR_STATE;
     if (c->in.viscous || c->in.PMG || c->in.dtType != 0 || c->in.nDims != cases[0]->in.nDims ||
-        c->in.timeType != cases[0]->in.timeType) {
-      return FR_ERR_UNSUPPORTED;  // batches hold inviscid, fixed-dt cases of one RK scheme
+        c->in.timeType != cases[0]->in.timeType || c->opts.precision != cases[0]->opts.precision) {
+      return FR_ERR_UNSUPPORTED;  // batches hold inviscid, fixed-dt cases of one RK scheme and precision
     }
     b->members.push_back(c);
   }
@@ -1444,7 +1785,10 @@ int fr_batch_residual_norms(fr_batch *b, int resType, double *out, int nFields) 
     return FR_ERR_ARG;
   for (size_t gi = 0; gi < b->groups.size(); gi++) {
     fr_case &g = *b->groups[gi];
-    frk::launch_residual_norm(g.nS, g.E, g.nF, g.divF[0], g.detJ, g.wSpt, resType, g.eleRes, g.stream);
+    if (g.mixed)
+      frk::launch_residual_norm<float>(g.nS, g.E, g.nF, g.f32.divF[0], g.detJ, g.wSpt, resType, g.eleRes, g.stream);
+    else
+      frk::launch_residual_norm<double>(g.nS, g.E, g.nF, g.divF[0], g.detJ, g.wSpt, resType, g.eleRes, g.stream);
     std::vector<double> er((size_t)g.E * g.nF);
     if (!g.sync()) return FR_ERR_CUDA;
     cudaMemcpy(er.data(), g.eleRes, er.size() * sizeof(double), cudaMemcpyDeviceToHost);

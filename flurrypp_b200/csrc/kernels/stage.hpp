@@ -1,6 +1,9 @@
-// Launch interface of the per-stage FR kernels (FP64 plain form).
+// Launch interface of the per-stage FR kernels.
 // All arrays are device pointers in the reference layout
-// ([point][element][field], last index fastest).
+// ([point][element][field], last index fastest).  Kernels are templated on
+// the working type R: double for the plain form, float for the precision
+// form (FP32 state, fluxes and operator tables; time step, metrics at setup
+// and the norm reductions stay FP64).
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -24,23 +27,30 @@ struct Csr {
 void launch_apply_op(const Csr &A, const double *in, double *out, long long N, double alpha,
                      double beta, cudaStream_t st);
 
+// The same for data of the working type R (the precision form's state).
+template <typename R>
+void launch_apply_op_t(const Csr &A, const R *in, R *out, long long N, cudaStream_t st);
+
 // Face-point table, one entry per flux point of each face, sorted by left slot.
-struct FaceTable {
+template <typename R>
+struct FaceTableT {
   int n = 0;
   int nInterior = 0;            // interior points first, then boundary points
   const int *slotL = nullptr;   // fpt*E + e of the left side
   const int *slotR = nullptr;   // fpt*E + e of the right side, or -(bc+2) on a boundary
-  const double *nrm = nullptr;  // [n][nDims] left unit normal
-  const double *dAL = nullptr;
-  const double *dAR = nullptr;
+  const R *nrm = nullptr;       // [n][nDims] left unit normal
+  const R *dAL = nullptr;
+  const R *dAR = nullptr;
 };
+using FaceTable = FaceTableT<double>;
 
 // Common inviscid flux on every face point: Fn_fpts at both sides and the
 // left-side wave speed (reference: solver.cpp:752-758, face.cpp:163-208).
 // Interior and boundary points run as two kernels (no BC code in the
-// interior one).
-void launch_faces_inviscid(int nDims, const FaceTable &ft, const double *Ufpts, double *Fn,
-                           double *waveSp, const Phys &ph, cudaStream_t st);
+// interior one).  The wave speed is kept in FP64 for the time step.
+template <typename R>
+void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *Fn, double *waveSp,
+                           const Phys &ph, cudaStream_t st);
 
 enum ElemMode : int {
   MODE_RESIDUAL = 0,  // calcResidual only: divF -> divF_out
@@ -49,12 +59,21 @@ enum ElemMode : int {
   MODE_JAMESON = 3    // Jameson-form stage: U = U0 - RKa[s+1] divF/detJ dt
 };
 
-struct ElemArgs {
+// RK update of one stage.  Plain form (double): `acc` is the running
+// final-stage sum U0 - sum_j RKb_j dt divF_j/detJ, as timeStepB forms it.
+// Precision form (float): `acc` holds only the increments
+// -sum_j RKb_j dt divF_j/detJ, and the state is the pair (U, comp) with U the
+// float nearest the FP64 value and comp the rounding remainder; the final
+// stage adds the increments to that pair by an error-free (TwoSum) addition,
+// so the step-to-step accumulation keeps ~48 bits although every array is
+// FP32 (Kahan-compensated RK sums).
+template <typename R>
+struct ElemArgsT {
   int E = 0, nS = 0, nFp = 0, EB = 1;
-  const double *U = nullptr;       // current stage state [nS][E][nF]
-  const double *JGinv = nullptr;   // [nDims][nS][E][nDims]
-  const double *detJ = nullptr;    // [nS][E]
-  const double *Fn = nullptr;      // common normal flux * dA [nFp][E][nF]
+  const R *U = nullptr;            // current stage state [nS][E][nF]
+  const R *JGinv = nullptr;        // [nDims][nS][E][nDims]
+  const R *detJ = nullptr;         // [nS][E]
+  const R *Fn = nullptr;           // common normal flux * dA [nFp][E][nF]
   Csr grad[3], extFn[3], corr, ext;
   int mode = MODE_RESIDUAL;
   int stage = 0;
@@ -62,22 +81,24 @@ struct ElemArgs {
   double rka_next = 0.0, rkb = 0.0;
   const double *dt = nullptr;      // device scalar
   const double *eleDt = nullptr;   // per-element dt (dtType 2) or null
-  const double *src = nullptr;     // P-multigrid source or null
-  double *U0 = nullptr;            // RK base state (written at stage 0)
-  double *acc = nullptr;           // running final-stage sum
-  double *Uout = nullptr;          // next state
-  double *divF_out = nullptr;      // optional divF of this stage
-  double *Ufpts_out = nullptr;     // optional: next state at flux points
-  double *F_dbg = nullptr;         // optional: F_spts [nDims][nS][E][nF]
-  double *disFn_dbg = nullptr;     // optional: Fn - extrapolated flux [nFp][E][nF]
+  const R *src = nullptr;          // P-multigrid source or null
+  R *U0 = nullptr;                 // RK base state (written at stage 0)
+  R *acc = nullptr;                // running final-stage sum (see above)
+  R *comp = nullptr;               // precision form: rounding remainder of U
+  R *Uout = nullptr;               // next state
+  R *divF_out = nullptr;           // optional divF of this stage
+  R *Ufpts_out = nullptr;          // optional: next state at flux points
+  R *F_dbg = nullptr;              // optional: F_spts [nDims][nS][E][nF]
+  R *disFn_dbg = nullptr;          // optional: Fn - extrapolated flux [nFp][E][nF]
   unsigned int *err = nullptr;     // device status word (bit 0: a bounded wait ran out)
   double gamma = 1.4;
   // viscous stages: physical gradient at the solution points
   // [nDims][nS][E][nF] (stride between dimensions dUsStride), and constants
-  const double *dUs = nullptr;
+  const R *dUs = nullptr;
   long long dUsStride = 0;
   Phys ph{};
 };
+using ElemArgs = ElemArgsT<double>;
 
 size_t elem_smem_bytes(int nDims, int nS, int nFp, int EB);
 void launch_element_stage(int nDims, const ElemArgs &a, cudaStream_t st);
@@ -88,16 +109,18 @@ void launch_element_stage(int nDims, const ElemArgs &a, cudaStream_t st);
 //   ext[f][s]    = E1[side(f)][m] for s on the line of f (normal dim dn(f))
 //   extFn_dn     = (side ? +1 : -1) * ext
 //   corr[s][f]   = corrVal[s][face] at f = corrFpt[s][face], one per face
-struct TpTables {
-  const double *D = nullptr;        // [n][n]
-  const double *E1 = nullptr;       // [2][n]   side 0: xi=-1, side 1: xi=+1
-  const double *EFn1 = nullptr;     // [2][n]   E1 times the reference normal
+template <typename R>
+struct TpTablesT {
+  const R *D = nullptr;             // [n][n]
+  const R *E1 = nullptr;            // [2][n]   side 0: xi=-1, side 1: xi=+1
+  const R *EFn1 = nullptr;          // [2][n]   E1 times the reference normal
   const int *fptBase = nullptr;     // [nFp] first solution point of the line
   const int *fptDn = nullptr;       // [nFp] normal dimension
   const int *fptSide = nullptr;     // [nFp]
   const int *corrFpt = nullptr;     // [nS][2*nDims]
-  const double *corrVal = nullptr;  // [nS][2*nDims]
+  const R *corrVal = nullptr;       // [nS][2*nDims]
 };
+using TpTables = TpTablesT<double>;
 bool tp_supported(int nDims, int order);
 
 // TMA descriptors of the tiles the TMA element kernel moves (one row block of
@@ -110,37 +133,55 @@ struct TmaMaps {
   CUtensorMap Ufpts;  // [nFp][E*nF]   store
   CUtensorMap J;      // [nDims][nS][E*nDims]
   CUtensorMap det;    // [nS][E]
+  CUtensorMap comp;   // [nS][E*nF]    precision form: rounding remainder of U
 };
-int tma_elems_per_block(int nDims, int order);
-size_t tma_smem_bytes(int nDims, int order);
-void launch_element_stage_tma(int nDims, int order, const ElemArgs &a, const TpTables &t,
-                              const TmaMaps &m, cudaStream_t st);
+// Elements per CTA of the TMA kernel for (nDims, order, working type); the
+// precision form has several instantiations (tile shapes) and `variant`
+// picks one of them (0 .. tma_variants()-1), chosen by the autotuner.
+int tma_variants(bool fp32);
+template <typename R>
+int tma_elems_per_block(int nDims, int order, int variant = 0);
+template <typename R>
+size_t tma_smem_bytes(int nDims, int order, int variant = 0);
+template <typename R>
+void launch_element_stage_tma(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
+                              const TmaMaps &m, cudaStream_t st, int variant = 0);
+template <typename R>
 int tp_elems_per_block(int nDims, int order);
-void launch_element_stage_tp(int nDims, int order, const ElemArgs &a, const TpTables &t,
+template <typename R>
+void launch_element_stage_tp(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
                              cudaStream_t st);
 
-// Viscous (LDG) stage pieces (kernels/stage_visc_fp64.cu).
-struct GradArgs {
+// Viscous (LDG) stage pieces (kernels/stage_visc.cu).
+template <typename R>
+struct GradArgsT {
   int E = 0;
-  const double *U = nullptr;      // [nS][E][nF]
-  const double *dUc = nullptr;    // [nFp][E][nF] LDG jumps
-  const double *JGinv = nullptr;
-  const double *detJ = nullptr;
-  double *dUs = nullptr;          // [nDims][nS][E][nF]
-  double *dUf = nullptr;          // [nDims][nFp][E][nF]
+  const R *U = nullptr;      // [nS][E][nF]
+  const R *dUc = nullptr;    // [nFp][E][nF] LDG jumps
+  const R *JGinv = nullptr;
+  const R *detJ = nullptr;
+  R *dUs = nullptr;          // [nDims][nS][E][nF]
+  R *dUf = nullptr;          // [nDims][nFp][E][nF]
   long long sStride = 0, fStride = 0;
 };
-void launch_faces_ldg(int nDims, const FaceTable &ft, const double *Ufpts, double *dUc, const Phys &ph,
+using GradArgs = GradArgsT<double>;
+template <typename R>
+void launch_faces_ldg(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *dUc, const Phys &ph,
                       cudaStream_t st);
-void launch_elem_grad(int nDims, int order, const GradArgs &g, const TpTables &t, cudaStream_t st);
-void launch_faces_visc(int nDims, const FaceTable &ft, const double *Ufpts, const double *dUf, long long fStride,
-                       double *Fn, double *waveSp, const Phys &ph, cudaStream_t st);
+template <typename R>
+void launch_elem_grad(int nDims, int order, const GradArgsT<R> &g, const TpTablesT<R> &t, cudaStream_t st);
+template <typename R>
+void launch_faces_visc(int nDims, const FaceTableT<R> &ft, const R *Ufpts, const R *dUf, long long fStride,
+                       R *Fn, double *waveSp, const Phys &ph, cudaStream_t st);
 // tensor-product element stage with the viscous flux added at the solution points
-void launch_element_stage_tp_visc(int nDims, int order, const ElemArgs &a, const TpTables &t, cudaStream_t st);
+template <typename R>
+void launch_element_stage_tp_visc(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
+                                  cudaStream_t st);
 
 // Wave speed at every flux point from U_fpts (reference: ele.cpp:1076-1125).
-void launch_wavesp_init(int nDims, int nFp, int E, const double *Ufpts, const double *norm,
-                        double gamma, double *waveSp, cudaStream_t st);
+template <typename R>
+void launch_wavesp_init(int nDims, int nFp, int E, const R *Ufpts, const double *norm, double gamma,
+                        double *waveSp, cudaStream_t st);
 
 // Element CFL time step (reference: ele.cpp:1127-1146) and its minimum.
 void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double *detJ,
@@ -156,12 +197,24 @@ void launch_add_time(const double *dt, double *time_acc, cudaStream_t st);
 // P-multigrid cycle (reference: multigrid.cpp:199-205, 282-290, 366-384).
 void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st);
 
-// Per-element residual norm contributions (reference: ele.cpp:1922-1944).
-void launch_residual_norm(int nS, int E, int nF, const double *divF, const double *detJ,
+// Per-element residual norm contributions (reference: ele.cpp:1922-1944),
+// accumulated in FP64 whatever the type of divF.
+template <typename R>
+void launch_residual_norm(int nS, int E, int nF, const R *divF, const double *detJ,
                           const double *wSpt, int resType, double *eleRes, cudaStream_t st);
 
 // Device health: counts non-finite or non-positive density entries in U.
-void launch_check_state(int nS, int E, int nF, const double *U, unsigned int *bad,
-                        cudaStream_t st);
+template <typename R>
+void launch_check_state(int nS, int E, int nF, const R *U, unsigned int *bad, cudaStream_t st);
+
+// Precision-form conversions at the boundary and at setup:
+//   split   : U64 -> (U32 = fl32(U64), comp = fl32(U64 - U32))
+//   join    : (U32, comp) -> U64 = U32 + comp
+//   narrow  : FP64 -> FP32 (metrics, normals, face areas)
+//   widen   : FP32 -> FP64 (residuals, traces read back by tools)
+void launch_split(long long n, const double *U64, float *U32, float *comp, cudaStream_t st);
+void launch_join(long long n, const float *U32, const float *comp, double *U64, cudaStream_t st);
+void launch_narrow(long long n, const double *in, float *out, cudaStream_t st);
+void launch_widen(long long n, const float *in, double *out, cudaStream_t st);
 
 }  // namespace frk

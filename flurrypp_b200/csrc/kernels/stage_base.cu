@@ -1,4 +1,5 @@
-// FP64 plain-form stage kernels for sm_100a.
+// Stage kernels for sm_100a: faces, the general sparse-operator element
+// kernel (FP64), time step, norms and the precision form's conversions.
 //
 // One RK stage is two kernels:
 //   faces   : common flux Fn at every face point, gathered from U_fpts through
@@ -35,20 +36,18 @@ __global__ void k_apply_op(int nRows, const int *__restrict__ rp, const int *__r
 
 // Interior face points: Rusanov (or 2-D Roe) on the left normal, written to
 // both sides (reference: face.cpp:163-208, intFace.cpp:147-154).
-template <int ND>
+template <int ND, typename R>
 __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__restrict__ slotL,
-                                                        const int *__restrict__ slotR,
-                                                        const double *__restrict__ nrm,
-                                                        const double *__restrict__ dAL,
-                                                        const double *__restrict__ dAR,
-                                                        const double *__restrict__ Uf, double *__restrict__ Fn,
-                                                        double *__restrict__ waveSp, double gam, int roe) {
+                                                        const int *__restrict__ slotR, const R *__restrict__ nrm,
+                                                        const R *__restrict__ dAL, const R *__restrict__ dAR,
+                                                        const R *__restrict__ Uf, R *__restrict__ Fn,
+                                                        double *__restrict__ waveSp, R gam, int roe) {
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int sL = slotL[i];
   const int sR = slotR[i];
-  double UL[NF], UR[NF], nv[ND], F[NF];
+  R UL[NF], UR[NF], nv[ND], F[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
 #pragma unroll
@@ -56,11 +55,11 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
 #pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
   if (ND == 2 && roe) {
-    roe2d<double>(UL, UR, nv, gam, F);
+    roe2d<R>(UL, UR, nv, gam, F);
   } else {
-    waveSp[sL] = rusanov<ND, double>(UL, UR, nv, gam, F);
+    waveSp[sL] = rusanov<ND, R>(UL, UR, nv, gam, F);
   }
-  const double aL = dAL[i], aR = dAR[i];
+  const R aL = dAL[i], aR = dAR[i];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
     Fn[(long long)sL * NF + k] = F[k] * aL;
@@ -70,24 +69,23 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
 
 // Boundary face points: ghost state from the BC, then Rusanov (boundaries
 // always use Rusanov, face.cpp:174-176; ghost states boundFace.cpp:65-314).
-template <int ND>
+template <int ND, typename R>
 __global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
-                                 const double *__restrict__ nrm, const double *__restrict__ dAL,
-                                 const double *__restrict__ Uf, double *__restrict__ Fn,
-                                 double *__restrict__ waveSp, Phys ph) {
+                                 const R *__restrict__ nrm, const R *__restrict__ dAL, const R *__restrict__ Uf,
+                                 R *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
   constexpr int NF = ND + 2;
   int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int sL = slotL[i];
   const int bc = -slotR[i] - 2;
-  double UL[NF], UR[NF], nv[ND], F[NF];
+  R UL[NF], UR[NF], nv[ND], F[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
 #pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
-  boundary_state<ND, double>(bc, UL, nv, ph, UR);
-  waveSp[sL] = rusanov<ND, double>(UL, UR, nv, ph.gamma, F);
-  const double aL = dAL[i];
+  boundary_state<ND, R>(bc, UL, nv, ph, UR);
+  waveSp[sL] = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  const R aL = dAL[i];
 #pragma unroll
   for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
 }
@@ -233,14 +231,14 @@ __global__ void __launch_bounds__(256) k_element_stage(ElemArgs a) {
   }
 }
 
-template <int ND>
-__global__ void k_wavesp_init(int nFp, int E, const double *__restrict__ Uf,
-                              const double *__restrict__ norm, double gam,
+// FP64 arithmetic for either state type (the time step stays FP64)
+template <int ND, typename R>
+__global__ void k_wavesp_init(int nFp, int E, const R *__restrict__ Uf, const double *__restrict__ norm, double gam,
                               double *__restrict__ waveSp) {
   constexpr int NF = ND + 2;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)nFp * E) return;
-  const double *U = &Uf[i * NF];
+  const R *U = &Uf[i * NF];
   const double *n = &norm[i * ND];
   double rho = U[0];
   double u = U[1] / rho;
@@ -284,9 +282,9 @@ __global__ void k_store_min(const unsigned long long *bits, double *dt, double *
 
 __global__ void k_add_time(const double *dt, double *time_acc) { *time_acc += *dt; }
 
-__global__ void k_residual_norm(int nS, int E, int nF, const double *__restrict__ divF,
-                                const double *__restrict__ detJ, const double *__restrict__ w,
-                                int resType, double *__restrict__ eleRes) {
+template <typename R>
+__global__ void k_residual_norm(int nS, int E, int nF, const R *__restrict__ divF, const double *__restrict__ detJ,
+                                const double *__restrict__ w, int resType, double *__restrict__ eleRes) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
   for (int k = 0; k < nF; k++) {
@@ -311,13 +309,52 @@ __global__ void k_add(long long n, double *__restrict__ out, const double *__res
   out[i] = sgn > 0 ? x[i] + y[i] : x[i] - y[i];
 }
 
-__global__ void k_check_state(long long n, int nF, const double *__restrict__ U, unsigned int *bad) {
+template <typename R>
+__global__ void k_check_state(long long n, int nF, const R *__restrict__ U, unsigned int *bad) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double v = U[i];
+  R v = U[i];
   bool b = !(v == v) || isinf(v);
-  if ((i % nF) == 0 && !(v > 0.0)) b = true;
+  if ((i % nF) == 0 && !(v > R(0))) b = true;
   if (b) atomicAdd(bad, 1u);
+}
+
+template <typename R>
+__global__ void k_apply_op_t(int nRows, const int *__restrict__ rp, const int *__restrict__ ci,
+                             const double *__restrict__ v, const R *__restrict__ in, R *__restrict__ out, long long N) {
+  long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (n >= N || r >= nRows) return;
+  R s = R(0);
+  for (int j = rp[r]; j < rp[r + 1]; j++) s += R(v[j]) * in[(long long)ci[j] * N + n];
+  out[(long long)r * N + n] = s;
+}
+
+__global__ void k_split(long long n, const double *__restrict__ U64, float *__restrict__ U32,
+                        float *__restrict__ comp) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double u = U64[i];
+  const float hi = __double2float_rn(u);
+  U32[i] = hi;
+  comp[i] = __double2float_rn(u - (double)hi);
+}
+
+__global__ void k_join(long long n, const float *__restrict__ U32, const float *__restrict__ comp,
+                       double *__restrict__ U64) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  U64[i] = (double)U32[i] + (double)comp[i];
+}
+
+__global__ void k_narrow(long long n, const double *__restrict__ in, float *__restrict__ out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __double2float_rn(in[i]);
+}
+
+__global__ void k_widen(long long n, const float *__restrict__ in, double *__restrict__ out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)in[i];
 }
 
 }  // namespace
@@ -329,25 +366,33 @@ void launch_apply_op(const Csr &A, const double *in, double *out, long long N, d
   k_apply_op<<<g, 256, 0, st>>>(A.nRows, A.rowptr, A.col, A.val, in, out, N, alpha, beta);
 }
 
-void launch_faces_inviscid(int nDims, const FaceTable &ft, const double *Ufpts, double *Fn,
-                           double *waveSp, const Phys &ph, cudaStream_t st) {
+template <typename R>
+void launch_apply_op_t(const Csr &A, const R *in, R *out, long long N, cudaStream_t st) {
+  if (N <= 0 || A.nRows <= 0) return;
+  dim3 g((unsigned)((N + 255) / 256), (unsigned)A.nRows);
+  k_apply_op_t<R><<<g, 256, 0, st>>>(A.nRows, A.rowptr, A.col, A.val, in, out, N);
+}
+
+template <typename R>
+void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *Fn, double *waveSp,
+                           const Phys &ph, cudaStream_t st) {
   const int b = 256;
   const int nI = ft.nInterior, nB = ft.n - ft.nInterior;
   if (nI > 0) {
     const int g = (nI + b - 1) / b;
     if (nDims == 2)
-      k_faces_interior<2><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
-                                           ph.gamma, ph.riemannType == 1);
+      k_faces_interior<2, R><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
+                                              R(ph.gamma), ph.riemannType == 1);
     else
-      k_faces_interior<3><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
-                                           ph.gamma, 0);
+      k_faces_interior<3, R><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
+                                              R(ph.gamma), 0);
   }
   if (nB > 0) {
     const int g = (nB + b - 1) / b;
     if (nDims == 2)
-      k_faces_boundary<2><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
+      k_faces_boundary<2, R><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
     else
-      k_faces_boundary<3><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
+      k_faces_boundary<3, R><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
   }
 }
 
@@ -369,15 +414,16 @@ void launch_element_stage(int nDims, const ElemArgs &a, cudaStream_t st) {
   }
 }
 
-void launch_wavesp_init(int nDims, int nFp, int E, const double *Ufpts, const double *norm,
-                        double gamma, double *waveSp, cudaStream_t st) {
+template <typename R>
+void launch_wavesp_init(int nDims, int nFp, int E, const R *Ufpts, const double *norm, double gamma,
+                        double *waveSp, cudaStream_t st) {
   long long n = (long long)nFp * E;
   if (n <= 0) return;
   unsigned g = (unsigned)((n + 255) / 256);
   if (nDims == 2)
-    k_wavesp_init<2><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
+    k_wavesp_init<2, R><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
   else
-    k_wavesp_init<3><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
+    k_wavesp_init<3, R><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
 }
 
 void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double *detJ,
@@ -400,10 +446,11 @@ void launch_add_time(const double *dt, double *time_acc, cudaStream_t st) {
   k_add_time<<<1, 1, 0, st>>>(dt, time_acc);
 }
 
-void launch_residual_norm(int nS, int E, int nF, const double *divF, const double *detJ,
-                          const double *wSpt, int resType, double *eleRes, cudaStream_t st) {
+template <typename R>
+void launch_residual_norm(int nS, int E, int nF, const R *divF, const double *detJ, const double *wSpt,
+                          int resType, double *eleRes, cudaStream_t st) {
   if (E <= 0) return;
-  k_residual_norm<<<(E + 127) / 128, 128, 0, st>>>(nS, E, nF, divF, detJ, wSpt, resType, eleRes);
+  k_residual_norm<R><<<(E + 127) / 128, 128, 0, st>>>(nS, E, nF, divF, detJ, wSpt, resType, eleRes);
 }
 
 void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st) {
@@ -411,10 +458,36 @@ void launch_add(long long n, double *out, const double *x, const double *y, doub
   k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, out, x, y, sgn);
 }
 
-void launch_check_state(int nS, int E, int nF, const double *U, unsigned int *bad, cudaStream_t st) {
+template <typename R>
+void launch_check_state(int nS, int E, int nF, const R *U, unsigned int *bad, cudaStream_t st) {
   long long n = (long long)nS * E * nF;
   if (n <= 0) return;
-  k_check_state<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nF, U, bad);
+  k_check_state<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nF, U, bad);
 }
+
+void launch_split(long long n, const double *U64, float *U32, float *comp, cudaStream_t st) {
+  if (n > 0) k_split<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, U64, U32, comp);
+}
+void launch_join(long long n, const float *U32, const float *comp, double *U64, cudaStream_t st) {
+  if (n > 0) k_join<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, U32, comp, U64);
+}
+void launch_narrow(long long n, const double *in, float *out, cudaStream_t st) {
+  if (n > 0) k_narrow<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, in, out);
+}
+void launch_widen(long long n, const float *in, double *out, cudaStream_t st) {
+  if (n > 0) k_widen<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, in, out);
+}
+
+#define FR_BASE_INST(R)                                                                                        \
+  template void launch_apply_op_t<R>(const Csr &, const R *, R *, long long, cudaStream_t);                   \
+  template void launch_faces_inviscid<R>(int, const FaceTableT<R> &, const R *, R *, double *, const Phys &,  \
+                                         cudaStream_t);                                                       \
+  template void launch_wavesp_init<R>(int, int, int, const R *, const double *, double, double *, cudaStream_t); \
+  template void launch_residual_norm<R>(int, int, int, const R *, const double *, const double *, int, double *, \
+                                        cudaStream_t);                                                        \
+  template void launch_check_state<R>(int, int, int, const R *, unsigned int *, cudaStream_t);
+FR_BASE_INST(double)
+FR_BASE_INST(float)
+#undef FR_BASE_INST
 
 }  // namespace frk

@@ -1,0 +1,451 @@
+// Tensor-product element kernel with TMA tile transfers, FP64 plain form and
+// FP32 precision form.
+//
+// The same stage as k_elem_tp (reference: solver.cpp:470-572, 707-736,
+// 906-1058), but each CTA fetches all of its input tiles with
+// cp.async.bulk.tensor loads completing on two mbarriers (state U and the
+// metrics JGinv first; then the common flux Fn, the RK base U0, the running
+// sum acc, detJ and, precision form, the state's rounding remainder comp), and
+// writes U, acc, U0, comp and U_fpts back with cp.async.bulk.tensor stores.
+// A tile is one operator row block [points][EB elements x fields], which is
+// contiguous in the reference layout, so every transfer is one TMA
+// instruction.
+//
+// Requirements (checked on the host): every x offset and row pitch a
+// multiple of 16 bytes, i.e. for FP64 E and EB even, for FP32 E and EB
+// multiples of 4.
+#include <type_traits>
+
+#include "stage.hpp"
+#include "tma.cuh"
+
+namespace frk {
+
+namespace {
+
+constexpr int ipow2(int b, int e) { return e == 0 ? 1 : b * ipow2(b, e - 1); }
+constexpr int pow2_floor(int x) { return x >= 2 ? 2 * pow2_floor(x / 2) : 1; }
+
+constexpr int kFp32Variants = 3;
+constexpr size_t kMaxSmem = 227 * 1024;
+
+template <int ND, int P, typename R, int V>
+struct Tm {
+  static constexpr bool F32 = std::is_same<R, float>::value;
+  static constexpr int N = P + 1;
+  static constexpr int NF = ND + 2;
+  static constexpr int NS = ipow2(N, ND);
+  static constexpr int NPF = ipow2(N, ND - 1);
+  static constexpr int NFP = 2 * ND * NPF;
+  // in elements of R; every tile starts on 128 bytes
+  static constexpr int AL = 128 / (int)sizeof(R);
+  static constexpr int al(int n) { return (n + AL - 1) / AL * AL; }
+  static constexpr size_t smem_for(int eb) {
+    // U, U0, acc, comp tiles; Fn; J; det; F; tables; indices; barriers
+    return sizeof(R) * (size_t)(4 * al(NS * eb * NF) + al(NFP * eb * NF) + al(ND * NS * eb * ND) + al(NS * eb) +
+                                al(ND * NS * eb * NF) + al(N * N + 4 * N) + al(NS * 2 * ND) +
+                                al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1) + AL) +
+           128;
+  }
+  static constexpr bool fits(int eb) { return NS * eb <= 1024 && smem_for(eb) <= kMaxSmem && eb * NF <= 256; }
+  // FP64: largest power of two <= 32 with NS*EB <= 160, at least 2.
+  // FP32: 128/NS rounded down to a power of two, at least 4 (16-byte
+  // offsets), times 2^V, at most 32, halved until it fits.
+  static constexpr int eb64() {
+    return NS * 32 <= 160 ? 32 : NS * 16 <= 160 ? 16 : NS * 8 <= 160 ? 8 : NS * 4 <= 160 ? 4 : 2;
+  }
+  static constexpr int eb32_want() {
+    return (pow2_floor(128 / NS) < 4 ? 4 : pow2_floor(128 / NS)) << V > 32
+               ? 32
+               : (pow2_floor(128 / NS) < 4 ? 4 : pow2_floor(128 / NS)) << V;
+  }
+  static constexpr int shrink(int eb) { return (eb <= 4 || fits(eb)) ? eb : shrink(eb / 2); }
+  static constexpr int EB = F32 ? shrink(eb32_want()) : eb64();
+  static constexpr int NT = NS * EB;
+  static constexpr int ROW = EB * NF;
+  static constexpr int O_U = 0;
+  static constexpr int O_U0 = O_U + al(NS * ROW);
+  static constexpr int O_ACC = O_U0 + al(NS * ROW);
+  static constexpr int O_CMP = O_ACC + al(NS * ROW);
+  static constexpr int O_FN = O_CMP + (F32 ? al(NS * ROW) : 0);
+  static constexpr int O_J = O_FN + al(NFP * ROW);
+  static constexpr int O_DET = O_J + al(ND * NS * EB * ND);
+  static constexpr int O_F = O_DET + al(NS * EB);
+  static constexpr int O_TAB = O_F + al(ND * NS * ROW);
+  static constexpr int O_CV = O_TAB + al(N * N + 4 * N);     // corrVal [NS][2ND]
+  static constexpr int O_IDX = O_CV + al(NS * 2 * ND);        // ints: fpt line [NFP], corrFpt [NS][2ND]
+  static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1);
+  static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
+  static_assert(SMEM <= kMaxSmem, "TMA tile set does not fit in shared memory");
+  static_assert(NT <= 1024, "too many threads");
+  static_assert(!F32 || EB % 4 == 0, "FP32 tiles need 16-byte x offsets");
+};
+
+// s + e = a + b exactly (Knuth's TwoSum); the intrinsics keep the compiler
+// from contracting or reassociating the steps.
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+template <int ND, int P, typename R, int V>
+__global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a, TpTablesT<R> t,
+                                                                  const __grid_constant__ TmaMaps mp) {
+  using T = Tm<ND, P, R, V>;
+  constexpr bool F32 = T::F32;
+  constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  extern __shared__ __align__(128) unsigned char smem_bytes[];
+  // tiles start on 128-byte boundaries relative to an aligned base
+  R *smem = reinterpret_cast<R *>((reinterpret_cast<uintptr_t>(smem_bytes) + 127) & ~uintptr_t(127));
+  R *sU = smem + T::O_U;
+  R *sU0 = smem + T::O_U0;
+  R *sAcc = smem + T::O_ACC;
+  R *sCmp = smem + T::O_CMP;  // precision form only
+  R *sFn = smem + T::O_FN;    // Fn -> Fn - extrapolated flux -> new U_fpts
+  R *sJ = smem + T::O_J;      // [ND][NS][EB*ND]
+  R *sDet = smem + T::O_DET;  // [NS][EB]
+  R *sF = smem + T::O_F;      // [ND][NS][ROW]
+  R *sD = smem + T::O_TAB;
+  R *sE = sD + N * N;
+  R *sEF = sE + 2 * N;
+  R *sCV = smem + T::O_CV;
+  int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);  // base | dn << 16 | side << 20
+  int *sCF = sLine + NFP;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::O_BAR);
+
+  const int E = a.E;
+  const int e0 = blockIdx.x * EB;
+  const int nValid = min(EB, E - e0);
+  const int tid = threadIdx.x;
+  const int s = tid / EB, el = tid - (tid / EB) * EB;
+  const int e = e0 + el;
+  const bool valid = el < nValid;
+
+  // the last stage of the step: the precision form adds the increments to
+  // the compensated state there
+  const bool finalStage = a.mode == MODE_RK_FINAL || (a.mode == MODE_JAMESON && a.stage == a.nRK - 1);
+  const bool needU0 = ((a.mode == MODE_RK_STAGE || a.mode == MODE_JAMESON) && a.stage > 0) ||
+                      (F32 && a.mode == MODE_RK_FINAL && a.nRK > 1);
+  const bool needAcc = (a.mode == MODE_RK_STAGE && a.stage > 0) || (a.mode == MODE_RK_FINAL && a.nRK > 1);
+  const bool needCmp = F32 && finalStage;
+  const bool needDet = a.mode != MODE_RESIDUAL;
+
+  // two transaction barriers: bar[0] for what the flux needs (U, JGinv),
+  // bar[1] for what the correction and update need, so the second batch
+  // lands while the flux and divergence are computed
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar[0], sizeof(R) * (NS * ROW + ND * NS * EB * ND));
+    tma_load_2d(sU, &mp.U, e0 * NF, 0, &bar[0]);
+    tma_load_3d(sJ, &mp.J, e0 * ND, 0, 0, &bar[0]);
+    uint32_t bytes = sizeof(R) * NFP * ROW;
+    if (needU0) bytes += sizeof(R) * NS * ROW;
+    if (needAcc) bytes += sizeof(R) * NS * ROW;
+    if (needCmp) bytes += sizeof(R) * NS * ROW;
+    if (needDet) bytes += sizeof(R) * NS * EB;
+    mbar_arrive_expect_tx(&bar[1], bytes);
+    tma_load_2d(sFn, &mp.Fn, e0 * NF, 0, &bar[1]);
+    if (needU0) tma_load_2d(sU0, &mp.U0, e0 * NF, 0, &bar[1]);
+    if (needAcc) tma_load_2d(sAcc, &mp.acc, e0 * NF, 0, &bar[1]);
+    if (needCmp) tma_load_2d(sCmp, &mp.comp, e0 * NF, 0, &bar[1]);
+    if (needDet) tma_load_2d(sDet, &mp.det, e0, 0, &bar[1]);
+  }
+  for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
+  for (int i = tid; i < 2 * N; i += NT) {
+    sE[i] = t.E1[i];
+    sEF[i] = t.EFn1[i];
+  }
+  for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
+  for (int i = tid; i < NS * 2 * ND; i += NT) {
+    sCF[i] = t.corrFpt[i];
+    sCV[i] = t.corrVal[i];
+  }
+  if (!mbar_wait_bounded(&bar[0], 0, 1u << 22)) {
+    // give up: flag it, let the copies in flight land (bounded), leave
+    if (a.err) atomicOr(a.err, 1);
+    mbar_wait_bounded(&bar[0], 0, 1u << 22);
+    mbar_wait_bounded(&bar[1], 0, 1u << 22);
+    return;
+  }
+  __syncthreads();  // tables
+
+  // stage 0: the RK base state is the state at the start of the step
+  if ((a.mode == MODE_RK_STAGE || a.mode == MODE_JAMESON) && a.stage == 0 && tid == 0) {
+    tma_store_2d(&mp.U0, e0 * NF, 0, sU);
+    tma_commit();
+  }
+
+  // B: reference-space flux at (s, el)
+  {
+    R Fp[ND][NF];
+    const R *u = &sU[s * ROW + el * NF];
+    if (valid) {
+      inviscid_flux<ND, R>(u, Fp, R(a.gamma));
+    } else {
+#pragma unroll
+      for (int d = 0; d < ND; d++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) Fp[d][k] = R(0);
+    }
+#pragma unroll
+    for (int d1 = 0; d1 < ND; d1++) {
+      const R *Jr = &sJ[(d1 * NS + s) * EB * ND + el * ND];
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        R f = R(0);
+#pragma unroll
+        for (int d2 = 0; d2 < ND; d2++) f += Jr[d2] * Fp[d2][k];
+        sF[(d1 * NS + s) * ROW + el * NF + k] = f;
+        if (a.F_dbg && valid) a.F_dbg[(((long long)d1 * NS + s) * E + e) * NF + k] = f;
+      }
+    }
+  }
+  __syncthreads();
+
+  // C1: flux divergence at (s, el)
+  int idx3[3];
+  idx3[0] = s % N;
+  idx3[1] = ND > 1 ? (s / N) % N : 0;
+  idx3[2] = ND > 2 ? s / (N * N) : 0;
+  R div[NF];
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
+    const int base = s - idx3[d] * stride;
+    const R *Dr = &sD[idx3[d] * N];
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R dv = Dr[m];
+      const R *x = &sF[(d * NS + base + m * stride) * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) div[k] = d == 0 ? acc[k] : div[k] + acc[k];
+  }
+
+  if (!mbar_wait_bounded(&bar[1], 0, 1u << 22)) {
+    if (a.err) atomicOr(a.err, 1);
+    mbar_wait_bounded(&bar[1], 0, 1u << 22);
+    if (tid == 0) tma_wait_read_all();
+    return;
+  }
+
+  // C2: Fn - extrapolated normal flux, in place in the Fn tile
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    const int ln = sLine[f];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R ev = sEF[side * N + m];
+      const R *x = &sF[(dn * NS + base + m * stride) * ROW + fe * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+    }
+    R *q = &sFn[f * ROW + fe * NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      q[k] = q[k] - acc[k];
+      if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = q[k];
+    }
+  }
+  if (tid == 0) tma_wait_read_all();  // the U0 store has read sU
+  __syncthreads();
+
+  // D: correction and RK update at (s, el), in place in sU / sAcc / sCmp
+  {
+    R cq[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) cq[k] = R(0);
+#pragma unroll
+    for (int fc = 0; fc < 2 * ND; fc++) {
+      const int fp = sCF[s * 2 * ND + fc];
+      const R cv = sCV[s * 2 * ND + fc];
+      const R *x = &sFn[fp * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
+    }
+    // one reciprocal per point instead of a division per update term
+    const R rdJ = needDet ? R(1.0) / sDet[s * EB + el] : R(1.0);
+    const R dt = R(a.mode == MODE_RESIDUAL ? 0.0 : (a.eleDt ? (valid ? a.eleDt[e] : 0.0) : *a.dt));
+    const R rka = R(a.rka_next), rkb = R(a.rkb);
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const int li = s * ROW + el * NF + k;
+      const long long gi = ((long long)s * E + e) * NF + k;
+      R dv = cq[k] + div[k];
+      if (a.divF_out && valid) a.divF_out[gi] = dv;
+      if (a.mode == MODE_RESIDUAL) continue;
+      if (a.src && valid) dv = dv + a.src[gi];
+      const R u = sU[li];
+      R unew;
+      if constexpr (!F32) {
+        if (a.mode == MODE_RK_STAGE) {
+          const R u0 = a.stage == 0 ? u : sU0[li];
+          unew = u0 - rka * dv * rdJ * dt;
+          const R base = a.stage == 0 ? u0 : sAcc[li];
+          sAcc[li] = base - rkb * dv * rdJ * dt;
+        } else if (a.mode == MODE_RK_FINAL) {
+          const R base = a.nRK == 1 ? u : sAcc[li];
+          unew = base - rkb * dv * rdJ * dt;
+        } else {
+          const R u0 = a.stage == 0 ? u : sU0[li];
+          unew = u0 - rka * dv * rdJ * dt;
+        }
+      } else {
+        const R inc = dv * rdJ * dt;
+        if (a.mode == MODE_RK_STAGE) {
+          const R u0 = a.stage == 0 ? u : sU0[li];
+          unew = u0 - rka * inc;
+          sAcc[li] = (a.stage == 0 ? R(0) : sAcc[li]) - rkb * inc;
+        } else if (finalStage) {
+          const R u0 = (a.mode == MODE_RK_FINAL && a.nRK > 1) || (a.mode == MODE_JAMESON && a.stage > 0) ? sU0[li] : u;
+          const R sum = a.mode == MODE_RK_FINAL ? (a.nRK > 1 ? sAcc[li] : R(0)) - rkb * inc : -(rka * inc);
+          R c;
+          two_sum(u0, sCmp[li] + sum, unew, c);
+          sCmp[li] = c;
+        } else {
+          const R u0 = a.stage == 0 ? u : sU0[li];
+          unew = u0 - rka * inc;
+        }
+      }
+      sU[li] = unew;
+    }
+  }
+  if (a.mode == MODE_RESIDUAL) return;
+  fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_2d(&mp.U, e0 * NF, 0, sU);
+    if (a.mode == MODE_RK_STAGE) tma_store_2d(&mp.acc, e0 * NF, 0, sAcc);
+    if (needCmp) tma_store_2d(&mp.comp, e0 * NF, 0, sCmp);
+    tma_commit();
+  }
+  if (!a.Ufpts_out) {
+    if (tid == 0) tma_wait_read_all();
+    return;
+  }
+
+  // E: new state at the flux points, into the Fn tile
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    const int ln = sLine[f];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R ev = sE[side * N + m];
+      const R *x = &sU[(base + m * stride) * ROW + fe * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+    }
+    R *o = &sFn[f * ROW + fe * NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) o[k] = acc[k];
+  }
+  fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_2d(&mp.Ufpts, e0 * NF, 0, sFn);
+    tma_commit();
+    tma_wait_read_all();
+  }
+}
+
+template <int ND, int P, typename R, int V>
+void launch_tma(const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m, cudaStream_t st) {
+  using T = Tm<ND, P, R, V>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_elem_tma<ND, P, R, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    attr = true;
+  }
+  int g = (a.E + T::EB - 1) / T::EB;
+  k_elem_tma<ND, P, R, V><<<g, T::NT, T::SMEM, st>>>(a, t, m);
+}
+
+// (nDims, order) -> compile-time case; variants only for the precision form
+#define FR_TM_ORDERS(X) X(2, 0) X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 5) X(3, 0) X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 5)
+
+template <typename R, int V>
+int eb_of(int nDims, int order) {
+#define FR_TM_EB(ND, P) \
+  if (nDims == ND && order == P) return Tm<ND, P, R, V>::EB;
+  FR_TM_ORDERS(FR_TM_EB)
+#undef FR_TM_EB
+  return 0;
+}
+template <typename R, int V>
+size_t smem_of(int nDims, int order) {
+#define FR_TM_SM(ND, P) \
+  if (nDims == ND && order == P) return Tm<ND, P, R, V>::SMEM;
+  FR_TM_ORDERS(FR_TM_SM)
+#undef FR_TM_SM
+  return 0;
+}
+template <typename R, int V>
+void launch_v(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m,
+              cudaStream_t st) {
+#define FR_TM_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_tma<ND, P, R, V>(a, t, m, st);
+  FR_TM_ORDERS(FR_TM_CASE)
+#undef FR_TM_CASE
+}
+
+}  // namespace
+
+int tma_variants(bool fp32) { return fp32 ? kFp32Variants : 1; }
+
+template <>
+int tma_elems_per_block<double>(int nDims, int order, int) {
+  return eb_of<double, 0>(nDims, order);
+}
+template <>
+int tma_elems_per_block<float>(int nDims, int order, int v) {
+  return v == 0 ? eb_of<float, 0>(nDims, order) : v == 1 ? eb_of<float, 1>(nDims, order) : eb_of<float, 2>(nDims, order);
+}
+template <>
+size_t tma_smem_bytes<double>(int nDims, int order, int) {
+  return smem_of<double, 0>(nDims, order);
+}
+template <>
+size_t tma_smem_bytes<float>(int nDims, int order, int v) {
+  return v == 0 ? smem_of<float, 0>(nDims, order) : v == 1 ? smem_of<float, 1>(nDims, order) : smem_of<float, 2>(nDims, order);
+}
+
+template <>
+void launch_element_stage_tma<double>(int nDims, int order, const ElemArgsT<double> &a, const TpTablesT<double> &t,
+                                      const TmaMaps &m, cudaStream_t st, int) {
+  if (a.E <= 0) return;
+  launch_v<double, 0>(nDims, order, a, t, m, st);
+}
+template <>
+void launch_element_stage_tma<float>(int nDims, int order, const ElemArgsT<float> &a, const TpTablesT<float> &t,
+                                     const TmaMaps &m, cudaStream_t st, int v) {
+  if (a.E <= 0) return;
+  if (v == 0)
+    launch_v<float, 0>(nDims, order, a, t, m, st);
+  else if (v == 1)
+    launch_v<float, 1>(nDims, order, a, t, m, st);
+  else
+    launch_v<float, 2>(nDims, order, a, t, m, st);
+}
+
+}  // namespace frk

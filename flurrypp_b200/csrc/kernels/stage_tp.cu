@@ -1,0 +1,319 @@
+// Tensor-product element kernel (quads and hexes, orders 0..5), FP64 plain
+// form and FP32 precision form.
+//
+// Same stage as k_element_stage (flux at the solution points, divergence,
+// extrapolated normal flux, correction, RK update, extrapolation of the new
+// state to the flux points; reference: solver.cpp:470-572, 707-736,
+// 906-1058), with compile-time sizes: one thread per (solution point,
+// element), all fields in registers, the 1-D operator tables in shared
+// memory.  Every sum is the one the dense operator would form, over its
+// nonzero terms in ascending column order.
+#include <type_traits>
+
+#include "stage.hpp"
+
+namespace frk {
+
+namespace {
+
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+template <int ND, int P, typename R = double>
+struct Tp {
+  static constexpr int N = P + 1;
+  static constexpr int NF = ND + 2;
+  static constexpr int NS = ipow(N, ND);
+  static constexpr int NPF = ipow(N, ND - 1);
+  static constexpr int NFP = 2 * ND * NPF;
+  static constexpr int EB = NS >= 256 ? 1 : (NS * 2 > 256 ? 1 : (NS * 4 > 256 ? 2 : (NS * 8 > 256 ? 4 : (NS * 16 > 256 ? 8 : (NS * 32 > 256 ? 16 : 32)))));
+  static constexpr int NT = NS * EB;
+  static constexpr int ROW = EB * NF;  // values per point row of a tile
+  static constexpr size_t SMEM = sizeof(R) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 4 * N);
+};
+
+// s + e = a + b exactly (TwoSum), not contracted or reassociated
+__device__ __forceinline__ void two_sum_tp(float a, float b, float &s, float &e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+template <int ND, int P, bool VISC, typename R>
+__global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, TpTablesT<R> t) {
+  using T = Tp<ND, P, R>;
+  constexpr bool F32 = std::is_same<R, float>::value;
+  constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  R *smem = reinterpret_cast<R *>(smem_bytes);
+  R *sU = smem;                 // [NS][EB][NF]
+  R *sF = sU + NS * ROW;        // [ND][NS][EB][NF]
+  R *sQ = sF + ND * NS * ROW;   // [NFP][EB][NF]
+  R *sD = sQ + NFP * ROW;       // [N][N]
+  R *sE = sD + N * N;           // [2][N]
+  R *sEF = sE + 2 * N;          // [2][N]
+
+  const int E = a.E;
+  const int e0 = blockIdx.x * EB;
+  const int nValid = min(EB, E - e0);
+  const int tid = threadIdx.x;
+  const int s = tid / EB, el = tid - (tid / EB) * EB;
+  const int e = e0 + el;
+  const bool valid = el < nValid;
+
+  for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
+  for (int i = tid; i < 2 * N; i += NT) {
+    sE[i] = t.E1[i];
+    sEF[i] = t.EFn1[i];
+  }
+  // A: state tile, coalesced along (element, field)
+  for (int idx = tid; idx < NS * ROW; idx += NT) {
+    const int ss = idx / ROW, r = idx - ss * ROW;
+    sU[idx] = (r < nValid * NF) ? a.U[((long long)ss * E + e0) * NF + r] : R(1.0);
+  }
+  R J[ND][ND];
+#pragma unroll
+  for (int d1 = 0; d1 < ND; d1++)
+#pragma unroll
+    for (int d2 = 0; d2 < ND; d2++)
+      J[d1][d2] = valid ? a.JGinv[(((long long)d1 * NS + s) * E + e) * ND + d2] : R(0.0);
+  __syncthreads();
+
+  // B: reference-space flux at (s, el)
+  {
+    R Fp[ND][NF];
+    const R *u = &sU[s * ROW + el * NF];
+    if (valid) {
+      inviscid_flux<ND, R>(u, Fp, R(a.gamma));
+      if (VISC) {
+        // physical viscous flux added to the physical inviscid flux
+        // (reference: solver.cpp:777-811)
+        R gU[ND][NF], Fv[ND][NF];
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+#pragma unroll
+          for (int k = 0; k < NF; k++) gU[d][k] = a.dUs[d * a.dUsStride + ((long long)s * E + e) * NF + k];
+        viscous_flux<ND, R>(u, gU, a.ph, Fv);
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+#pragma unroll
+          for (int k = 0; k < NF; k++) Fp[d][k] = Fv[d][k] + Fp[d][k];
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < ND; d++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) Fp[d][k] = R(0.0);
+    }
+#pragma unroll
+    for (int d1 = 0; d1 < ND; d1++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        R f = R(0.0);
+#pragma unroll
+        for (int d2 = 0; d2 < ND; d2++) f += J[d1][d2] * Fp[d2][k];
+        sF[(d1 * NS + s) * ROW + el * NF + k] = f;
+        if (a.F_dbg && valid) a.F_dbg[(((long long)d1 * NS + s) * E + e) * NF + k] = f;
+      }
+  }
+  __syncthreads();
+
+  // C1: divergence at (s, el): sum over d of D-lines
+  int idx3[3];
+  idx3[0] = s % N;
+  idx3[1] = ND > 1 ? (s / N) % N : 0;
+  idx3[2] = ND > 2 ? s / (N * N) : 0;
+  R div[NF];
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
+    const int base = s - idx3[d] * stride;
+    const R *Dr = &sD[idx3[d] * N];
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R dv = Dr[m];
+      const R *x = &sF[(d * NS + base + m * stride) * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) div[k] = d == 0 ? acc[k] : div[k] + acc[k];
+  }
+
+  // C2: Fn - extrapolated normal flux at every (fpt, el)
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    const int ee = e0 + fe;
+    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R ev = sEF[side * N + m];
+      const R *x = &sF[(dn * NS + base + m * stride) * ROW + fe * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+    }
+    const bool v = fe < nValid;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const R q = v ? a.Fn[((long long)f * E + ee) * NF + k] - acc[k] : R(0.0);
+      sQ[f * ROW + fe * NF + k] = q;
+      if (a.disFn_dbg && v) a.disFn_dbg[((long long)f * E + ee) * NF + k] = q;
+    }
+  }
+  __syncthreads();
+
+  // D: correction and RK update at (s, el)
+  if (valid) {
+    R cq[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) cq[k] = R(0.0);
+#pragma unroll
+    for (int fc = 0; fc < 2 * ND; fc++) {
+      const int fp = __ldg(&t.corrFpt[s * 2 * ND + fc]);
+      const R cv = __ldg(&t.corrVal[s * 2 * ND + fc]);
+      const R *x = &sQ[fp * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
+    }
+    const R rdJ = R(1.0) / a.detJ[(long long)s * E + e];  // one reciprocal per point
+    const R dt = R(a.eleDt ? a.eleDt[e] : (a.mode != MODE_RESIDUAL ? *a.dt : 0.0));
+    const R rka = R(a.rka_next), rkb = R(a.rkb);
+    const bool finalStage = a.mode == MODE_RK_FINAL || (a.mode == MODE_JAMESON && a.stage == a.nRK - 1);
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const long long gi = ((long long)s * E + e) * NF + k;
+      R dv = cq[k] + div[k];
+      if (a.divF_out) a.divF_out[gi] = dv;
+      if (a.mode == MODE_RESIDUAL) continue;
+      if (a.src) dv = dv + a.src[gi];
+      const R u = sU[s * ROW + el * NF + k];
+      R unew;
+      if constexpr (!F32) {
+        if (a.mode == MODE_RK_STAGE) {
+          const R u0 = a.stage == 0 ? u : a.U0[gi];
+          if (a.stage == 0) a.U0[gi] = u;
+          unew = u0 - rka * dv * rdJ * dt;
+          const R base = a.stage == 0 ? u0 : a.acc[gi];
+          a.acc[gi] = base - rkb * dv * rdJ * dt;
+        } else if (a.mode == MODE_RK_FINAL) {
+          const R base = a.nRK == 1 ? u : a.acc[gi];
+          unew = base - rkb * dv * rdJ * dt;
+        } else {
+          const R u0 = a.stage == 0 ? u : a.U0[gi];
+          if (a.stage == 0) a.U0[gi] = u;
+          unew = u0 - rka * dv * rdJ * dt;
+        }
+      } else {
+        // precision form: increments in acc, compensated final addition
+        const R inc = dv * rdJ * dt;
+        if (a.mode == MODE_RK_STAGE) {
+          const R u0 = a.stage == 0 ? u : a.U0[gi];
+          if (a.stage == 0) a.U0[gi] = u;
+          unew = u0 - rka * inc;
+          a.acc[gi] = (a.stage == 0 ? R(0) : a.acc[gi]) - rkb * inc;
+        } else if (finalStage) {
+          const bool fromU0 = (a.mode == MODE_RK_FINAL && a.nRK > 1) || (a.mode == MODE_JAMESON && a.stage > 0);
+          const R u0 = fromU0 ? a.U0[gi] : u;
+          const R sum = a.mode == MODE_RK_FINAL ? (a.nRK > 1 ? a.acc[gi] : R(0)) - rkb * inc : -(rka * inc);
+          R c;
+          two_sum_tp(u0, a.comp[gi] + sum, unew, c);
+          a.comp[gi] = c;
+        } else {
+          const R u0 = a.stage == 0 ? u : a.U0[gi];
+          if (a.stage == 0) a.U0[gi] = u;
+          unew = u0 - rka * inc;
+        }
+      }
+      a.Uout[gi] = unew;
+      sU[s * ROW + el * NF + k] = unew;
+    }
+  }
+  if (a.mode == MODE_RESIDUAL || !a.Ufpts_out) return;
+  __syncthreads();
+
+  // E: new state at the flux points
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    if (fe >= nValid) continue;
+    const int ee = e0 + fe;
+    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R ev = sE[side * N + m];
+      const R *x = &sU[(base + m * stride) * ROW + fe * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) a.Ufpts_out[((long long)f * E + ee) * NF + k] = acc[k];
+  }
+}
+
+template <int ND, int P, typename R, bool VISC = false>
+void launch_tp(const ElemArgsT<R> &a, const TpTablesT<R> &t, cudaStream_t st) {
+  using T = Tp<ND, P, R>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_elem_tp<ND, P, VISC, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    attr = true;
+  }
+  int g = (a.E + T::EB - 1) / T::EB;
+  k_elem_tp<ND, P, VISC, R><<<g, T::NT, T::SMEM, st>>>(a, t);
+}
+
+#define FR_TP_ORDERS(X) X(2, 0) X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 5) X(3, 0) X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 5)
+
+}  // namespace
+
+bool tp_supported(int nDims, int order) { return (nDims == 2 || nDims == 3) && order >= 0 && order <= 5; }
+
+template <typename R>
+int tp_elems_per_block(int nDims, int order) {
+#define FR_TP_EB(ND, P) \
+  if (nDims == ND && order == P) return Tp<ND, P, R>::EB;
+  FR_TP_ORDERS(FR_TP_EB)
+#undef FR_TP_EB
+  return 0;
+}
+
+template <typename R>
+void launch_element_stage_tp(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t, cudaStream_t st) {
+  if (a.E <= 0) return;
+#define FR_TP_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_tp<ND, P, R>(a, t, st);
+  FR_TP_ORDERS(FR_TP_CASE)
+#undef FR_TP_CASE
+}
+
+template <typename R>
+void launch_element_stage_tp_visc(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
+                                  cudaStream_t st) {
+  if (a.E <= 0) return;
+#define FR_TPV_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_tp<ND, P, R, true>(a, t, st);
+  FR_TP_ORDERS(FR_TPV_CASE)
+#undef FR_TPV_CASE
+}
+
+template int tp_elems_per_block<double>(int, int);
+template int tp_elems_per_block<float>(int, int);
+template void launch_element_stage_tp<double>(int, int, const ElemArgsT<double> &, const TpTablesT<double> &,
+                                              cudaStream_t);
+template void launch_element_stage_tp<float>(int, int, const ElemArgsT<float> &, const TpTablesT<float> &,
+                                             cudaStream_t);
+template void launch_element_stage_tp_visc<double>(int, int, const ElemArgsT<double> &, const TpTablesT<double> &,
+                                                   cudaStream_t);
+template void launch_element_stage_tp_visc<float>(int, int, const ElemArgsT<float> &, const TpTablesT<float> &,
+                                                  cudaStream_t);
+
+}  // namespace frk

@@ -1,5 +1,5 @@
-// Viscous (LDG) pieces of an FP64 stage (reference: solver.cpp:366-445 with
-// viscous = 1):
+// Viscous (LDG) pieces of a stage, FP64 plain form and FP32 precision form
+// (reference: solver.cpp:366-445 with viscous = 1):
 //   k_faces_ldg_*   LDG interface solution UC and the jumps dUc = UC - U at
 //                   both sides of every face point (face.cpp:188-202, 588-615);
 //   k_elem_grad     corrected gradient at the solution points, transformed to
@@ -17,83 +17,83 @@ namespace {
 constexpr int ipow3(int b, int e) { return e == 0 ? 1 : b * ipow3(b, e - 1); }
 
 // LDG penalty direction switch (face.cpp:596-604, 244-252).
-template <int ND>
-__device__ __forceinline__ double ldg_pen(const double *n, double penFact) {
+template <int ND, typename R>
+__device__ __forceinline__ R ldg_pen(const R *n, R penFact) {
   if (ND == 2) return (n[0] + n[1] < 0) ? -penFact : penFact;
-  return (n[0] + n[1] + sqrt(2.) * n[ND - 1] < 0) ? -penFact : penFact;
+  return (n[0] + n[1] + sqrt(R(2.)) * n[ND - 1] < 0) ? -penFact : penFact;
 }
 
-template <int ND>
+template <int ND, typename R>
 __global__ void k_faces_ldg_interior(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
-                                     const double *__restrict__ nrm, const double *__restrict__ Uf,
-                                     double *__restrict__ dUc, double penFact) {
+                                     const R *__restrict__ nrm, const R *__restrict__ Uf,
+                                     R *__restrict__ dUc, R penFact) {
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int sL = slotL[i], sR = slotR[i];
-  double nv[ND];
+  R nv[ND];
 #pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
-  const double pen = ldg_pen<ND>(nv, penFact);
+  const R pen = ldg_pen<ND, R>(nv, penFact);
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    const double ul = Uf[(long long)sL * NF + k], ur = Uf[(long long)sR * NF + k];
-    const double uc = 0.5 * (ul + ur) - pen * (ul - ur);
+    const R ul = Uf[(long long)sL * NF + k], ur = Uf[(long long)sR * NF + k];
+    const R uc = R(0.5) * (ul + ur) - pen * (ul - ur);
     dUc[(long long)sL * NF + k] = uc - ul;
     dUc[(long long)sR * NF + k] = uc - ur;
   }
 }
 
-template <int ND>
+template <int ND, typename R>
 __global__ void k_faces_ldg_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
-                                     const double *__restrict__ nrm, const double *__restrict__ Uf,
-                                     double *__restrict__ dUc, Phys ph) {
+                                     const R *__restrict__ nrm, const R *__restrict__ Uf,
+                                     R *__restrict__ dUc, Phys ph) {
   constexpr int NF = ND + 2;
   int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int sL = slotL[i];
   const int bc = -slotR[i] - 2;
-  double UL[NF], UR[NF], nv[ND];
+  R UL[NF], UR[NF], nv[ND];
 #pragma unroll
   for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
 #pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
-  boundary_state<ND, double>(bc, UL, nv, ph, UR);
+  boundary_state<ND, R>(bc, UL, nv, ph, UR);
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    const double uc = 0.5 * (UL[k] + UR[k]);
+    const R uc = R(0.5) * (UL[k] + UR[k]);
     dUc[(long long)sL * NF + k] = uc - UL[k];
   }
 }
 
 // Common viscous flux added to the inviscid one (face.cpp:216-287), then *dA.
-template <int ND>
-__device__ __forceinline__ void ldg_interior_flux(const double *UL, const double *UR,
-                                                  const double gL[ND][ND + 2], const double gR[ND][ND + 2],
-                                                  const double *n, const Phys &ph, double *Fn) {
+template <int ND, typename R>
+__device__ __forceinline__ void ldg_interior_flux(const R *UL, const R *UR,
+                                                  const R gL[ND][ND + 2], const R gR[ND][ND + 2],
+                                                  const R *n, const Phys &ph, R *Fn) {
   constexpr int NF = ND + 2;
-  double FL[ND][NF], FR[ND][NF];
-  viscous_flux<ND, double>(UL, gL, ph, FL);
-  viscous_flux<ND, double>(UR, gR, ph, FR);
-  const double pen = ldg_pen<ND>(n, ph.penFact);
-  const double nx = n[0], ny = n[1], nz = ND == 3 ? n[ND - 1] : 0.0;
-  double Fc[ND][NF];
+  R FL[ND][NF], FR[ND][NF];
+  viscous_flux<ND, R>(UL, gL, ph, FL);
+  viscous_flux<ND, R>(UR, gR, ph, FR);
+  const R pen = ldg_pen<ND, R>(n, R(ph.penFact));
+  const R nx = n[0], ny = n[1], nz = ND == 3 ? n[ND - 1] : R(0.0);
+  R Fc[ND][NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    const double dF0 = FL[0][k] - FR[0][k];
-    const double dF1 = FL[1][k] - FR[1][k];
-    const double dU = UL[k] - UR[k];
+    const R dF0 = FL[0][k] - FR[0][k];
+    const R dF1 = FL[1][k] - FR[1][k];
+    const R dU = UL[k] - UR[k];
     if (ND == 2) {
-      Fc[0][k] = 0.5 * (FL[0][k] + FR[0][k]) + pen * nx * (nx * (dF0) + ny * (dF1)) + ph.tau * nx * (dU);
-      Fc[1][k] = 0.5 * (FL[1][k] + FR[1][k]) + pen * ny * (nx * (dF0) + ny * (dF1)) + ph.tau * ny * (dU);
+      Fc[0][k] = R(0.5) * (FL[0][k] + FR[0][k]) + pen * nx * (nx * (dF0) + ny * (dF1)) + R(ph.tau) * nx * (dU);
+      Fc[1][k] = R(0.5) * (FL[1][k] + FR[1][k]) + pen * ny * (nx * (dF0) + ny * (dF1)) + R(ph.tau) * ny * (dU);
     } else {
       // the reference pairs the left y-flux with the right z-flux here
       // (face.cpp:277); reproduced unless the quirk switch is off
-      const double dF2 = ph.viscFluxQuirk ? FL[1][k] - FR[ND - 1][k] : FL[ND - 1][k] - FR[ND - 1][k];
-      const double s = nx * (dF0) + ny * (dF1) + nz * (dF2);
-      Fc[0][k] = 0.5 * (FL[0][k] + FR[0][k]) + pen * nx * s + ph.tau * nx * (dU);
-      Fc[1][k] = 0.5 * (FL[1][k] + FR[1][k]) + pen * ny * s + ph.tau * ny * (dU);
-      Fc[ND - 1][k] = 0.5 * (FL[ND - 1][k] + FR[ND - 1][k]) + pen * nz * s + ph.tau * nz * (dU);
+      const R dF2 = ph.viscFluxQuirk ? FL[1][k] - FR[ND - 1][k] : FL[ND - 1][k] - FR[ND - 1][k];
+      const R s = nx * (dF0) + ny * (dF1) + nz * (dF2);
+      Fc[0][k] = R(0.5) * (FL[0][k] + FR[0][k]) + pen * nx * s + R(ph.tau) * nx * (dU);
+      Fc[1][k] = R(0.5) * (FL[1][k] + FR[1][k]) + pen * ny * s + R(ph.tau) * ny * (dU);
+      Fc[ND - 1][k] = R(0.5) * (FL[ND - 1][k] + FR[ND - 1][k]) + pen * nz * s + R(ph.tau) * nz * (dU);
     }
   }
 #pragma unroll
@@ -102,17 +102,17 @@ __device__ __forceinline__ void ldg_interior_flux(const double *UL, const double
     for (int k = 0; k < NF; k++) Fn[k] += Fc[d][k] * n[d];
 }
 
-template <int ND>
+template <int ND, typename R>
 __global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
-                                      const double *__restrict__ nrm, const double *__restrict__ dAL,
-                                      const double *__restrict__ dAR, const double *__restrict__ Uf,
-                                      const double *__restrict__ dUf, long long dStride, double *__restrict__ Fn,
+                                      const R *__restrict__ nrm, const R *__restrict__ dAL,
+                                      const R *__restrict__ dAR, const R *__restrict__ Uf,
+                                      const R *__restrict__ dUf, long long dStride, R *__restrict__ Fn,
                                       double *__restrict__ waveSp, Phys ph) {
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int sL = slotL[i], sR = slotR[i];
-  double UL[NF], UR[NF], nv[ND], F[NF], gL[ND][NF], gR[ND][NF];
+  R UL[NF], UR[NF], nv[ND], F[NF], gL[ND][NF], gR[ND][NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
     UL[k] = Uf[(long long)sL * NF + k];
@@ -128,11 +128,11 @@ __global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, cons
     }
   }
   if (ND == 2 && ph.riemannType == 1)
-    roe2d<double>(UL, UR, nv, ph.gamma, F);
+    roe2d<R>(UL, UR, nv, R(ph.gamma), F);
   else
-    waveSp[sL] = rusanov<ND, double>(UL, UR, nv, ph.gamma, F);
-  ldg_interior_flux<ND>(UL, UR, gL, gR, nv, ph, F);
-  const double aL = dAL[i], aR = dAR[i];
+    waveSp[sL] = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  ldg_interior_flux<ND, R>(UL, UR, gL, gR, nv, ph, F);
+  const R aL = dAL[i], aR = dAR[i];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
     Fn[(long long)sL * NF + k] = F[k] * aL;
@@ -140,18 +140,18 @@ __global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, cons
   }
 }
 
-template <int ND>
+template <int ND, typename R>
 __global__ void k_faces_visc_boundary(int n0, int n, const int *__restrict__ slotL,
-                                      const int *__restrict__ slotR, const double *__restrict__ nrm,
-                                      const double *__restrict__ dAL, const double *__restrict__ Uf,
-                                      const double *__restrict__ dUf, long long dStride, double *__restrict__ Fn,
+                                      const int *__restrict__ slotR, const R *__restrict__ nrm,
+                                      const R *__restrict__ dAL, const R *__restrict__ Uf,
+                                      const R *__restrict__ dUf, long long dStride, R *__restrict__ Fn,
                                       double *__restrict__ waveSp, Phys ph) {
   constexpr int NF = ND + 2;
   int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int sL = slotL[i];
   const int bc = -slotR[i] - 2;
-  double UL[NF], UR[NF], nv[ND], F[NF], g[ND][NF];
+  R UL[NF], UR[NF], nv[ND], F[NF], g[ND][NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
 #pragma unroll
@@ -160,54 +160,54 @@ __global__ void k_faces_visc_boundary(int n0, int n, const int *__restrict__ slo
 #pragma unroll
     for (int k = 0; k < NF; k++) g[d][k] = dUf[d * dStride + (long long)sL * NF + k];
   }
-  boundary_state<ND, double>(bc, UL, nv, ph, UR);
-  waveSp[sL] = rusanov<ND, double>(UL, UR, nv, ph.gamma, F);
-  double Fv[ND][NF];
+  boundary_state<ND, R>(bc, UL, nv, ph, UR);
+  waveSp[sL] = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  R Fv[ND][NF];
   if (bc == BC_ADI_NOSLIP) {
     // adiabatic wall: right gradient with the temperature gradient removed
     // (boundFace.cpp:316-350), right-state viscous flux
-    const double gam = ph.gamma;
-    double rhovSq = 0.;
+    const R gam = R(ph.gamma);
+    R rhovSq = R(0.);
 #pragma unroll
     for (int d = 0; d < ND; d++) rhovSq += UL[d + 1] * UL[d + 1];
-    const double pL = (gam - 1.) * (UL[ND + 1] - 0.5 * rhovSq / UL[0]);
-    const double pR = pL;
-    const double e = pR / ((gam - 1.) * UR[0]);
-    double gradVel[ND][ND];
+    const R pL = (gam - R(1.)) * (UL[ND + 1] - R(0.5) * rhovSq / UL[0]);
+    const R pR = pL;
+    const R e = pR / ((gam - R(1.)) * UR[0]);
+    R gradVel[ND][ND];
 #pragma unroll
     for (int d1 = 0; d1 < ND; d1++)
 #pragma unroll
       for (int d2 = 0; d2 < ND; d2++) gradVel[d1][d2] = (g[d1][d2 + 1] - g[d1][0] * UR[d2 + 1] / UR[0]) / UR[0];
-    double vSq = 0.;
+    R vSq = R(0.);
 #pragma unroll
     for (int d = 0; d < ND; d++) vSq += UR[d + 1] * UR[d + 1] / (UR[0] * UR[0]);
 #pragma unroll
     for (int d1 = 0; d1 < ND; d1++) {
-      double v = (e + 0.5 * vSq) * g[d1][0];
+      R v = (e + R(0.5) * vSq) * g[d1][0];
 #pragma unroll
       for (int d2 = 0; d2 < ND; d2++) v += UR[d2 + 1] * gradVel[d2][d1];
       g[d1][ND + 1] = v;
     }
-    viscous_flux<ND, double>(UR, g, ph, Fv);
+    viscous_flux<ND, R>(UR, g, ph, Fv);
   } else {
-    viscous_flux<ND, double>(UL, g, ph, Fv);
+    viscous_flux<ND, R>(UL, g, ph, Fv);
   }
 #pragma unroll
   for (int d = 0; d < ND; d++)
 #pragma unroll
-    for (int k = 0; k < NF; k++) Fv[d][k] = Fv[d][k] + ph.tau * nv[d] * (UL[k] - UR[k]);
+    for (int k = 0; k < NF; k++) Fv[d][k] = Fv[d][k] + R(ph.tau) * nv[d] * (UL[k] - UR[k]);
 #pragma unroll
   for (int d = 0; d < ND; d++)
 #pragma unroll
     for (int k = 0; k < NF; k++) F[k] += Fv[d][k] * nv[d];
-  const double aL = dAL[i];
+  const R aL = dAL[i];
 #pragma unroll
   for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
 }
 
 // Corrected, physical solution gradient at the solution points and at the
 // flux points, tensor-product form, one thread per (solution point, element).
-template <int ND, int P>
+template <int ND, int P, typename R>
 struct Tg {
   static constexpr int N = P + 1;
   static constexpr int NF = ND + 2;
@@ -216,19 +216,20 @@ struct Tg {
   static constexpr int EB = NS >= 128 ? 1 : (NS * 2 > 128 ? 1 : (NS * 4 > 128 ? 2 : (NS * 8 > 128 ? 4 : (NS * 16 > 128 ? 8 : (NS * 32 > 128 ? 16 : 32)))));
   static constexpr int NT = NS * EB;
   static constexpr int ROW = EB * NF;
-  static constexpr size_t SMEM = sizeof(double) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 2 * N);
+  static constexpr size_t SMEM = sizeof(R) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 2 * N);
 };
 
-template <int ND, int P>
-__global__ void __launch_bounds__(Tg<ND, P>::NT) k_elem_grad(GradArgs g, TpTables t) {
-  using T = Tg<ND, P>;
+template <int ND, int P, typename R>
+__global__ void __launch_bounds__(Tg<ND, P, R>::NT) k_elem_grad(GradArgsT<R> g, TpTablesT<R> t) {
+  using T = Tg<ND, P, R>;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
-  extern __shared__ double smem[];
-  double *sU = smem;                 // [NS][ROW]
-  double *sG = sU + NS * ROW;        // [ND][NS][ROW] physical gradient
-  double *sC = sG + ND * NS * ROW;   // [NFP][ROW] dUc
-  double *sD = sC + NFP * ROW;
-  double *sE = sD + N * N;
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  R *smem = reinterpret_cast<R *>(smem_bytes);
+  R *sU = smem;                 // [NS][ROW]
+  R *sG = sU + NS * ROW;        // [ND][NS][ROW] physical gradient
+  R *sC = sG + ND * NS * ROW;   // [NFP][ROW] dUc
+  R *sD = sC + NFP * ROW;
+  R *sE = sD + N * N;
   const int E = g.E;
   const int e0 = blockIdx.x * EB;
   const int nValid = min(EB, E - e0);
@@ -240,50 +241,50 @@ __global__ void __launch_bounds__(Tg<ND, P>::NT) k_elem_grad(GradArgs g, TpTable
   for (int i = tid; i < 2 * N; i += NT) sE[i] = t.E1[i];
   for (int idx = tid; idx < NS * ROW; idx += NT) {
     const int ss = idx / ROW, r = idx - ss * ROW;
-    sU[idx] = (r < nValid * NF) ? g.U[((long long)ss * E + e0) * NF + r] : 0.0;
+    sU[idx] = (r < nValid * NF) ? g.U[((long long)ss * E + e0) * NF + r] : R(0.0);
   }
   for (int idx = tid; idx < NFP * ROW; idx += NT) {
     const int f = idx / ROW, r = idx - f * ROW;
-    sC[idx] = (r < nValid * NF) ? g.dUc[((long long)f * E + e0) * NF + r] : 0.0;
+    sC[idx] = (r < nValid * NF) ? g.dUc[((long long)f * E + e0) * NF + r] : R(0.0);
   }
-  double J[ND][ND];
+  R J[ND][ND];
 #pragma unroll
   for (int d1 = 0; d1 < ND; d1++)
 #pragma unroll
-    for (int d2 = 0; d2 < ND; d2++) J[d1][d2] = valid ? g.JGinv[(((long long)d1 * NS + s) * E + e) * ND + d2] : 0.0;
-  const double invDet = valid ? 1. / g.detJ[(long long)s * E + e] : 0.0;
+    for (int d2 = 0; d2 < ND; d2++) J[d1][d2] = valid ? g.JGinv[(((long long)d1 * NS + s) * E + e) * ND + d2] : R(0.0);
+  const R invDet = valid ? R(1.) / g.detJ[(long long)s * E + e] : R(0.0);
   __syncthreads();
 
   int idx3[3];
   idx3[0] = s % N;
   idx3[1] = ND > 1 ? (s / N) % N : 0;
   idx3[2] = ND > 2 ? s / (N * N) : 0;
-  double gr[ND][NF];
+  R gr[ND][NF];
 #pragma unroll
   for (int d = 0; d < ND; d++) {
     const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
     const int base = s - idx3[d] * stride;
-    const double *Dr = &sD[idx3[d] * N];
-    double acc[NF];
+    const R *Dr = &sD[idx3[d] * N];
+    R acc[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[k] = 0.0;
+    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const double dv = Dr[m];
-      const double *x = &sU[(base + m * stride) * ROW + el * NF];
+      const R dv = Dr[m];
+      const R *x = &sU[(base + m * stride) * ROW + el * NF];
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
     }
     // + opp_correctU[d] . dUc: the faces normal to d, ascending
-    double cq[NF];
+    R cq[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) cq[k] = 0.0;
+    for (int k = 0; k < NF; k++) cq[k] = R(0.0);
 #pragma unroll
     for (int fc = 0; fc < 2 * ND; fc++) {
       const int fp = __ldg(&t.corrFpt[s * 2 * ND + fc]);
       if (__ldg(&t.fptDn[fp]) != d) continue;
-      const double cv = __ldg(&t.corrVal[s * 2 * ND + fc]) * (__ldg(&t.fptSide[fp]) ? 1.0 : -1.0);
-      const double *x = &sC[fp * ROW + el * NF];
+      const R cv = __ldg(&t.corrVal[s * 2 * ND + fc]) * (__ldg(&t.fptSide[fp]) ? R(1.0) : -R(1.0));
+      const R *x = &sC[fp * ROW + el * NF];
 #pragma unroll
       for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
     }
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(Tg<ND, P>::NT) k_elem_grad(GradArgs g, TpTable
   for (int d2 = 0; d2 < ND; d2++)
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      double v = gr[0][k] * J[0][d2] + gr[1][k] * J[1][d2];
+      R v = gr[0][k] * J[0][d2] + gr[1][k] * J[1][d2];
       if (ND == 3) v = gr[0][k] * J[0][d2] + gr[1][k] * J[1][d2] + gr[ND - 1][k] * J[ND - 1][d2];
       v = invDet * v;
       sG[(d2 * NS + s) * ROW + el * NF + k] = v;
@@ -309,13 +310,13 @@ __global__ void __launch_bounds__(Tg<ND, P>::NT) k_elem_grad(GradArgs g, TpTable
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-      double acc[NF];
+      R acc[NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] = 0.0;
+      for (int k = 0; k < NF; k++) acc[k] = R(0.0);
 #pragma unroll
       for (int m = 0; m < N; m++) {
-        const double ev = sE[side * N + m];
-        const double *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
+        const R ev = sE[side * N + m];
+        const R *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
         for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
       }
@@ -325,64 +326,75 @@ __global__ void __launch_bounds__(Tg<ND, P>::NT) k_elem_grad(GradArgs g, TpTable
   }
 }
 
-template <int ND, int P>
-void launch_grad(const GradArgs &g, const TpTables &t, cudaStream_t st) {
-  using T = Tg<ND, P>;
+template <int ND, int P, typename R>
+void launch_grad(const GradArgsT<R> &g, const TpTablesT<R> &t, cudaStream_t st) {
+  using T = Tg<ND, P, R>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_elem_grad<ND, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    cudaFuncSetAttribute(k_elem_grad<ND, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
-  k_elem_grad<ND, P><<<(g.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st>>>(g, t);
+  k_elem_grad<ND, P, R><<<(g.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st>>>(g, t);
 }
 
 }  // namespace
 
-void launch_faces_ldg(int nDims, const FaceTable &ft, const double *Ufpts, double *dUc, const Phys &ph,
-                      cudaStream_t st) {
+template <typename R>
+void launch_faces_ldg(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *dUc, const Phys &ph, cudaStream_t st) {
   const int b = 256, nI = ft.nInterior, nB = ft.n - ft.nInterior;
   if (nI > 0) {
     if (nDims == 2)
-      k_faces_ldg_interior<2><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
+      k_faces_ldg_interior<2, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
     else
-      k_faces_ldg_interior<3><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
+      k_faces_ldg_interior<3, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
   }
   if (nB > 0) {
     if (nDims == 2)
-      k_faces_ldg_boundary<2><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
+      k_faces_ldg_boundary<2, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
     else
-      k_faces_ldg_boundary<3><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
+      k_faces_ldg_boundary<3, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
   }
 }
 
-void launch_faces_visc(int nDims, const FaceTable &ft, const double *Ufpts, const double *dUf, long long fStride,
-                       double *Fn, double *waveSp, const Phys &ph, cudaStream_t st) {
+template <typename R>
+void launch_faces_visc(int nDims, const FaceTableT<R> &ft, const R *Ufpts, const R *dUf, long long fStride, R *Fn,
+                       double *waveSp, const Phys &ph, cudaStream_t st) {
   const int b = 128, nI = ft.nInterior, nB = ft.n - ft.nInterior;
   if (nI > 0) {
     if (nDims == 2)
-      k_faces_visc_interior<2><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
+      k_faces_visc_interior<2, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
     else
-      k_faces_visc_interior<3><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
+      k_faces_visc_interior<3, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
   }
   if (nB > 0) {
     if (nDims == 2)
-      k_faces_visc_boundary<2><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
+      k_faces_visc_boundary<2, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
     else
-      k_faces_visc_boundary<3><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
+      k_faces_visc_boundary<3, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
   }
 }
 
-void launch_elem_grad(int nDims, int order, const GradArgs &g, const TpTables &t, cudaStream_t st) {
+template <typename R>
+void launch_elem_grad(int nDims, int order, const GradArgsT<R> &g, const TpTablesT<R> &t, cudaStream_t st) {
   if (g.E <= 0) return;
 #define FR_G_CASE(ND, P) \
-  if (nDims == ND && order == P) return launch_grad<ND, P>(g, t, st);
+  if (nDims == ND && order == P) return launch_grad<ND, P, R>(g, t, st);
   FR_G_CASE(2, 0) FR_G_CASE(2, 1) FR_G_CASE(2, 2) FR_G_CASE(2, 3) FR_G_CASE(2, 4) FR_G_CASE(2, 5)
   FR_G_CASE(3, 0) FR_G_CASE(3, 1) FR_G_CASE(3, 2) FR_G_CASE(3, 3) FR_G_CASE(3, 4) FR_G_CASE(3, 5)
 #undef FR_G_CASE
 }
+
+#define FR_VISC_INST(R)                                                                                    \
+  template void launch_faces_ldg<R>(int, const FaceTableT<R> &, const R *, R *, const Phys &, cudaStream_t);      \
+  template void launch_faces_visc<R>(int, const FaceTableT<R> &, const R *, const R *, long long, R *, double *, \
+                                     const Phys &, cudaStream_t);                                                \
+  template void launch_elem_grad<R>(int, int, const GradArgsT<R> &, const TpTablesT<R> &, cudaStream_t);
+FR_VISC_INST(double)
+FR_VISC_INST(float)
+#undef FR_VISC_INST
 
 }  // namespace frk

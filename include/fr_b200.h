@@ -60,6 +60,7 @@ typedef struct fr_setup_opts {
   int device;                  /* CUDA device ordinal; -1: host-side setup only */
   int generic_kernels;         /* 1: use the general sparse-operator element kernel */
   int no_tma;                  /* 1: tensor-product element kernel without TMA tiles */
+  int tile_variant;            /* precision form: element tile shape, -1 (default) = autotuned at setup */
 } fr_setup_opts;
 
 /* Mesh supplied by the caller (linear quads or hexes, reference node order).
@@ -87,6 +88,8 @@ typedef struct fr_info {
   double time, dt;
   long long launches; /* kernels this case has launched (graph replays counted per kernel) */
   int tensor_kernels; /* 0 general, 1 tensor-product, 2 tensor-product with TMA tiles */
+  int tile_variant;   /* precision form: element tile shape in use (-1: none) */
+  int elems_per_block;
 } fr_info;
 
 /* Default fr_setup_opts (FP64, no perturbation, reference quirks on). */
