@@ -6,12 +6,33 @@ hex, 10,485,760 DOF), Rusanov flux, DG correction, classic RK4, dt from CFL 0.5
 on the initial state, FP64 throughout (the plain form).  Inputs are larger than
 L2 (the state alone is 84 MB, one stage touches ~1.2 GB), so no flush is needed.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--forms LIST]
 
 One JSON line (rank 0).  value = DOF * RK stages / s over all ranks with the
 state resident in HBM; e2e = the same metric through the C ABI with the state
 in pinned host memory, copied in and out every step.  N > 1 runs independent
 replicas (one case per GPU, no collective on the data path).
+
+At N = 1 the line also carries "forms", the other workloads of the path,
+each beside its plain-FP64 counterpart:
+  precision_tgv32  the same 32^3 P3 Taylor-Green run in the precision form
+                   (FP32 state/fluxes/operators, compensated RK sums), its
+                   throughput and its L2/max error vs the FP64 run after 200
+                   steps;
+  precision_ns_tgv40  3-D Navier-Stokes Taylor-Green, Re 1600, Pr 0.71,
+                   Mach 0.1, 40^3 hexes with interior vertices perturbed by
+                   U(-0.05h, 0.05h) (seed 2024), P=4, LDG (tau 0.1, beta 0.5),
+                   RK4: FP64 and precision form, 500 steps each, L2/max error;
+  batch256         256 seeded 2-D vortex cases (N~U{8..96}, P~U{2..5},
+                   strength~U(1,5), centre~U(-2,2)^2, Mach~U(0.2,0.6)), 500
+                   RK4 steps: precision form batched (one launch per stage
+                   per order, graph-captured step) vs the plain FP64 path
+                   case by case, with the L2 error of every case;
+  serve            a Poisson stream of channel-over-bump steady solves
+                   (h~U(0.02,0.1), nx~U{24..96}, ny=nx/3, P~U{1..4},
+                   Mach~U(0.2,0.5), local-CFL RK4 + P-multigrid, residual
+                   drop 1e-8) through the solve server: solves/s, p50/p99
+                   latency, vs the same solves one after another.
 """
 from __future__ import annotations
 
@@ -155,6 +176,260 @@ def run_reference_arm(args, rank):
     print(json.dumps(out))
 
 
+DECK_NS = os.path.join(ROOT, "flurrypp_b200", "decks", "ns_tgv3d_p4_40.deck")
+
+
+def dev_ms(torch, stream, fn):
+    """Device time of fn's work on `stream` (CUDA events, synchronized)."""
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def state_errors(U, ref):
+    """relative L2, max |diff| / max |ref|, and relative L2 per field."""
+    import numpy as np
+
+    d = U - ref
+    per = [float(np.linalg.norm(d[..., k]) / max(np.linalg.norm(ref[..., k]), 1e-300)) for k in range(ref.shape[-1])]
+    return {"l2_rel": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+            "max_rel": float(np.abs(d).max() / np.abs(ref).max()), "l2_rel_per_field": per}
+
+
+def elem_bytes(s, wbytes):
+    """Algorithmic bytes of one intermediate-stage element launch: read U, U0,
+    acc (3 nS nF), Fn (nFp nF), JGinv (nDims^2 nS), detJ (nS); write acc, U
+    (2 nS nF) and U_fpts (nFp nF); words of the working precision."""
+    nS, nFp, nF, nd, E = s.nSpts, s.nFpts, s.nFields, s.nDims, s.nEles
+    return wbytes * E * (5 * nS * nF + 2 * nFp * nF + nd * nd * nS + nS)
+
+
+def kernel_ms(torch, stream, s, kernel, reps=20):
+    s.bench_kernel(kernel, 2)
+    return dev_ms(torch, stream, lambda: s.bench_kernel(kernel, reps)) / reps
+
+
+def form_precision_tgv32(args, fb, torch, stream, dt):
+    s = fb.Solver(DECK_GPU, precision=fb.FR_PREC_MIXED)
+    s.set_stream(stream.cuda_stream)
+    s.initialize_solution(fb.IC_TGV, (0.1,))
+    s.set_dt(dt)
+    dof, nrk = s.nSpts * s.nEles * s.nFields, s.nRKSteps
+    s.run(args.warmup)
+    ms = dev_ms(torch, stream, lambda: s.run(args.steps))
+    inf = s.info()
+    km = kernel_ms(torch, stream, s, "element_stage")
+    fm = kernel_ms(torch, stream, s, "faces")
+    peak, _ = measured_peak_hbm()
+    eb = elem_bytes(s, 4)
+    ach = eb / (km / 1e3) / 1e9
+    del s
+    # error after 200 steps vs the plain form, same initial state and dt
+    runs = {}
+    for prec in (fb.FR_PREC_FP64, fb.FR_PREC_MIXED):
+        c = fb.Solver(DECK_GPU, precision=prec)
+        c.set_stream(stream.cuda_stream)
+        c.initialize_solution(fb.IC_TGV, (0.1,))
+        c.set_dt(dt)
+        c.run(args.err_steps)
+        runs[prec] = c.get_state()
+        del c
+    return {
+        "workload": "3D Euler TGV 32^3 P3 RK4, precision form (FP32 state/fluxes/operators, TwoSum RK sums)",
+        "value": dof * nrk * args.steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / args.steps,
+        "dtype": "f32 (FP64 dt, metrics at setup, norms)",
+        "tile_variant": inf.tile_variant, "elems_per_block": inf.elems_per_block,
+        "kernels_ms": {"element_stage": km, "faces": fm},
+        "roofline": {"bound": "hbm", "kernel": f"k_elem_tma<3, 3, float, {inf.tile_variant}>",
+                     "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "algorithmic_bytes": eb},
+        "error_vs_fp64": dict(steps=args.err_steps, **state_errors(runs[fb.FR_PREC_MIXED], runs[fb.FR_PREC_FP64])),
+    }
+
+
+def form_ns_tgv40(args, fb, torch, stream):
+    opts = dict(perturb=1, seed=2024, perturb_frac=0.05, mu_override=1, mu_inf=1.0 / 1600.0)
+    out, states, dt = {}, {}, None
+    for prec, tag in ((fb.FR_PREC_FP64, "fp64"), (fb.FR_PREC_MIXED, "precision")):
+        t0 = time.perf_counter()
+        c = fb.Solver(DECK_NS, precision=prec, **opts)
+        setup_s = time.perf_counter() - t0
+        c.set_stream(stream.cuda_stream)
+        c.initialize_solution(fb.IC_TGV, (0.1,))
+        if dt is None:
+            dt = c.calc_dt()
+        c.set_dt(dt)
+        dof, nrk = c.nSpts * c.nEles * c.nFields, c.nRKSteps
+        w = min(3, args.ns_steps)
+        c.run(w)
+        ms = dev_ms(torch, stream, lambda: c.run(args.ns_steps - w))
+        states[tag] = c.get_state()  # after exactly ns_steps steps
+        km = kernel_ms(torch, stream, c, "element_stage", 5)
+        fm = kernel_ms(torch, stream, c, "faces", 5)
+        out[tag] = {"value": dof * nrk * (args.ns_steps - w) / (ms / 1e3), "unit": METRIC,
+                    "ms_per_step": ms / (args.ns_steps - w), "setup_s": setup_s,
+                    "kernels_ms": {"element_stage": km, "faces_ldg_grad_visc": fm}}
+        del c
+    out["workload"] = ("3D Navier-Stokes TGV Re 1600 Pr 0.71 Mach 0.1, 40^3 hexes perturbed U(-0.05h,0.05h) "
+                       "seed 2024, P=4, LDG tau 0.1 beta 0.5, Rusanov, RK4")
+    out["dof"] = dof
+    out["dt"] = dt
+    out["speedup_precision_vs_fp64"] = out["precision"]["value"] / out["fp64"]["value"]
+    out["error_vs_fp64"] = dict(steps=args.ns_steps, **state_errors(states["precision"], states["fp64"]))
+    return out
+
+
+def form_batch256(args, fb, torch, stream):
+    import tempfile
+
+    import numpy as np
+    from flurrypp_b200.decks import vortex_case
+
+    rng = np.random.default_rng(args.batch_seed)
+    specs = []
+    for _ in range(args.batch_cases):
+        n = int(rng.integers(8, 97))
+        P = int(rng.integers(2, 6))
+        eps = float(rng.uniform(1, 5))
+        xc, yc = (float(v) for v in rng.uniform(-2, 2, 2))
+        M = float(rng.uniform(0.2, 0.6))
+        specs.append((n, P, eps, xc, yc, M))
+    tmp = tempfile.mkdtemp(prefix="fr_batch_")
+    t0 = time.perf_counter()
+    c64, c32, dofs = [], [], []
+    for i, (n, P, eps, xc, yc, M) in enumerate(specs):
+        deck = vortex_case(os.path.join(tmp, f"b{i}.deck"), n, P, M)
+        a = fb.Solver(deck)
+        a.set_stream(stream.cuda_stream)
+        a.initialize_solution(fb.IC_VORTEX, (eps, xc, yc, M))
+        dt = a.calc_dt()
+        a.set_dt(dt)
+        b = fb.Solver(deck, precision=fb.FR_PREC_MIXED)
+        b.initialize_solution(fb.IC_VORTEX, (eps, xc, yc, M))
+        b.set_dt(dt)
+        c64.append(a)
+        c32.append(b)
+        dofs.append(a.nSpts * a.nEles * a.nFields)
+    setup_s = time.perf_counter() - t0
+    nrk = c64[0].nRKSteps
+    tot = float(sum(dofs))
+    # plain FP64 path, case by case (each case its own graph-replayed run)
+    ms_alone = 0.0
+    for a in c64:
+        a.run(3)
+        ms_alone += dev_ms(torch, stream, lambda: a.run(args.alone_steps))
+    for i, (n, P, eps, xc, yc, M) in enumerate(specs):
+        c64[i].initialize_solution(fb.IC_VORTEX, (eps, xc, yc, M))
+    res = {}
+    for tag, cs in (("fp64_batched", c64), ("precision_batched", c32)):
+        bt = fb.Batch(cs)
+        w = 3
+        bt.run(w)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        bt.run(args.batch_steps - w)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t1
+        bt.gather()
+        inf = bt.info()
+        res[tag] = {"value": tot * nrk * (args.batch_steps - w) / sec, "unit": METRIC,
+                    "seconds": sec, "groups": inf["groups"]}
+        del bt
+    errs = [state_errors(b.get_state(), a.get_state())["l2_rel"] for a, b in zip(c64, c32)]
+    plain = tot * nrk * args.alone_steps / (ms_alone / 1e3)
+    return {
+        "workload": (f"{args.batch_cases} 2-D Euler vortex cases, seed {args.batch_seed}, N~U{{8..96}}, "
+                     "P~U{2..5}, strength~U(1,5), centre~U(-2,2)^2, Mach~U(0.2,0.6), RK4, dt CFL 0.5 per case, "
+                     f"{args.batch_steps} steps"),
+        "total_dof": int(tot), "setup_s": setup_s,
+        "plain_fp64_case_by_case": {"value": plain, "unit": METRIC, "steps_timed_per_case": args.alone_steps},
+        "fp64_batched": res["fp64_batched"], "precision_batched": res["precision_batched"],
+        "speedup_precision_batched_vs_plain_fp64": res["precision_batched"]["value"] / plain,
+        "timer": "host clock around a synchronized batch run (order groups run on their own streams)",
+        "error_vs_fp64": {"steps": args.batch_steps, "l2_rel_max": max(errs),
+                          "l2_rel_median": float(np.median(errs))},
+    }
+
+
+def form_serve(args, fb, torch):
+    import tempfile
+
+    import numpy as np
+    from flurrypp_b200.decks import channel_case
+    from flurrypp_b200.meshgen import channel_bump, write_gmsh
+
+    rng = np.random.default_rng(args.serve_seed)
+    tmp = tempfile.mkdtemp(prefix="fr_serve_")
+    reqs = []
+    for i in range(args.serve_requests):
+        h = float(rng.uniform(0.02, 0.1))
+        nx = int(rng.integers(24, 97))
+        P = int(rng.integers(1, 5))
+        M = float(rng.uniform(0.2, 0.5))
+        msh = os.path.join(tmp, f"bump{i}.msh")
+        write_gmsh(msh, channel_bump(nx, nx // 3, h))
+        reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), nx, P))
+    gaps = rng.exponential(1.0 / args.serve_rate, len(reqs))
+
+    def serve(max_inflight, paced):
+        srv = fb.Server(budget_bytes=args.serve_budget_gb << 30, max_inflight=max_inflight, check_every=10)
+        t0 = time.perf_counter()
+        ids = []
+        for (deck, nx, P), g in zip(reqs, gaps):
+            if paced:
+                time.sleep(g)
+            ids.append(srv.submit(deck, tol=1e-8, max_steps=args.serve_max_steps))
+        polls = []
+        for r in ids:
+            try:
+                srv.wait(r, 3600)
+            except fb.FrError:
+                pass
+            polls.append(srv.poll(r))
+        sec = time.perf_counter() - t0
+        srv.close()
+        lat = sorted(p["latency_s"] for p in polls)
+        done = [p for p in polls if p["status"] == 2]
+        return {"solves_per_s": len(done) / sec, "seconds": sec, "completed": len(done),
+                "converged_1e-8": sum(1 for p in done if p["res_ratio"] <= 1e-8),
+                "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                "steps_mean": float(np.mean([p["steps"] for p in polls]))}
+
+    stream_res = serve(args.serve_inflight, True)
+    seq = serve(1, False)
+    return {
+        "workload": (f"{len(reqs)} channel-over-bump requests, seed {args.serve_seed}, Poisson rate "
+                     f"{args.serve_rate}/s, h~U(0.02,0.1), nx~U{{24..96}}, ny=nx/3, P~U{{1..4}}, Mach~U(0.2,0.5), "
+                     "local-CFL RK4 + P-multigrid (lowOrder 0, 2 smoothing steps), residual drop 1e-8 "
+                     f"(at most {args.serve_max_steps} steps), FP64"),
+        "served": dict(max_inflight=args.serve_inflight, **stream_res),
+        "one_at_a_time": seq,
+        "speedup_solves_per_s": stream_res["solves_per_s"] / max(seq["solves_per_s"], 1e-30),
+    }
+
+
+def run_forms(args, fb, torch, stream, dt):
+    forms = {}
+    want = set(args.forms.split(",")) if args.forms else set()
+    jobs = [("precision_tgv32", lambda: form_precision_tgv32(args, fb, torch, stream, dt)),
+            ("precision_ns_tgv40", lambda: form_ns_tgv40(args, fb, torch, stream)),
+            ("batch256", lambda: form_batch256(args, fb, torch, stream)),
+            ("serve", lambda: form_serve(args, fb, torch))]
+    for name, fn in jobs:
+        if name not in want:
+            continue
+        try:
+            forms[name] = fn()
+        except Exception as e:  # report, keep the headline line
+            forms[name] = {"error": f"{type(e).__name__}: {e}"}
+    return forms
+
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -164,6 +439,20 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="precision_tgv32,precision_ns_tgv40,batch256,serve",
+                    help="comma list of extra workloads measured at N=1 ('' for none)")
+    ap.add_argument("--err-steps", type=int, default=200)
+    ap.add_argument("--ns-steps", type=int, default=500)
+    ap.add_argument("--batch-cases", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=500)
+    ap.add_argument("--batch-seed", type=int, default=2024)
+    ap.add_argument("--alone-steps", type=int, default=20)
+    ap.add_argument("--serve-requests", type=int, default=8)
+    ap.add_argument("--serve-rate", type=float, default=4.0)
+    ap.add_argument("--serve-seed", type=int, default=7)
+    ap.add_argument("--serve-max-steps", type=int, default=2000)
+    ap.add_argument("--serve-inflight", type=int, default=8)
+    ap.add_argument("--serve-budget-gb", type=int, default=64)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -296,6 +585,8 @@ def main():
             else:
                 out["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
                                        "sample": err}
+        if world == 1 and args.forms:
+            out["forms"] = run_forms(args, fb, torch, stream, dt)
         print(json.dumps(out))
     del s
     if world > 1:
