@@ -58,6 +58,7 @@ class SetupOpts(ctypes.Structure):
         ("generic_kernels", ctypes.c_int),
         ("no_tma", ctypes.c_int),
         ("tile_variant", ctypes.c_int),
+        ("no_tensor_cores", ctypes.c_int),
     ]
 
 

@@ -94,6 +94,7 @@ struct fr_case {
     frk::TmaMaps tm;
     bool useTma = false;
     int variant = 0;
+    float *tcOps = nullptr;     // 2-D tensor-core variant: operators in MMA layout
     std::vector<float> tuneMs;  // element-stage time per tile variant (autotuner)
   } f32;
 
@@ -645,7 +646,15 @@ struct fr_case {
   // variant computes each point with the same operations, so the choice
   // changes the speed only, never the result.
   bool autotune_tiles() {
-    const int nv = frk::tma_variants(true);
+    const bool tc = frk::tc2d_supported(nDims, in.order) && !opts.no_tensor_cores;
+    if (tc && !f32.tcOps) {
+      const double *g[2] = {op.grad[0].data(), op.grad[1].data()};
+      const double *x[2] = {op.extFn[0].data(), op.extFn[1].data()};
+      std::vector<float> blob;
+      if (!frk::tc2d_pack_ops(in.order, g, x, op.corr.data(), op.ext.data(), blob) || !upload(f32.tcOps, blob))
+        return fail(FR_ERR_CUDA, "tensor-core operator upload");
+    }
+    const int nv = frk::tma_variants(true) + (tc ? 1 : 0);
     int forced = opts.tile_variant;
     f32.tuneMs.assign(nv, -1.0f);
     if (forced >= nv) return fail(FR_ERR_ARG, "tile_variant out of range");
@@ -669,11 +678,10 @@ struct fr_case {
       a.mode = frk::MODE_RK_STAGE;
       a.stage = 1;
       a.Ufpts_out = f32.Ufpts;
-      for (int i = 0; i < 2; i++) frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
+      for (int i = 0; i < 2; i++) launch_tma32(a, v);
       cudaEventRecord(e0, stream);
       const int reps = 5;
-      for (int i = 0; i < reps; i++)
-        frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
+      for (int i = 0; i < reps; i++) launch_tma32(a, v);
       cudaEventRecord(e1, stream);
       if (cudaEventSynchronize(e1) != cudaSuccess) break;
       float ms = 0.0f;
@@ -990,11 +998,19 @@ struct fr_case {
       frk::launch_element_stage(nDims, a, stream);
     launches++;
   }
+  // precision-form TMA element stage of tile variant v: CUDA-core variants
+  // 0 .. tma_variants-1, then the 2-D tensor-core one
+  void launch_tma32(const frk::ElemArgsT<float> &a, int v) {
+    if (v == frk::tma_variants(true))
+      frk::launch_element_stage_tc2d(in.order, a, f32.tcOps, f32.tm, stream);
+    else
+      frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
+  }
   void element32(const frk::ElemArgsT<float> &a) {
     if (in.viscous)
       frk::launch_element_stage_tp_visc<float>(nDims, in.order, a, f32.tp, stream);
     else if (f32.useTma)
-      frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, f32.variant);
+      launch_tma32(a, f32.variant);
     else
       frk::launch_element_stage_tp<float>(nDims, in.order, a, f32.tp, stream);
     launches++;
@@ -1592,6 +1608,10 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
     int s = std::atoi(n.c_str() + 5);
     if (s < 0 || s >= c->nRK) return FR_ERR_ARG;
     return copy_dev(c, c->divF[s], nU, host, count);
+  }
+  if (n == "tile_ms") {  // precision form: element-stage ms per tile variant timed by the autotuner (-1: not run)
+    std::vector<double> v(c->f32.tuneMs.begin(), c->f32.tuneMs.end());
+    return copy_out(c, v, host, count);
   }
   if (n == "pos_spts") return copy_out(c, c->geo.pos_spts, host, count);
   if (n == "detJac_spts") return copy_out(c, c->geo.detJac_spts, host, count);

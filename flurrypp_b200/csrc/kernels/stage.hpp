@@ -8,6 +8,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fr_physics.cuh"
 
 namespace frk {
@@ -146,6 +148,15 @@ size_t tma_smem_bytes(int nDims, int order, int variant = 0);
 template <typename R>
 void launch_element_stage_tma(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
                               const TmaMaps &m, cudaStream_t st, int variant = 0);
+// 2-D precision-form element stage on the tensor cores (tcgen05 kind::tf32,
+// 3xTF32), 32 elements per CTA; the tile variant after the CUDA-core ones.
+// The operators are packed once on the host into the MMA operand layout.
+bool tc2d_supported(int nDims, int order);
+bool tc2d_pack_ops(int order, const double *const grad[2], const double *const extFn[2], const double *corr,
+                   const double *ext, std::vector<float> &blob);
+size_t tc2d_smem_bytes(int order);
+void launch_element_stage_tc2d(int order, const ElemArgsT<float> &a, const float *ops, const TmaMaps &m,
+                               cudaStream_t st);
 template <typename R>
 int tp_elems_per_block(int nDims, int order);
 template <typename R>

@@ -60,7 +60,9 @@ typedef struct fr_setup_opts {
   int device;                  /* CUDA device ordinal; -1: host-side setup only */
   int generic_kernels;         /* 1: use the general sparse-operator element kernel */
   int no_tma;                  /* 1: tensor-product element kernel without TMA tiles */
-  int tile_variant;            /* precision form: element tile shape, -1 (default) = autotuned at setup */
+  int tile_variant;            /* precision form: element tile shape, -1 (default) = autotuned at setup;
+                                  the last variant of 2-D orders 1..4 is the tensor-core (tcgen05) kernel */
+  int no_tensor_cores;         /* 1: leave the tensor-core variant out of the autotuner's choice */
 } fr_setup_opts;
 
 /* Mesh supplied by the caller (linear quads or hexes, reference node order).

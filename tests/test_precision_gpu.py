@@ -142,3 +142,42 @@ def test_mixed_batch_equals_alone(tmp_path):
         Ua, ra = alone[i]
         assert np.max(np.abs(U - Ua)) <= 1e-6 * np.max(np.abs(Ua)), i
         assert np.allclose(norms[i], ra, rtol=1e-4, atol=0)
+
+
+TC_CASES = ["vortex2d_p3_8", "channel2d_p2", "roe2d_p2", "hu2d_p3", "cplus2d_p2", "lobatto_sd2d_p4",
+            "jameson5_2d_p2", "euler_fwd2d_p1", "localdt_jameson2d_p3", "ic1_2d_p3"]
+
+
+def tensor_case(meta, **kw):
+    s = mixed_case(meta, tile_variant=3, **kw)
+    if s.info().tile_variant != 3:
+        pytest.skip("element count not a multiple of 4 or order outside 1..4: no TMA tiles")
+    return s
+
+
+@pytest.mark.parametrize("case", TC_CASES)
+def test_tensor_core_variant_residual_and_steps(case):
+    """The tcgen05 (3xTF32) element stage: residual within FP32 round-off of
+    the reference's and the state after N steps within the L2 bound."""
+    a, meta = load_golden(case)
+    s = tensor_case(meta, debug_arrays=1)
+    s.set_state(a["U_init"])
+    s.calc_residual(0)
+    d = s.get_residual(0)
+    scale = max(np.abs(a["divF_0"]).max(), np.abs(a["F_spts"]).max())
+    assert np.abs(d - a["divF_0"]).max() / scale < RESID_TOL
+    s2 = tensor_case(meta)
+    s2.set_state(a["U_init"])
+    s2.run(meta["steps"])
+    assert rel_l2(s2.get_state(), a["U_final"]) < L2_TOL
+
+
+def test_tensor_core_variant_near_cuda_core_variant():
+    a, meta = load_golden("vortex2d_p3_8")
+    out = []
+    for v in (0, 3):
+        s = mixed_case(meta, tile_variant=v)
+        s.set_state(a["U_init"])
+        s.run(20)
+        out.append(s.get_state())
+    assert rel_l2(out[1], out[0]) < 1e-7
