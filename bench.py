@@ -430,6 +430,60 @@ def run_forms(args, fb, torch, stream, dt):
 
 
 
+PROFILE_CASES = {
+    # name: (deck kind, order, size, precision, tile variant)
+    "fp64_tgv32_p3": ("tgv", 3, 32, 0, -1),
+    "fp32_tgv32_p3": ("tgv", 3, 32, 1, -1),
+    "fp32_vortex256_p3": ("vortex", 3, 256, 1, -1),
+    "tc_vortex256_p3": ("vortex", 3, 256, 1, 3),
+    "fp32_ns_tgv24_p4": ("ns", 4, 24, 1, -1),
+}
+
+
+def run_profile(names):
+    """Set each case up, then launch its element stage and face pass once
+    between cudaProfilerStart/Stop (for `ncu --profile-from-start off`)."""
+    import tempfile
+
+    import torch
+    import flurrypp_b200 as fb
+    from flurrypp_b200.decks import vortex_case, write_deck
+
+    tmp = tempfile.mkdtemp(prefix="fr_prof_")
+    out = {}
+    for name in names.split(","):
+        kind, P, n, prec, var = PROFILE_CASES[name]
+        opts = dict(precision=prec, tile_variant=var)
+        if kind == "tgv":
+            deck, ic = DECK_GPU if n == 32 else None, (fb.IC_TGV, (0.1,))
+        elif kind == "vortex":
+            deck, ic = vortex_case(os.path.join(tmp, f"{name}.deck"), n, P, 0.5), (fb.IC_VORTEX, (5.0, 0.0, 0.0, 0.5))
+        else:
+            src = open(DECK_NS).read().replace("nx            40", f"nx            {n}")
+            src = src.replace("ny            40", f"ny            {n}").replace("nz            40", f"nz            {n}")
+            deck = os.path.join(tmp, f"{name}.deck")
+            open(deck, "w").write(src)
+            ic = (fb.IC_TGV, (0.1,))
+            opts.update(perturb=1, seed=2024, perturb_frac=0.05, mu_override=1, mu_inf=1.0 / 1600.0)
+        s = fb.Solver(deck, **opts)
+        s.initialize_solution(*ic)
+        s.set_dt(s.calc_dt())
+        s.run(2)
+        s.synchronize()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        s.bench_kernel("element_stage", 1)
+        s.bench_kernel("faces", 1)
+        s.synchronize()
+        torch.cuda.profiler.stop()
+        inf = s.info()
+        out[name] = {"nEles": s.nEles, "order": s.order, "nDims": s.nDims, "precision": prec,
+                     "tile_variant": inf.tile_variant, "elems_per_block": inf.elems_per_block}
+        del s
+    print(json.dumps({"profile": out}))
+
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,7 +507,12 @@ def main():
     ap.add_argument("--serve-max-steps", type=int, default=2000)
     ap.add_argument("--serve-inflight", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=int, default=64)
+    ap.add_argument("--profile", default="", help="comma list of PROFILE_CASES: one element stage and one "
+                    "face pass each between cudaProfilerStart/Stop, then exit")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args.profile)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

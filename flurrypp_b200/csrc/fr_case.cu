@@ -327,7 +327,7 @@ struct fr_case {
     if (!alloc(devErr, 1)) return false;
     if (!mixed) {
       useTma = useTp && !in.viscous && !opts.no_tma && build_tma();
-    } else if (useTp && !in.viscous && !opts.no_tma && E % 4 == 0) {
+    } else if (useTp && !in.viscous && !opts.no_tma && (E * nF) % 4 == 0) {
       if (!autotune_tiles()) return false;
     }
     hostDt = in.dt;
@@ -592,40 +592,6 @@ struct fr_case {
     return o;
   }
 
-  // TMA descriptors of the precision form's tiles for tile variant v (the
-  // box width is that variant's element block); rows are 16-byte multiples
-  // when E is a multiple of 4.
-  bool build_tma32(int v) {
-    if (E % 4 != 0 || nS > 256 || nFp > 256) return false;
-    auto encode = tensor_map_encoder();
-    if (!encode) return false;
-    const int eb = frk::tma_elems_per_block<float>(nDims, in.order, v);
-    if (eb <= 0 || eb % 4 != 0) return false;
-    auto map2 = [&](CUtensorMap *m, void *p, cuuint64_t inner, cuuint64_t outer, cuuint32_t bi, cuuint32_t bo) {
-      cuuint64_t dims[2] = {inner, outer};
-      cuuint64_t str[1] = {inner * sizeof(float)};
-      cuuint32_t box[2] = {bi, bo};
-      cuuint32_t es[2] = {1, 1};
-      return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, p, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-    };
-    const cuuint64_t rowU = (cuuint64_t)E * nF;
-    frk::TmaMaps &t = f32.tm;
-    bool ok = map2(&t.U, f32.U, rowU, nS, eb * nF, nS) && map2(&t.U0, f32.U0, rowU, nS, eb * nF, nS) &&
-              map2(&t.acc, f32.acc, rowU, nS, eb * nF, nS) && map2(&t.comp, f32.comp, rowU, nS, eb * nF, nS) &&
-              map2(&t.Fn, f32.Fn, rowU, nFp, eb * nF, nFp) && map2(&t.Ufpts, f32.Ufpts, rowU, nFp, eb * nF, nFp) &&
-              map2(&t.det, f32.detJ, E, nS, eb, nS);
-    if (!ok) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)E * nDims, (cuuint64_t)nS, (cuuint64_t)nDims};
-    cuuint64_t str[2] = {(cuuint64_t)E * nDims * sizeof(float), (cuuint64_t)nS * E * nDims * sizeof(float)};
-    cuuint32_t box[3] = {(cuuint32_t)(eb * nDims), (cuuint32_t)nS, (cuuint32_t)nDims};
-    cuuint32_t es[3] = {1, 1, 1};
-    return encode(&t.J, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, f32.JGinv, dims, str, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-  }
-
   static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -666,8 +632,8 @@ struct fr_case {
       return fail(FR_ERR_CUDA, "event create");
     for (int v = 0; v < nv; v++) {
       if (forced >= 0 && v != forced) continue;
-      bool dup = false;  // variants that clamp to the same tile are timed once
-      for (int w = 0; w < v; w++)
+      bool dup = false;  // CUDA-core variants that clamp to the same tile are timed once
+      for (int w = 0; w < v && v < frk::tma_variants(true); w++)
         if (frk::tma_elems_per_block<float>(nDims, in.order, w) == frk::tma_elems_per_block<float>(nDims, in.order, v))
           dup = true;
       if (dup && forced < 0) continue;
@@ -712,36 +678,76 @@ struct fr_case {
     return sync();
   }
 
-  // TMA descriptors for the tile copies of the TMA element kernel.  The row
-  // pitch of every tensor must be a multiple of 16 bytes: E even.
-  bool build_tma() {
-    if (E % 2 != 0 || nS > 256 || nFp > 256) return false;
+  // The metric arrays as the TMA element kernels read them: every row pitch
+  // of a tensor map must be a multiple of 16 bytes, so when E is not a
+  // multiple of `align` elements, copies of detJ and JGinv with the element
+  // axis padded to Ep (zeros in the padding) serve the tensor maps.
+  template <typename T>
+  bool tma_metrics(int align, T *det, T *jg, T *&detOut, T *&jgOut, int &Ep) {
+    Ep = (E + align - 1) / align * align;
+    detOut = det;
+    jgOut = jg;
+    if (Ep == E) return true;
+    std::vector<T> d((size_t)nS * Ep, T(0)), j((size_t)nDims * nS * Ep * nDims, T(0));
+    for (int s = 0; s < nS; s++)
+      for (int e = 0; e < E; e++) d[(size_t)s * Ep + e] = (T)geo.detJac_spts[(size_t)s * E + e];
+    for (int a = 0; a < nDims * nS; a++)
+      for (int e = 0; e < E; e++)
+        for (int b = 0; b < nDims; b++)
+          j[((size_t)a * Ep + e) * nDims + b] = (T)geo.JGinv_spts[((size_t)a * E + e) * nDims + b];
+    return upload(detOut, d) && upload(jgOut, j);
+  }
+
+  // TMA descriptors for the tile copies of a TMA element kernel: element
+  // block eb, element type T.  State rows need E*nF*sizeof(T) to be a
+  // multiple of 16 bytes (2-D always; 3-D E even in FP64, E a multiple of 4
+  // in FP32); the metrics use padded copies where needed.
+  template <typename T>
+  bool build_maps(frk::TmaMaps &t, int eb, T *u, T *u0, T *ac, T *cmp, T *fn, T *uf, T *det, T *jg,
+                  T *&detPad, T *&jgPad) {
+    const int align = 16 / (int)sizeof(T);
+    if ((E * nF) % align != 0 || nS > 256 || nFp > 256 || eb <= 0 || (eb * nF) % align != 0 ||
+        (eb * nDims) % align != 0 || eb % align != 0)
+      return false;
     auto encode = tensor_map_encoder();
     if (!encode) return false;
-    const int eb = frk::tma_elems_per_block<double>(nDims, in.order);
-    auto map2 = [&](CUtensorMap *m, void *p, cuuint64_t inner, cuuint64_t outer, cuuint32_t bi, cuuint32_t bo) {
+    const CUtensorMapDataType ty = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    auto map2 = [&](CUtensorMap *m, void *p, cuuint64_t inner, cuuint64_t outer, cuuint64_t pitch, cuuint32_t bi,
+                    cuuint32_t bo) {
       cuuint64_t dims[2] = {inner, outer};
-      cuuint64_t str[1] = {inner * sizeof(double)};
+      cuuint64_t str[1] = {pitch * sizeof(T)};
       cuuint32_t box[2] = {bi, bo};
       cuuint32_t es[2] = {1, 1};
-      return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+      return encode(m, ty, 2, p, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     };
+    int Ep = E;
+    if (!detPad && !tma_metrics<T>(align, det, jg, detPad, jgPad, Ep)) return false;
+    Ep = (E + align - 1) / align * align;
     const cuuint64_t rowU = (cuuint64_t)E * nF;
-    bool ok = map2(&tm.U, U, rowU, nS, eb * nF, nS) && map2(&tm.U0, U0, rowU, nS, eb * nF, nS) &&
-              map2(&tm.acc, acc, rowU, nS, eb * nF, nS) && map2(&tm.Fn, Fn, rowU, nFp, eb * nF, nFp) &&
-              map2(&tm.Ufpts, Ufpts, rowU, nFp, eb * nF, nFp) && map2(&tm.det, detJ, E, nS, eb, nS);
+    bool ok = map2(&t.U, u, rowU, nS, rowU, eb * nF, nS) && map2(&t.Fn, fn, rowU, nFp, rowU, eb * nF, nFp) &&
+              map2(&t.Ufpts, uf, rowU, nFp, rowU, eb * nF, nFp) && map2(&t.det, detPad, E, nS, Ep, eb, nS);
+    if (u0) ok = ok && map2(&t.U0, u0, rowU, nS, rowU, eb * nF, nS);
+    if (ac) ok = ok && map2(&t.acc, ac, rowU, nS, rowU, eb * nF, nS);
+    if (cmp) ok = ok && map2(&t.comp, cmp, rowU, nS, rowU, eb * nF, nS);
     if (!ok) return false;
     cuuint64_t dims[3] = {(cuuint64_t)E * nDims, (cuuint64_t)nS, (cuuint64_t)nDims};
-    cuuint64_t str[2] = {(cuuint64_t)E * nDims * sizeof(double), (cuuint64_t)nS * E * nDims * sizeof(double)};
+    cuuint64_t str[2] = {(cuuint64_t)Ep * nDims * sizeof(T), (cuuint64_t)nS * Ep * nDims * sizeof(T)};
     cuuint32_t box[3] = {(cuuint32_t)(eb * nDims), (cuuint32_t)nS, (cuuint32_t)nDims};
     cuuint32_t es[3] = {1, 1, 1};
-    if (encode(&tm.J, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, JGinv, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return false;
-    return true;
+    return encode(&t.J, ty, 3, jgPad, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  double *detTma = nullptr, *jgTma = nullptr;
+  float *detTma32 = nullptr, *jgTma32 = nullptr;
+
+  bool build_tma() {
+    return build_maps<double>(tm, frk::tma_elems_per_block<double>(nDims, in.order), U, U0, acc, nullptr, Fn, Ufpts,
+                              detJ, JGinv, detTma, jgTma);
+  }
+  bool build_tma32(int v) {
+    return build_maps<float>(f32.tm, frk::tma_elems_per_block<float>(nDims, in.order, v), f32.U, f32.U0, f32.acc,
+                             f32.comp, f32.Fn, f32.Ufpts, f32.detJ, f32.JGinv, detTma32, jgTma32);
   }
 
   // Merge the host data of several same-order cases along the element axis
