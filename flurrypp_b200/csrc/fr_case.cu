@@ -326,8 +326,16 @@ struct fr_case {
     }
     if (!alloc(devErr, 1)) return false;
     if (!mixed) {
-      useTma = useTp && !in.viscous && !opts.no_tma && build_tma();
-    } else if (useTp && !in.viscous && !opts.no_tma && (E * nF) % 4 == 0) {
+      useTma = useTp && !opts.no_tma && build_tma();
+      if (useTma && in.viscous) EB = frk::tma_elems_per_block<double>(nDims, in.order);
+    } else if (useTp && in.viscous && !opts.no_tma && (E * nF) % 4 == 0) {
+      // viscous precision form: tile variant 0
+      if (build_tma32(0)) {
+        f32.useTma = true;
+        f32.variant = 0;
+        EB = frk::tma_elems_per_block<float>(nDims, in.order, 0);
+      }
+    } else if (useTp && !opts.no_tma && (E * nF) % 4 == 0) {
       if (!autotune_tiles()) return false;
     }
     hostDt = in.dt;
@@ -704,7 +712,7 @@ struct fr_case {
   // in FP32); the metrics use padded copies where needed.
   template <typename T>
   bool build_maps(frk::TmaMaps &t, int eb, T *u, T *u0, T *ac, T *cmp, T *fn, T *uf, T *det, T *jg,
-                  T *&detPad, T *&jgPad) {
+                  T *&detPad, T *&jgPad, T *dus = nullptr, T *duc = nullptr, T *duf = nullptr) {
     const int align = 16 / (int)sizeof(T);
     if ((E * nF) % align != 0 || nS > 256 || nFp > 256 || eb <= 0 || (eb * nF) % align != 0 ||
         (eb * nDims) % align != 0 || eb % align != 0)
@@ -731,23 +739,34 @@ struct fr_case {
     if (ac) ok = ok && map2(&t.acc, ac, rowU, nS, rowU, eb * nF, nS);
     if (cmp) ok = ok && map2(&t.comp, cmp, rowU, nS, rowU, eb * nF, nS);
     if (!ok) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)E * nDims, (cuuint64_t)nS, (cuuint64_t)nDims};
-    cuuint64_t str[2] = {(cuuint64_t)Ep * nDims * sizeof(T), (cuuint64_t)nS * Ep * nDims * sizeof(T)};
-    cuuint32_t box[3] = {(cuuint32_t)(eb * nDims), (cuuint32_t)nS, (cuuint32_t)nDims};
-    cuuint32_t es[3] = {1, 1, 1};
-    return encode(&t.J, ty, 3, jgPad, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    auto map3 = [&](CUtensorMap *m, void *p, cuuint64_t d0, cuuint64_t d1, cuuint64_t d2, cuuint64_t pitch0,
+                    cuuint32_t b0, cuuint32_t b1, cuuint32_t b2) {
+      cuuint64_t dims[3] = {d0, d1, d2};
+      cuuint64_t str[2] = {pitch0 * sizeof(T), pitch0 * d1 * sizeof(T)};
+      cuuint32_t box[3] = {b0, b1, b2};
+      cuuint32_t es[3] = {1, 1, 1};
+      return encode(m, ty, 3, p, dims, str, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    if (!map3(&t.J, jgPad, (cuuint64_t)E * nDims, nS, nDims, (cuuint64_t)Ep * nDims, eb * nDims, nS, nDims))
+      return false;
+    // viscous: gradients [nDims][points][E*nF], jumps [nFp][E*nF]
+    if (dus && !map3(&t.dUs, dus, rowU, nS, nDims, rowU, eb * nF, nS, nDims)) return false;
+    if (duf && !map3(&t.dUf, duf, rowU, nFp, nDims, rowU, eb * nF, nFp, nDims)) return false;
+    if (duc && !map2(&t.dUc, duc, rowU, nFp, rowU, eb * nF, nFp)) return false;
+    return true;
   }
   double *detTma = nullptr, *jgTma = nullptr;
   float *detTma32 = nullptr, *jgTma32 = nullptr;
 
   bool build_tma() {
     return build_maps<double>(tm, frk::tma_elems_per_block<double>(nDims, in.order), U, U0, acc, nullptr, Fn, Ufpts,
-                              detJ, JGinv, detTma, jgTma);
+                              detJ, JGinv, detTma, jgTma, dUs, dUc, dUf);
   }
   bool build_tma32(int v) {
     return build_maps<float>(f32.tm, frk::tma_elems_per_block<float>(nDims, in.order, v), f32.U, f32.U0, f32.acc,
-                             f32.comp, f32.Fn, f32.Ufpts, f32.detJ, f32.JGinv, detTma32, jgTma32);
+                             f32.comp, f32.Fn, f32.Ufpts, f32.detJ, f32.JGinv, detTma32, jgTma32, f32.dUs, f32.dUc,
+                             f32.dUf);
   }
 
   // Merge the host data of several same-order cases along the element axis
@@ -968,7 +987,10 @@ struct fr_case {
     g.dUf = dUf;
     g.sStride = (long long)nS * E * nF;
     g.fStride = (long long)nFp * E * nF;
-    frk::launch_elem_grad(nDims, in.order, g, tp, stream);
+    if (useTma)
+      frk::launch_elem_grad_tma<double>(nDims, in.order, E, tp, tm, devErr, stream);
+    else
+      frk::launch_elem_grad(nDims, in.order, g, tp, stream);
     frk::launch_faces_visc(nDims, ft, Ufpts, dUf, g.fStride, Fn, waveSp, ph, stream);
     launches += 2 * nk + 1;
   }
@@ -989,12 +1011,17 @@ struct fr_case {
     g.dUf = f32.dUf;
     g.sStride = (long long)nS * E * nF;
     g.fStride = (long long)nFp * E * nF;
-    frk::launch_elem_grad<float>(nDims, in.order, g, f32.tp, stream);
+    if (f32.useTma)
+      frk::launch_elem_grad_tma<float>(nDims, in.order, E, f32.tp, f32.tm, devErr, stream);
+    else
+      frk::launch_elem_grad<float>(nDims, in.order, g, f32.tp, stream);
     frk::launch_faces_visc<float>(nDims, f32.ft, f32.Ufpts, f32.dUf, g.fStride, f32.Fn, waveSp, ph, stream);
     launches += 2 * nk + 1;
   }
   void element(const frk::ElemArgs &a) {
-    if (in.viscous)
+    if (in.viscous && useTma)
+      frk::launch_element_stage_tma_visc<double>(nDims, in.order, a, tp, tm, stream);
+    else if (in.viscous)
       frk::launch_element_stage_tp_visc<double>(nDims, in.order, a, tp, stream);
     else if (useTma)
       frk::launch_element_stage_tma<double>(nDims, in.order, a, tp, tm, stream);
@@ -1013,7 +1040,9 @@ struct fr_case {
       frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
   }
   void element32(const frk::ElemArgsT<float> &a) {
-    if (in.viscous)
+    if (in.viscous && f32.useTma)
+      frk::launch_element_stage_tma_visc<float>(nDims, in.order, a, f32.tp, f32.tm, stream);
+    else if (in.viscous)
       frk::launch_element_stage_tp_visc<float>(nDims, in.order, a, f32.tp, stream);
     else if (f32.useTma)
       launch_tma32(a, f32.variant);

@@ -136,6 +136,10 @@ struct TmaMaps {
   CUtensorMap J;      // [nDims][nS][E*nDims]
   CUtensorMap det;    // [nS][E]
   CUtensorMap comp;   // [nS][E*nF]    precision form: rounding remainder of U
+  // viscous stages
+  CUtensorMap dUs;    // [nDims][nS][E*nF]   physical gradient at the solution points
+  CUtensorMap dUc;    // [nFp][E*nF]         LDG jumps
+  CUtensorMap dUf;    // [nDims][nFp][E*nF]  gradient at the flux points
 };
 // Elements per CTA of the TMA kernel for (nDims, order, working type); the
 // precision form has several instantiations (tile shapes) and `variant`
@@ -148,6 +152,16 @@ size_t tma_smem_bytes(int nDims, int order, int variant = 0);
 template <typename R>
 void launch_element_stage_tma(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
                               const TmaMaps &m, cudaStream_t st, int variant = 0);
+// The same with the viscous flux added at the solution points; the gradient
+// tiles (TmaMaps::dUs) arrive by TMA.  Tile variant 0.
+template <typename R>
+void launch_element_stage_tma_visc(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
+                                   const TmaMaps &m, cudaStream_t st);
+// Corrected physical gradient at the solution and flux points with TMA tiles
+// (U, dUc, JGinv, detJ in; dUs, dUf out), element block of tile variant 0.
+template <typename R>
+void launch_elem_grad_tma(int nDims, int order, int E, const TpTablesT<R> &t, const TmaMaps &m,
+                          unsigned int *err, cudaStream_t st);
 // 2-D precision-form element stage on the tensor cores (tcgen05 kind::tf32,
 // 3xTF32), 32 elements per CTA; the tile variant after the CUDA-core ones.
 // The operators are packed once on the host into the MMA operand layout.

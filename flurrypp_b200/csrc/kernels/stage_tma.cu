@@ -89,7 +89,7 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
-template <int ND, int P, typename R, int V>
+template <int ND, int P, typename R, int V, bool VISC>
 __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a, TpTablesT<R> t,
                                                                   const __grid_constant__ TmaMaps mp) {
   using T = Tm<ND, P, R, V>;
@@ -141,9 +141,12 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
   }
   __syncthreads();
   if (tid == 0) {
-    mbar_arrive_expect_tx(&bar[0], sizeof(R) * (NS * ROW + ND * NS * EB * ND));
+    mbar_arrive_expect_tx(&bar[0], sizeof(R) * (NS * ROW + ND * NS * EB * ND + (VISC ? ND * NS * ROW : 0)));
     tma_load_2d(sU, &mp.U, e0 * NF, 0, &bar[0]);
     tma_load_3d(sJ, &mp.J, e0 * ND, 0, 0, &bar[0]);
+    // viscous: the physical gradient lands in the flux tile, which the flux
+    // phase then overwrites point by point
+    if (VISC) tma_load_3d(sF, &mp.dUs, e0 * NF, 0, 0, &bar[0]);
     uint32_t bytes = sizeof(R) * NFP * ROW;
     if (needU0) bytes += sizeof(R) * NS * ROW;
     if (needAcc) bytes += sizeof(R) * NS * ROW;
@@ -187,6 +190,20 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     const R *u = &sU[s * ROW + el * NF];
     if (valid) {
       inviscid_flux<ND, R>(u, Fp, R(a.gamma));
+      if (VISC) {
+        // physical viscous flux added to the physical inviscid flux
+        // (reference: solver.cpp:777-811)
+        R gU[ND][NF], Fv[ND][NF];
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+#pragma unroll
+          for (int k = 0; k < NF; k++) gU[d][k] = sF[(d * NS + s) * ROW + el * NF + k];
+        viscous_flux<ND, R>(u, gU, a.ph, Fv);
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+#pragma unroll
+          for (int k = 0; k < NF; k++) Fp[d][k] = Fv[d][k] + Fp[d][k];
+      }
     } else {
 #pragma unroll
       for (int d = 0; d < ND; d++)
@@ -369,16 +386,16 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
   }
 }
 
-template <int ND, int P, typename R, int V>
+template <int ND, int P, typename R, int V, bool VISC = false>
 void launch_tma(const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m, cudaStream_t st) {
   using T = Tm<ND, P, R, V>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_elem_tma<ND, P, R, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    cudaFuncSetAttribute(k_elem_tma<ND, P, R, V, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
   int g = (a.E + T::EB - 1) / T::EB;
-  k_elem_tma<ND, P, R, V><<<g, T::NT, T::SMEM, st>>>(a, t, m);
+  k_elem_tma<ND, P, R, V, VISC><<<g, T::NT, T::SMEM, st>>>(a, t, m);
 }
 
 // (nDims, order) -> compile-time case; variants only for the precision form
@@ -409,7 +426,219 @@ void launch_v(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t
 #undef FR_TM_CASE
 }
 
+
+// Corrected, physical solution gradient at the solution points and its
+// extrapolation to the flux points (reference: solver.cpp:1060-1158), one
+// thread per (solution point, element) of a block of EB elements, all tiles
+// moved by TMA: U, the LDG jumps dUc, JGinv and detJ in; dU_spts and dU_fpts
+// out.  Same sums, in the same order, as k_elem_grad.
+template <int ND, int P, typename R>
+struct Tg2 {
+  using T = Tm<ND, P, R, 0>;
+  static constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  static constexpr int AL = T::AL;
+  static constexpr int al(int n) { return (n + AL - 1) / AL * AL; }
+  static constexpr int O_U = 0;
+  static constexpr int O_C = O_U + al(NS * ROW);
+  static constexpr int O_J = O_C + al(NFP * ROW);
+  static constexpr int O_DET = O_J + al(ND * NS * EB * ND);
+  static constexpr int O_G = O_DET + al(NS * EB);
+  static constexpr int O_GF = O_G + al(ND * NS * ROW);
+  static constexpr int O_TAB = O_GF + al(ND * NFP * ROW);
+  static constexpr int O_CV = O_TAB + al(N * N + 2 * N);
+  static constexpr int O_IDX = O_CV + al(NS * 2 * ND);
+  static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1);
+  static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
+  static_assert(SMEM <= kMaxSmem, "gradient tile set does not fit in shared memory");
+};
+
+template <int ND, int P, typename R>
+__global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT<R> t, unsigned int *err,
+                                                                const __grid_constant__ TmaMaps mp) {
+  using T = Tg2<ND, P, R>;
+  constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  extern __shared__ __align__(128) unsigned char smem_bytes[];
+  R *smem = reinterpret_cast<R *>((reinterpret_cast<uintptr_t>(smem_bytes) + 127) & ~uintptr_t(127));
+  R *sU = smem + T::O_U;
+  R *sC = smem + T::O_C;      // [NFP][ROW] LDG jumps
+  R *sJ = smem + T::O_J;      // [ND][NS][EB*ND]
+  R *sDet = smem + T::O_DET;  // [NS][EB]
+  R *sG = smem + T::O_G;      // [ND][NS][ROW] physical gradient
+  R *sGf = smem + T::O_GF;    // [ND][NFP][ROW] at the flux points
+  R *sD = smem + T::O_TAB;
+  R *sE = sD + N * N;
+  R *sCV = smem + T::O_CV;
+  int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);
+  int *sCF = sLine + NFP;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::O_BAR);
+
+  const int e0 = blockIdx.x * EB;
+  const int nValid = min(EB, E - e0);
+  const int tid = threadIdx.x;
+  const int s = tid / EB, el = tid - (tid / EB) * EB;
+  const bool valid = el < nValid;
+
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar[0], sizeof(R) * (NS * ROW + NFP * ROW + ND * NS * EB * ND + NS * EB));
+    tma_load_2d(sU, &mp.U, e0 * NF, 0, &bar[0]);
+    tma_load_2d(sC, &mp.dUc, e0 * NF, 0, &bar[0]);
+    tma_load_3d(sJ, &mp.J, e0 * ND, 0, 0, &bar[0]);
+    tma_load_2d(sDet, &mp.det, e0, 0, &bar[0]);
+  }
+  for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
+  for (int i = tid; i < 2 * N; i += NT) sE[i] = t.E1[i];
+  for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
+  for (int i = tid; i < NS * 2 * ND; i += NT) {
+    sCF[i] = t.corrFpt[i];
+    sCV[i] = t.corrVal[i];
+  }
+  const bool ok = __syncthreads_and(mbar_wait_bounded(&bar[0], 0, 1u << 22));
+  if (!ok) {
+    if (tid == 0 && err) atomicOr(err, 1);
+    mbar_wait_bounded(&bar[0], 0, 1u << 22);
+    return;
+  }
+
+  R J[ND][ND];
+#pragma unroll
+  for (int d1 = 0; d1 < ND; d1++)
+#pragma unroll
+    for (int d2 = 0; d2 < ND; d2++) J[d1][d2] = valid ? sJ[(d1 * NS + s) * EB * ND + el * ND + d2] : R(0.0);
+  const R invDet = valid ? R(1.) / sDet[s * EB + el] : R(0.0);
+  int idx3[3];
+  idx3[0] = s % N;
+  idx3[1] = ND > 1 ? (s / N) % N : 0;
+  idx3[2] = ND > 2 ? s / (N * N) : 0;
+  R gr[ND][NF];
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
+    const int base = s - idx3[d] * stride;
+    const R *Dr = &sD[idx3[d] * N];
+    R acc[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+#pragma unroll
+    for (int m = 0; m < N; m++) {
+      const R dv = Dr[m];
+      const R *x = &sU[(base + m * stride) * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
+    }
+    // + opp_correctU[d] . dUc: the faces normal to d, ascending
+    R cq[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) cq[k] = R(0.0);
+#pragma unroll
+    for (int fc = 0; fc < 2 * ND; fc++) {
+      const int fp = sCF[s * 2 * ND + fc];
+      const int ln = sLine[fp];
+      if (((ln >> 16) & 0xf) != d) continue;
+      const R cv = sCV[s * 2 * ND + fc] * ((ln >> 20) ? R(1.0) : -R(1.0));
+      const R *x = &sC[fp * ROW + el * NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) gr[d][k] = cq[k] + acc[k];
+  }
+  // physical gradient (solver.cpp:1101-1134)
+#pragma unroll
+  for (int d2 = 0; d2 < ND; d2++)
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      R v = gr[0][k] * J[0][d2] + gr[1][k] * J[1][d2];
+      if (ND == 3) v = gr[0][k] * J[0][d2] + gr[1][k] * J[1][d2] + gr[ND - 1][k] * J[ND - 1][d2];
+      v = invDet * v;
+      sG[(d2 * NS + s) * ROW + el * NF + k] = v;
+    }
+  fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_3d(&mp.dUs, e0 * NF, 0, 0, sG);
+    tma_commit();
+  }
+  for (int it = tid; it < NFP * EB; it += NT) {
+    const int f = it / EB, fe = it - (it / EB) * EB;
+    const int ln = sLine[f];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
+    const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      R acc[NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+#pragma unroll
+      for (int m = 0; m < N; m++) {
+        const R ev = sE[side * N + m];
+        const R *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+      }
+#pragma unroll
+      for (int k = 0; k < NF; k++) sGf[(d * NFP + f) * ROW + fe * NF + k] = acc[k];
+    }
+  }
+  fence_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_3d(&mp.dUf, e0 * NF, 0, 0, sGf);
+    tma_commit();
+    tma_wait_read_all();
+  }
+}
+
+template <int ND, int P, typename R>
+void launch_grad(int E, const TpTablesT<R> &t, const TmaMaps &m, unsigned int *err, cudaStream_t st) {
+  using T = Tg2<ND, P, R>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_grad_tma<ND, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    attr = true;
+  }
+  k_grad_tma<ND, P, R><<<(E + T::EB - 1) / T::EB, T::NT, T::SMEM, st>>>(E, t, err, m);
+}
+
+template <typename R>
+void launch_v_visc(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m,
+                   cudaStream_t st) {
+#define FR_TMV_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_tma<ND, P, R, 0, true>(a, t, m, st);
+  FR_TM_ORDERS(FR_TMV_CASE)
+#undef FR_TMV_CASE
+}
+
 }  // namespace
+
+template <typename R>
+void launch_element_stage_tma_visc(int nDims, int order, const ElemArgsT<R> &a, const TpTablesT<R> &t,
+                                   const TmaMaps &m, cudaStream_t st) {
+  if (a.E <= 0) return;
+  launch_v_visc<R>(nDims, order, a, t, m, st);
+}
+template void launch_element_stage_tma_visc<double>(int, int, const ElemArgsT<double> &, const TpTablesT<double> &,
+                                                    const TmaMaps &, cudaStream_t);
+template void launch_element_stage_tma_visc<float>(int, int, const ElemArgsT<float> &, const TpTablesT<float> &,
+                                                   const TmaMaps &, cudaStream_t);
+
+template <typename R>
+void launch_elem_grad_tma(int nDims, int order, int E, const TpTablesT<R> &t, const TmaMaps &m, unsigned int *err,
+                          cudaStream_t st) {
+  if (E <= 0) return;
+#define FR_TG_CASE(ND, P) \
+  if (nDims == ND && order == P) return launch_grad<ND, P, R>(E, t, m, err, st);
+  FR_TM_ORDERS(FR_TG_CASE)
+#undef FR_TG_CASE
+}
+template void launch_elem_grad_tma<double>(int, int, int, const TpTablesT<double> &, const TmaMaps &, unsigned int *,
+                                           cudaStream_t);
+template void launch_elem_grad_tma<float>(int, int, int, const TpTablesT<float> &, const TmaMaps &, unsigned int *,
+                                          cudaStream_t);
 
 int tma_variants(bool fp32) { return fp32 ? kFp32Variants : 1; }
 

@@ -71,6 +71,12 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int x, int 
                : "memory");
 }
 
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, int x, int y, int z, const void *src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map), "r"(x),
+               "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
 // Waits until the shared-memory sources of all committed stores have been read.
