@@ -28,11 +28,11 @@ each beside its plain-FP64 counterpart:
                    RK4 steps: precision form batched (one launch per stage
                    per order, graph-captured step) vs the plain FP64 path
                    case by case, with the L2 error of every case;
-  serve            a Poisson stream of channel-over-bump steady solves
-                   (h~U(0.02,0.1), nx~U{24..96}, ny=nx/3, P~U{1..4},
+  serve            Poisson streams (rates swept) of channel-over-bump steady
+                   solves (h~U(0.02,0.1), nx~U{24..96}, ny=nx/3, P~U{1..4},
                    Mach~U(0.2,0.5), local-CFL RK4 + P-multigrid, residual
                    drop 1e-8) through the solve server: solves/s, p50/p99
-                   latency, vs the same solves one after another.
+                   latency, vs a sample of the same solves one at a time.
 """
 from __future__ import annotations
 
@@ -372,16 +372,17 @@ def form_serve(args, fb, torch):
         M = float(rng.uniform(0.2, 0.5))
         msh = os.path.join(tmp, f"bump{i}.msh")
         write_gmsh(msh, channel_bump(nx, nx // 3, h))
-        reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), nx, P))
-    gaps = rng.exponential(1.0 / args.serve_rate, len(reqs))
+        dof = nx * (nx // 3) * (P + 1) ** 2 * 4
+        reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), dof))
 
-    def serve(max_inflight, paced):
+    def serve(subset, max_inflight, rate):
         srv = fb.Server(budget_bytes=args.serve_budget_gb << 30, max_inflight=max_inflight, check_every=10)
+        gaps = np.random.default_rng(args.serve_seed + 1).exponential(1.0 / rate, len(subset)) if rate else None
         t0 = time.perf_counter()
         ids = []
-        for (deck, nx, P), g in zip(reqs, gaps):
-            if paced:
-                time.sleep(g)
+        for k, (deck, dof) in enumerate(subset):
+            if rate:
+                time.sleep(float(gaps[k]))
             ids.append(srv.submit(deck, tol=1e-8, max_steps=args.serve_max_steps))
         polls = []
         for r in ids:
@@ -392,23 +393,31 @@ def form_serve(args, fb, torch):
             polls.append(srv.poll(r))
         sec = time.perf_counter() - t0
         srv.close()
-        lat = sorted(p["latency_s"] for p in polls)
+        lat = [p["latency_s"] for p in polls]
         done = [p for p in polls if p["status"] == 2]
+        stages = sum(4 * p["steps"] * dof for p, (_, dof) in zip(polls, subset))
         return {"solves_per_s": len(done) / sec, "seconds": sec, "completed": len(done),
                 "converged_1e-8": sum(1 for p in done if p["res_ratio"] <= 1e-8),
+                "median_residual_drop": float(np.median([p["res_ratio"] for p in done])) if done else None,
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-                "steps_mean": float(np.mean([p["steps"] for p in polls]))}
+                "steps_mean": float(np.mean([p["steps"] for p in polls])),
+                "fine_dof_stage_per_s": stages / sec}
 
-    stream_res = serve(args.serve_inflight, True)
-    seq = serve(1, False)
+    sweep = {}
+    for rate in args.serve_rates:
+        sweep[f"rate_{rate:g}_per_s"] = dict(max_inflight=args.serve_inflight, **serve(reqs, args.serve_inflight, rate))
+    k = min(args.serve_alone, len(reqs))
+    alone = serve(reqs[:k], 1, 0.0)
+    alone["sample"] = f"the first {k} requests, submitted together, one in flight"
+    best = max(v["solves_per_s"] for v in sweep.values())
     return {
-        "workload": (f"{len(reqs)} channel-over-bump requests, seed {args.serve_seed}, Poisson rate "
-                     f"{args.serve_rate}/s, h~U(0.02,0.1), nx~U{{24..96}}, ny=nx/3, P~U{{1..4}}, Mach~U(0.2,0.5), "
-                     "local-CFL RK4 + P-multigrid (lowOrder 0, 2 smoothing steps), residual drop 1e-8 "
-                     f"(at most {args.serve_max_steps} steps), FP64"),
-        "served": dict(max_inflight=args.serve_inflight, **stream_res),
-        "one_at_a_time": seq,
-        "speedup_solves_per_s": stream_res["solves_per_s"] / max(seq["solves_per_s"], 1e-30),
+        "workload": (f"{len(reqs)} channel-over-bump requests, seed {args.serve_seed}, Poisson arrivals, "
+                     "h~U(0.02,0.1), nx~U{24..96}, ny=nx/3, P~U{1..4}, Mach~U(0.2,0.5), local-CFL RK4 + "
+                     "P-multigrid (lowOrder 0, 2 smoothing steps), run to a residual drop of 1e-8 "
+                     f"(at most {args.serve_max_steps} steps), FP64, programmatic dependent launch"),
+        "sweep": sweep,
+        "one_at_a_time": alone,
+        "speedup_solves_per_s": best / max(alone["solves_per_s"], 1e-30),
     }
 
 
@@ -501,11 +510,12 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--batch-seed", type=int, default=2024)
     ap.add_argument("--alone-steps", type=int, default=20)
-    ap.add_argument("--serve-requests", type=int, default=8)
-    ap.add_argument("--serve-rate", type=float, default=4.0)
+    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[2.0, 32.0])
+    ap.add_argument("--serve-alone", type=int, default=3)
     ap.add_argument("--serve-seed", type=int, default=7)
-    ap.add_argument("--serve-max-steps", type=int, default=2000)
-    ap.add_argument("--serve-inflight", type=int, default=8)
+    ap.add_argument("--serve-max-steps", type=int, default=3000)
+    ap.add_argument("--serve-inflight", type=int, default=16)
     ap.add_argument("--serve-budget-gb", type=int, default=64)
     ap.add_argument("--profile", default="", help="comma list of PROFILE_CASES: one element stage and one "
                     "face pass each between cudaProfilerStart/Stop, then exit")

@@ -59,6 +59,7 @@ class SetupOpts(ctypes.Structure):
         ("no_tma", ctypes.c_int),
         ("tile_variant", ctypes.c_int),
         ("no_tensor_cores", ctypes.c_int),
+        ("no_pdl", ctypes.c_int),
     ]
 
 

@@ -20,6 +20,7 @@
 
 #include "../../include/fr_b200.h"
 #include "host/fr_host.hpp"
+#include "kernels/launch.cuh"
 #include "kernels/stage.hpp"
 
 namespace {
@@ -84,6 +85,9 @@ struct fr_case {
   // the boundary copy, and detJ, norm, dA, waveSp, the time step and the
   // norm reductions stay FP64
   bool mixed = false;
+  // programmatic dependent launch for cases whose grids fit in about one wave
+  // (a solution point per thread: 148 SMs x 1024 threads)
+  bool usePdl = false;
   struct Fp32 {
     float *U = nullptr, *U0 = nullptr, *acc = nullptr, *comp = nullptr, *Ufpts = nullptr, *Fn = nullptr;
     float *JGinv = nullptr, *detJ = nullptr;
@@ -325,6 +329,7 @@ struct fr_case {
       }
     }
     if (!alloc(devErr, 1)) return false;
+    usePdl = !opts.no_pdl && (long long)nS * E <= 148LL * 1024;
     if (!mixed) {
       useTma = useTp && !opts.no_tma && build_tma();
       if (useTma && in.viscous) EB = frk::tma_elems_per_block<double>(nDims, in.order);
@@ -1203,6 +1208,13 @@ struct fr_batch {
 
 namespace {
 
+// launch policy of a case's calls: PDL on for small cases, restored on exit
+struct PdlScope {
+  bool prev;
+  explicit PdlScope(const fr_case *c) : prev(frk::pdl_enabled()) { frk::set_pdl(c && c->usePdl); }
+  ~PdlScope() { frk::set_pdl(prev); }
+};
+
 int status_of(fr_case *c, bool ok, int code = FR_ERR_CUDA) {
   if (ok) return FR_OK;
   if (c->err.find("cudaMalloc") != std::string::npos) return FR_ERR_CUDA;
@@ -1400,6 +1412,7 @@ int fr_set_stream(fr_case *c, void *stream) {
 }
 
 int fr_init_solution(fr_case *c, int kind, const double *prm, int nprm) {
+  PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;
   if (!c->U) {
     c->err = "host-only case: no device state";
@@ -1415,6 +1428,7 @@ int fr_init_solution(fr_case *c, int kind, const double *prm, int nprm) {
 }
 
 int fr_set_state(fr_case *c, const double *U, size_t count) {
+  PdlScope pdlScope(c);
   if (!c || !U) return FR_ERR_ARG;
   if (!c->U) {
     c->err = "host-only case: no device state";
@@ -1437,6 +1451,7 @@ int fr_set_state(fr_case *c, const double *U, size_t count) {
 }
 
 int fr_get_state(fr_case *c, double *U, size_t count) {
+  PdlScope pdlScope(c);
   if (!c || !U) return FR_ERR_ARG;
   size_t n = (size_t)c->nS * c->E * c->nF;
   if (count != n) {
@@ -1448,6 +1463,7 @@ int fr_get_state(fr_case *c, double *U, size_t count) {
 }
 
 int fr_calc_residual(fr_case *c, int step) {
+  PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;
   if (c->hostOnly) {
     c->err = "host-only case: no device state";
@@ -1473,6 +1489,7 @@ int fr_get_residual(fr_case *c, int step, double *divF, size_t count) {
 }
 
 int fr_update(fr_case *c, int pmg_source) {
+  PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;
   if (c->hostOnly) {
     c->err = "host-only case: no device state";
@@ -1487,6 +1504,7 @@ int fr_update(fr_case *c, int pmg_source) {
 }
 
 int fr_pmg_cycle(fr_case *c) {
+  PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;
   if (c->hostOnly || !c->stateSet) {
     c->err = "no device state";
@@ -1497,6 +1515,7 @@ int fr_pmg_cycle(fr_case *c) {
 }
 
 int fr_run(fr_case *c, int nsteps) {
+  PdlScope pdlScope(c);
   if (!c || nsteps < 0) return FR_ERR_ARG;
   if (c->hostOnly) {
     c->err = "host-only case: no device state";
@@ -1507,6 +1526,7 @@ int fr_run(fr_case *c, int nsteps) {
 }
 
 int fr_calc_dt(fr_case *c, double *dtOut) {
+  PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;
   if (c->hostOnly) {
     c->err = "host-only case: no device state";
@@ -1547,6 +1567,7 @@ int fr_set_dt(fr_case *c, double dt) {
 }
 
 int fr_residual_norm(fr_case *c, int resType, double *out, int nFields) {
+  PdlScope pdlScope(c);
   if (!c || !out || nFields != c->nF || resType < 1 || resType > 3) return FR_ERR_ARG;
   if (c->hostOnly) {
     c->err = "host-only case: no device state";
@@ -1577,6 +1598,7 @@ int fr_residual_norm(fr_case *c, int resType, double *out, int nFields) {
 }
 
 int fr_check_state(fr_case *c) {
+  PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;
   if (c->hostOnly) {
     c->err = "host-only case: no device state";
@@ -1598,6 +1620,7 @@ int fr_check_state(fr_case *c) {
 }
 
 int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
+  PdlScope pdlScope(c);
   if (!c || !name || !count) return FR_ERR_ARG;
   std::string n = name;
   size_t nU = (size_t)c->nS * c->E * c->nF, nUf = (size_t)c->nFp * c->E * c->nF;
@@ -1738,6 +1761,7 @@ int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes) {
 }
 
 int fr_bench_kernel(fr_case *c, const char *kernel, int reps) {
+  PdlScope pdlScope(c);
   if (!c || !kernel || reps < 0) return FR_ERR_ARG;
   if (c->hostOnly || !c->stateSet) {
     c->err = "no device state";
@@ -1804,11 +1828,13 @@ int fr_batch_create(fr_case *const *cases, int n, fr_batch **out) {
 
 int fr_batch_run(fr_batch *b, int nsteps) {
   if (!b || nsteps < 0) return FR_ERR_ARG;
-  for (auto &g : b->groups)
+  for (auto &g : b->groups) {
+    PdlScope pdlScope(g.get());
     if (!g->run(nsteps)) {
       b->err = g->err;
       return FR_ERR_CUDA;
     }
+  }
   for (auto &g : b->groups)
     if (!g->sync()) {
       b->err = g->err;

@@ -1,0 +1,47 @@
+// Kernel launches with programmatic dependent launch (PDL) for small cases.
+//
+// A small case (a served request, a P-multigrid coarse level) runs hundreds
+// of kernels per step, each a few microseconds long, so the gaps between
+// dependent launches dominate.  With PDL a kernel may be launched while its
+// predecessor on the stream is still finishing: every kernel of this library
+// calls pdl_wait() before it touches global memory (it returns once the
+// predecessor grid has completed and its writes are visible) and then
+// pdl_trigger(), which lets its own successor start launching.  Launched
+// without the PDL attribute both are no-ops.  The attribute is set only for
+// cases whose grids fit in about one wave (set_pdl), where an early successor
+// cannot take SM slots from later waves of its predecessor.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <utility>
+
+namespace frk {
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Launch policy of the calling host thread (set by the case around its
+// launch sequences, graph captures included).
+void set_pdl(bool on);
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args &&...args) {
+  if (!pdl_enabled()) {
+    k<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
+}  // namespace frk

@@ -15,15 +15,25 @@
 // reference's dense cblas_dgemm without changing any sum.
 #include <cstdio>
 
+#include "launch.cuh"
 #include "stage.hpp"
 
 namespace frk {
+
+namespace {
+thread_local bool g_pdl = false;
+}  // namespace
+
+void set_pdl(bool on) { g_pdl = on; }
+bool pdl_enabled() { return g_pdl; }
 
 namespace {
 
 __global__ void k_apply_op(int nRows, const int *__restrict__ rp, const int *__restrict__ ci,
                            const double *__restrict__ v, const double *__restrict__ in,
                            double *__restrict__ out, long long N, double alpha, double beta) {
+  pdl_wait();
+  pdl_trigger();
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int r = blockIdx.y;
   if (n >= N || r >= nRows) return;
@@ -42,6 +52,8 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
                                                         const R *__restrict__ dAL, const R *__restrict__ dAR,
                                                         const R *__restrict__ Uf, R *__restrict__ Fn,
                                                         double *__restrict__ waveSp, R gam, int roe) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -73,6 +85,8 @@ template <int ND, typename R>
 __global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
                                  const R *__restrict__ nrm, const R *__restrict__ dAL, const R *__restrict__ Uf,
                                  R *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -100,6 +114,8 @@ __device__ __forceinline__ double csr_dot(const Csr &A, int row, const double *_
 
 template <int ND>
 __global__ void __launch_bounds__(256) k_element_stage(ElemArgs a) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   extern __shared__ double smem[];
   const int EB = a.EB, nS = a.nS, nFp = a.nFp, E = a.E;
@@ -235,6 +251,8 @@ __global__ void __launch_bounds__(256) k_element_stage(ElemArgs a) {
 template <int ND, typename R>
 __global__ void k_wavesp_init(int nFp, int E, const R *__restrict__ Uf, const double *__restrict__ norm, double gam,
                               double *__restrict__ waveSp) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)nFp * E) return;
@@ -258,6 +276,8 @@ __global__ void k_element_dt(int nS, int nFp, int nPF, int E, const double *__re
                              const double *__restrict__ waveSp, const double *__restrict__ dA,
                              double cflFac, double *__restrict__ eleDt,
                              unsigned long long *dtMinBits) {
+  pdl_wait();
+  pdl_trigger();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
   double vol = 0;
@@ -272,19 +292,27 @@ __global__ void k_element_dt(int nS, int nFp, int nPF, int E, const double *__re
 }
 
 __global__ void k_reset_min(unsigned long long *bits) {
+  pdl_wait();
+  pdl_trigger();
   *bits = (unsigned long long)__double_as_longlong(__longlong_as_double(0x7ff0000000000000ll));
 }
 
 __global__ void k_store_min(const unsigned long long *bits, double *dt, double *time_acc) {
+  pdl_wait();
+  pdl_trigger();
   *dt = __longlong_as_double((long long)*bits);
   (void)time_acc;
 }
 
-__global__ void k_add_time(const double *dt, double *time_acc) { *time_acc += *dt; }
+__global__ void k_add_time(const double *dt, double *time_acc) {
+  pdl_wait();
+  pdl_trigger(); *time_acc += *dt; }
 
 template <typename R>
 __global__ void k_residual_norm(int nS, int E, int nF, const R *__restrict__ divF, const double *__restrict__ detJ,
                                 const double *__restrict__ w, int resType, double *__restrict__ eleRes) {
+  pdl_wait();
+  pdl_trigger();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
   for (int k = 0; k < nF; k++) {
@@ -304,6 +332,8 @@ __global__ void k_residual_norm(int nS, int E, int nF, const R *__restrict__ div
 
 __global__ void k_add(long long n, double *__restrict__ out, const double *__restrict__ x,
                       const double *__restrict__ y, double sgn) {
+  pdl_wait();
+  pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   out[i] = sgn > 0 ? x[i] + y[i] : x[i] - y[i];
@@ -311,6 +341,8 @@ __global__ void k_add(long long n, double *__restrict__ out, const double *__res
 
 template <typename R>
 __global__ void k_check_state(long long n, int nF, const R *__restrict__ U, unsigned int *bad) {
+  pdl_wait();
+  pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   R v = U[i];
@@ -322,6 +354,8 @@ __global__ void k_check_state(long long n, int nF, const R *__restrict__ U, unsi
 template <typename R>
 __global__ void k_apply_op_t(int nRows, const int *__restrict__ rp, const int *__restrict__ ci,
                              const double *__restrict__ v, const R *__restrict__ in, R *__restrict__ out, long long N) {
+  pdl_wait();
+  pdl_trigger();
   long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int r = blockIdx.y;
   if (n >= N || r >= nRows) return;
@@ -332,6 +366,8 @@ __global__ void k_apply_op_t(int nRows, const int *__restrict__ rp, const int *_
 
 __global__ void k_split(long long n, const double *__restrict__ U64, float *__restrict__ U32,
                         float *__restrict__ comp) {
+  pdl_wait();
+  pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double u = U64[i];
@@ -342,17 +378,23 @@ __global__ void k_split(long long n, const double *__restrict__ U64, float *__re
 
 __global__ void k_join(long long n, const float *__restrict__ U32, const float *__restrict__ comp,
                        double *__restrict__ U64) {
+  pdl_wait();
+  pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   U64[i] = (double)U32[i] + (double)comp[i];
 }
 
 __global__ void k_narrow(long long n, const double *__restrict__ in, float *__restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = __double2float_rn(in[i]);
 }
 
 __global__ void k_widen(long long n, const float *__restrict__ in, double *__restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (double)in[i];
 }
@@ -363,14 +405,14 @@ void launch_apply_op(const Csr &A, const double *in, double *out, long long N, d
                      double beta, cudaStream_t st) {
   if (N <= 0 || A.nRows <= 0) return;
   dim3 g((unsigned)((N + 255) / 256), (unsigned)A.nRows);
-  k_apply_op<<<g, 256, 0, st>>>(A.nRows, A.rowptr, A.col, A.val, in, out, N, alpha, beta);
+  launch_k(k_apply_op, g, 256, 0, st, A.nRows, A.rowptr, A.col, A.val, in, out, N, alpha, beta);
 }
 
 template <typename R>
 void launch_apply_op_t(const Csr &A, const R *in, R *out, long long N, cudaStream_t st) {
   if (N <= 0 || A.nRows <= 0) return;
   dim3 g((unsigned)((N + 255) / 256), (unsigned)A.nRows);
-  k_apply_op_t<R><<<g, 256, 0, st>>>(A.nRows, A.rowptr, A.col, A.val, in, out, N);
+  launch_k(k_apply_op_t<R>, g, 256, 0, st, A.nRows, A.rowptr, A.col, A.val, in, out, N);
 }
 
 template <typename R>
@@ -381,18 +423,18 @@ void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R
   if (nI > 0) {
     const int g = (nI + b - 1) / b;
     if (nDims == 2)
-      k_faces_interior<2, R><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
+      launch_k(k_faces_interior<2, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
                                               R(ph.gamma), ph.riemannType == 1);
     else
-      k_faces_interior<3, R><<<g, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
+      launch_k(k_faces_interior<3, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
                                               R(ph.gamma), 0);
   }
   if (nB > 0) {
     const int g = (nB + b - 1) / b;
     if (nDims == 2)
-      k_faces_boundary<2, R><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
+      launch_k(k_faces_boundary<2, R>, g, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
     else
-      k_faces_boundary<3, R><<<g, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
+      launch_k(k_faces_boundary<3, R>, g, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts, Fn, waveSp, ph);
   }
 }
 
@@ -407,10 +449,10 @@ void launch_element_stage(int nDims, const ElemArgs &a, cudaStream_t st) {
   size_t sm = elem_smem_bytes(nDims, a.nS, a.nFp, a.EB);
   if (nDims == 2) {
     cudaFuncSetAttribute(k_element_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_element_stage<2><<<g, 256, sm, st>>>(a);
+    launch_k(k_element_stage<2>, g, 256, sm, st, a);
   } else {
     cudaFuncSetAttribute(k_element_stage<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_element_stage<3><<<g, 256, sm, st>>>(a);
+    launch_k(k_element_stage<3>, g, 256, sm, st, a);
   }
 }
 
@@ -421,9 +463,9 @@ void launch_wavesp_init(int nDims, int nFp, int E, const R *Ufpts, const double 
   if (n <= 0) return;
   unsigned g = (unsigned)((n + 255) / 256);
   if (nDims == 2)
-    k_wavesp_init<2, R><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
+    launch_k(k_wavesp_init<2, R>, g, 256, 0, st, nFp, E, Ufpts, norm, gamma, waveSp);
   else
-    k_wavesp_init<3, R><<<g, 256, 0, st>>>(nFp, E, Ufpts, norm, gamma, waveSp);
+    launch_k(k_wavesp_init<3, R>, g, 256, 0, st, nFp, E, Ufpts, norm, gamma, waveSp);
 }
 
 void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double *detJ,
@@ -432,50 +474,50 @@ void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double 
                        unsigned long long *dtMinBits, cudaStream_t st) {
   (void)nDims;
   if (E <= 0) return;
-  k_element_dt<<<(E + 127) / 128, 128, 0, st>>>(nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA,
+  launch_k(k_element_dt, (E + 127) / 128, 128, 0, st, nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA,
                                                  cflFac, eleDt, dtMinBits);
 }
 
-void launch_reset_min(unsigned long long *bits, cudaStream_t st) { k_reset_min<<<1, 1, 0, st>>>(bits); }
+void launch_reset_min(unsigned long long *bits, cudaStream_t st) { launch_k(k_reset_min, 1, 1, 0, st, bits); }
 
 void launch_store_min(const unsigned long long *bits, double *dt, double *time_acc, cudaStream_t st) {
-  k_store_min<<<1, 1, 0, st>>>(bits, dt, time_acc);
+  launch_k(k_store_min, 1, 1, 0, st, bits, dt, time_acc);
 }
 
 void launch_add_time(const double *dt, double *time_acc, cudaStream_t st) {
-  k_add_time<<<1, 1, 0, st>>>(dt, time_acc);
+  launch_k(k_add_time, 1, 1, 0, st, dt, time_acc);
 }
 
 template <typename R>
 void launch_residual_norm(int nS, int E, int nF, const R *divF, const double *detJ, const double *wSpt,
                           int resType, double *eleRes, cudaStream_t st) {
   if (E <= 0) return;
-  k_residual_norm<R><<<(E + 127) / 128, 128, 0, st>>>(nS, E, nF, divF, detJ, wSpt, resType, eleRes);
+  launch_k(k_residual_norm<R>, (E + 127) / 128, 128, 0, st, nS, E, nF, divF, detJ, wSpt, resType, eleRes);
 }
 
 void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st) {
   if (n <= 0) return;
-  k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, out, x, y, sgn);
+  launch_k(k_add, (unsigned)((n + 255) / 256), 256, 0, st, n, out, x, y, sgn);
 }
 
 template <typename R>
 void launch_check_state(int nS, int E, int nF, const R *U, unsigned int *bad, cudaStream_t st) {
   long long n = (long long)nS * E * nF;
   if (n <= 0) return;
-  k_check_state<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nF, U, bad);
+  launch_k(k_check_state<R>, (unsigned)((n + 255) / 256), 256, 0, st, n, nF, U, bad);
 }
 
 void launch_split(long long n, const double *U64, float *U32, float *comp, cudaStream_t st) {
-  if (n > 0) k_split<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, U64, U32, comp);
+  if (n > 0) launch_k(k_split, (unsigned)((n + 255) / 256), 256, 0, st, n, U64, U32, comp);
 }
 void launch_join(long long n, const float *U32, const float *comp, double *U64, cudaStream_t st) {
-  if (n > 0) k_join<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, U32, comp, U64);
+  if (n > 0) launch_k(k_join, (unsigned)((n + 255) / 256), 256, 0, st, n, U32, comp, U64);
 }
 void launch_narrow(long long n, const double *in, float *out, cudaStream_t st) {
-  if (n > 0) k_narrow<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, in, out);
+  if (n > 0) launch_k(k_narrow, (unsigned)((n + 255) / 256), 256, 0, st, n, in, out);
 }
 void launch_widen(long long n, const float *in, double *out, cudaStream_t st) {
-  if (n > 0) k_widen<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, in, out);
+  if (n > 0) launch_k(k_widen, (unsigned)((n + 255) / 256), 256, 0, st, n, in, out);
 }
 
 #define FR_BASE_INST(R)                                                                                        \

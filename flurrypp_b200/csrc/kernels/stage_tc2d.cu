@@ -25,6 +25,7 @@
 #include <cstring>
 #include <vector>
 
+#include "launch.cuh"
 #include "stage.hpp"
 #include "umma.cuh"
 
@@ -103,6 +104,8 @@ constexpr uint32_t kWait = 1u << 22;
 template <int P>
 __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const float *__restrict__ ops,
                                                    const __grid_constant__ TmaMaps mp) {
+  pdl_wait();
+  pdl_trigger();
   using T = Tc<P>;
   constexpr int NS = T::NS, NFP = T::NFP, NF = 4, EB = 32, ROW = T::ROW;
   constexpr int NSp = T::NSp, K1p = T::K1p, K2p = T::K2p, K3p = T::K3p;
@@ -356,7 +359,7 @@ void launch_tc(const ElemArgsT<float> &a, const float *ops, const TmaMaps &m, cu
     cudaFuncSetAttribute(k_elem_tc2d<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
-  k_elem_tc2d<P><<<(a.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st>>>(a, ops, m);
+  launch_k(k_elem_tc2d<P>, (a.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, a, ops, m);
 }
 
 // host TF32 rounding, nearest with ties away from zero (as cvt.rna), low 13

@@ -16,6 +16,7 @@
 // multiples of 4.
 #include <type_traits>
 
+#include "launch.cuh"
 #include "stage.hpp"
 #include "tma.cuh"
 
@@ -92,6 +93,8 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
 template <int ND, int P, typename R, int V, bool VISC>
 __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a, TpTablesT<R> t,
                                                                   const __grid_constant__ TmaMaps mp) {
+  pdl_wait();
+  pdl_trigger();
   using T = Tm<ND, P, R, V>;
   constexpr bool F32 = T::F32;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
@@ -395,7 +398,7 @@ void launch_tma(const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m, 
     attr = true;
   }
   int g = (a.E + T::EB - 1) / T::EB;
-  k_elem_tma<ND, P, R, V, VISC><<<g, T::NT, T::SMEM, st>>>(a, t, m);
+  launch_k(k_elem_tma<ND, P, R, V, VISC>, g, T::NT, T::SMEM, st, a, t, m);
 }
 
 // (nDims, order) -> compile-time case; variants only for the precision form
@@ -455,6 +458,8 @@ struct Tg2 {
 template <int ND, int P, typename R>
 __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT<R> t, unsigned int *err,
                                                                 const __grid_constant__ TmaMaps mp) {
+  pdl_wait();
+  pdl_trigger();
   using T = Tg2<ND, P, R>;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
   extern __shared__ __align__(128) unsigned char smem_bytes[];
@@ -601,7 +606,7 @@ void launch_grad(int E, const TpTablesT<R> &t, const TmaMaps &m, unsigned int *e
     cudaFuncSetAttribute(k_grad_tma<ND, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
-  k_grad_tma<ND, P, R><<<(E + T::EB - 1) / T::EB, T::NT, T::SMEM, st>>>(E, t, err, m);
+  launch_k(k_grad_tma<ND, P, R>, (E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, E, t, err, m);
 }
 
 template <typename R>

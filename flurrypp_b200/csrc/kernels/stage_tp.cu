@@ -10,6 +10,7 @@
 // nonzero terms in ascending column order.
 #include <type_traits>
 
+#include "launch.cuh"
 #include "stage.hpp"
 
 namespace frk {
@@ -40,6 +41,8 @@ __device__ __forceinline__ void two_sum_tp(float a, float b, float &s, float &e)
 
 template <int ND, int P, bool VISC, typename R>
 __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, TpTablesT<R> t) {
+  pdl_wait();
+  pdl_trigger();
   using T = Tp<ND, P, R>;
   constexpr bool F32 = std::is_same<R, float>::value;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
@@ -268,7 +271,7 @@ void launch_tp(const ElemArgsT<R> &a, const TpTablesT<R> &t, cudaStream_t st) {
     attr = true;
   }
   int g = (a.E + T::EB - 1) / T::EB;
-  k_elem_tp<ND, P, VISC, R><<<g, T::NT, T::SMEM, st>>>(a, t);
+  launch_k(k_elem_tp<ND, P, VISC, R>, g, T::NT, T::SMEM, st, a, t);
 }
 
 #define FR_TP_ORDERS(X) X(2, 0) X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 5) X(3, 0) X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 5)

@@ -8,6 +8,7 @@
 //   k_faces_visc_*  inviscid + LDG viscous common flux, times dA, at both sides
 //                   (face.cpp:163-186, 210-311; boundFace.cpp:316-350).
 // The viscous flux at the solution points is added in the element kernel.
+#include "launch.cuh"
 #include "stage.hpp"
 
 namespace frk {
@@ -27,6 +28,8 @@ template <int ND, typename R>
 __global__ void k_faces_ldg_interior(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
                                      const R *__restrict__ nrm, const R *__restrict__ Uf,
                                      R *__restrict__ dUc, R penFact) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -48,6 +51,8 @@ template <int ND, typename R>
 __global__ void k_faces_ldg_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
                                      const R *__restrict__ nrm, const R *__restrict__ Uf,
                                      R *__restrict__ dUc, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -108,6 +113,8 @@ __global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, cons
                                       const R *__restrict__ dAR, const R *__restrict__ Uf,
                                       const R *__restrict__ dUf, long long dStride, R *__restrict__ Fn,
                                       double *__restrict__ waveSp, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -146,6 +153,8 @@ __global__ void k_faces_visc_boundary(int n0, int n, const int *__restrict__ slo
                                       const R *__restrict__ dAL, const R *__restrict__ Uf,
                                       const R *__restrict__ dUf, long long dStride, R *__restrict__ Fn,
                                       double *__restrict__ waveSp, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NF = ND + 2;
   int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -221,6 +230,8 @@ struct Tg {
 
 template <int ND, int P, typename R>
 __global__ void __launch_bounds__(Tg<ND, P, R>::NT) k_elem_grad(GradArgsT<R> g, TpTablesT<R> t) {
+  pdl_wait();
+  pdl_trigger();
   using T = Tg<ND, P, R>;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
   extern __shared__ __align__(16) unsigned char smem_bytes[];
@@ -334,7 +345,7 @@ void launch_grad(const GradArgsT<R> &g, const TpTablesT<R> &t, cudaStream_t st) 
     cudaFuncSetAttribute(k_elem_grad<ND, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
-  k_elem_grad<ND, P, R><<<(g.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st>>>(g, t);
+  launch_k(k_elem_grad<ND, P, R>, (g.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, g, t);
 }
 
 }  // namespace
@@ -344,15 +355,15 @@ void launch_faces_ldg(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *dUc
   const int b = 256, nI = ft.nInterior, nB = ft.n - ft.nInterior;
   if (nI > 0) {
     if (nDims == 2)
-      k_faces_ldg_interior<2, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
+      launch_k(k_faces_ldg_interior<2, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
     else
-      k_faces_ldg_interior<3, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
+      launch_k(k_faces_ldg_interior<3, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
   }
   if (nB > 0) {
     if (nDims == 2)
-      k_faces_ldg_boundary<2, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
+      launch_k(k_faces_ldg_boundary<2, R>, (nB + b - 1) / b, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
     else
-      k_faces_ldg_boundary<3, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
+      launch_k(k_faces_ldg_boundary<3, R>, (nB + b - 1) / b, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph);
   }
 }
 
@@ -362,18 +373,18 @@ void launch_faces_visc(int nDims, const FaceTableT<R> &ft, const R *Ufpts, const
   const int b = 128, nI = ft.nInterior, nB = ft.n - ft.nInterior;
   if (nI > 0) {
     if (nDims == 2)
-      k_faces_visc_interior<2, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
+      launch_k(k_faces_visc_interior<2, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
     else
-      k_faces_visc_interior<3, R><<<(nI + b - 1) / b, b, 0, st>>>(nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
+      launch_k(k_faces_visc_interior<3, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
   }
   if (nB > 0) {
     if (nDims == 2)
-      k_faces_visc_boundary<2, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
+      launch_k(k_faces_visc_boundary<2, R>, (nB + b - 1) / b, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
     else
-      k_faces_visc_boundary<3, R><<<(nB + b - 1) / b, b, 0, st>>>(nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
+      launch_k(k_faces_visc_boundary<3, R>, (nB + b - 1) / b, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
   }
 }

@@ -63,6 +63,7 @@ typedef struct fr_setup_opts {
   int tile_variant;            /* precision form: element tile shape, -1 (default) = autotuned at setup;
                                   the last variant of 2-D orders 1..4 is the tensor-core (tcgen05) kernel */
   int no_tensor_cores;         /* 1: leave the tensor-core variant out of the autotuner's choice */
+  int no_pdl;                  /* 1: no programmatic dependent launch (used for small cases by default) */
 } fr_setup_opts;
 
 /* Mesh supplied by the caller (linear quads or hexes, reference node order).
