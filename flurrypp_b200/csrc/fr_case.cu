@@ -59,6 +59,7 @@ struct fr_case {
   double *Fdbg = nullptr, *disFnDbg = nullptr;
   double *dUc = nullptr, *dUs = nullptr, *dUf = nullptr;  // viscous: LDG jumps, gradients
   unsigned long long *dtBits = nullptr;
+  unsigned int *dtCount = nullptr;  // blocks done in the fused dt kernel
   unsigned int *bad = nullptr;
   frk::FaceTable ft;
   frk::Csr grad[3], extFn[3], corr, ext;
@@ -218,8 +219,9 @@ struct fr_case {
       if (!upload(f32.JGinv, narrow(geo.JGinv_spts)) || !upload(f32.detJ, narrow(geo.detJac_spts))) return false;
     }
     if (!alloc(waveSp, (size_t)nFp * E) || !alloc(eleDt, E) || !alloc(dt, 1) || !alloc(timeAcc, 1) ||
-        !alloc(eleRes, (size_t)E * nF) || !alloc(dtBits, 1) || !alloc(bad, 1))
+        !alloc(eleRes, (size_t)E * nF) || !alloc(dtBits, 1) || !alloc(dtCount, 1) || !alloc(bad, 1))
       return false;
+    frk::launch_reset_min(dtBits, stream);  // the fused dt kernel starts from +inf
     if (!upload(detJ, geo.detJac_spts) || !upload(norm, geo.norm_fpts) || !upload(dA, geo.dA_fpts)) return false;
     if (!upload(wSpt, fr::spt_weights(nDims, in.order)) || !upload(wSurf, fr::face_weights(nDims, in.order)))
       return false;
@@ -954,11 +956,9 @@ struct fr_case {
       wavesp_init();
       launches++;
     }
-    launches += 3;
-    frk::launch_reset_min(dtBits, stream);
-    frk::launch_element_dt(nDims, nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA,
-                           in.CFL * fr::cfl_limit(in.order), eleDt, dtBits, stream);
-    frk::launch_store_min(dtBits, dt, timeAcc, stream);
+    launches++;
+    frk::launch_element_dt_min(nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA, in.CFL * fr::cfl_limit(in.order),
+                               eleDt, dtBits, dtCount, dt, stream);
   }
 
   // Everything of a stage before the element kernel: the common flux Fn (and,
@@ -972,13 +972,14 @@ struct fr_case {
 
   void faces_pass() {
     const int nk = (ft.nInterior > 0 ? 1 : 0) + (ft.n > ft.nInterior ? 1 : 0);
+    const int nkInv = (nk == 2 && frk::pdl_enabled()) ? 1 : nk;  // small cases: one face launch
     if (mixed) {
       faces_pass32(nk);
       return;
     }
     if (!in.viscous) {
       frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
-      launches += nk;
+      launches += nkInv;
       return;
     }
     frk::launch_faces_ldg(nDims, ft, Ufpts, dUc, ph, stream);
@@ -1002,7 +1003,7 @@ struct fr_case {
   void faces_pass32(int nk) {
     if (!in.viscous) {
       frk::launch_faces_inviscid<float>(nDims, f32.ft, f32.Ufpts, f32.Fn, waveSp, ph, stream);
-      launches += nk;
+      launches += (nk == 2 && frk::pdl_enabled()) ? 1 : nk;
       return;
     }
     frk::launch_faces_ldg<float>(nDims, f32.ft, f32.Ufpts, f32.dUc, ph, stream);
@@ -1082,7 +1083,9 @@ struct fr_case {
 
   bool calc_residual(int step) {
     if (step < 0 || step >= nRK) return fail(FR_ERR_ARG, "step out of range");
-    extrapolate();
+    // the last element stage extrapolated the state it wrote; otherwise
+    // (a new or restricted/prolonged state) extrapolate here
+    if (!fptsFresh) extrapolate();
     faces_pass();
     if (!mixed) {
       frk::ElemArgs a = elem_args();
@@ -1902,6 +1905,16 @@ int fr_batch_info(fr_batch *b, int *nGroups, long long *launches) {
 const char *fr_batch_last_error(const fr_batch *b) { return b ? b->err.c_str() : "null batch"; }
 
 void fr_batch_destroy(fr_batch *b) { delete b; }
+
+int fr_stream_idle(fr_case *c) {
+  if (!c || c->hostOnly || !c->stream) return FR_ERR_ARG;
+  const cudaError_t e = cudaStreamQuery(c->stream);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) return 0;
+  cudaGetLastError();
+  c->err = std::string("stream query: ") + cudaGetErrorString(e);
+  return -FR_ERR_CUDA;
+}
 
 int fr_synchronize(fr_case *c) {
   if (!c) return FR_ERR_ARG;

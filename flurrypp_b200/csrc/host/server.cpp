@@ -44,6 +44,8 @@ struct Request {
   fr_case *c = nullptr;
   size_t bytes = 0;
   int steps = 0;
+  int pending = 0;  // steps issued and not yet seen complete
+  int nFields = 0;
   std::vector<double> res0;
   // result
   int status = 0;  // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
@@ -114,6 +116,9 @@ struct fr_server {
     r.c = c;
     r.bytes = b;
     r.status = 1;
+    fr_info inf;
+    fr_get_info(c, &inf);
+    r.nFields = inf.nFields;
     inflightBytes += b;
     inflight.push_back(id);
     queue.pop_front();
@@ -148,32 +153,41 @@ struct fr_server {
       }
       std::vector<long long> ids = inflight;
       lk.unlock();
-      // advance every case in flight: the steps of all cases are issued
-      // before any result is read, so their kernels overlap on the device
+      // every case advances on its own stream at its own pace: a case whose
+      // last chunk of steps has completed is checked and given its next
+      // chunk at once, so small cases do not wait for large ones and the
+      // kernels of all cases overlap on the device
+      bool progressed = false;
       for (long long id : ids) {
         Request &r = *reqs[id];
-        int n = std::min(checkEvery, r.maxSteps - r.steps);
-        if (n > 0 && fr_run(r.c, n) == FR_OK) r.steps += n;
+        if (r.pending == 0) {
+          int n = std::min(checkEvery, r.maxSteps - r.steps);
+          if (n > 0 && fr_run(r.c, n) == FR_OK) r.pending = n;
+          progressed = true;
+        }
       }
       std::vector<std::pair<long long, int>> done;  // id, status
       for (long long id : ids) {
         Request &r = *reqs[id];
-        fr_info inf;
-        fr_get_info(r.c, &inf);
-        std::vector<double> res(inf.nFields);
-        int st = fr_residual_norm(r.c, 2, res.data(), inf.nFields);
+        if (r.pending == 0 || fr_stream_idle(r.c) != 1) continue;
+        progressed = true;
+        r.steps += r.pending;
+        r.pending = 0;
+        std::vector<double> res(r.nFields);
+        int st = fr_residual_norm(r.c, 2, res.data(), r.nFields);
         if (st != FR_OK) {
           done.push_back({id, 3});
           continue;
         }
         if (r.res0.empty()) r.res0 = res;
         double ratio = 0.0;
-        for (int k = 0; k < inf.nFields; k++)
+        for (int k = 0; k < r.nFields; k++)
           ratio = std::max(ratio, r.res0[k] > 0 ? res[k] / r.res0[k] : 0.0);
         r.finalRatio = ratio;
         if (ratio <= r.tol) done.push_back({id, 2});
         else if (r.steps >= r.maxSteps) done.push_back({id, 2});
       }
+      if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
       lk.lock();
       for (auto &d : done) {
         Request &r = *reqs[d.first];
@@ -185,6 +199,7 @@ struct fr_server {
       for (size_t i = 0; i < inflight.size();) {
         Request &r = *reqs[inflight[i]];
         if (r.status == 4) {
+          fr_synchronize(r.c);
           fr_destroy(r.c);
           r.c = nullptr;
           inflightBytes -= r.bytes;

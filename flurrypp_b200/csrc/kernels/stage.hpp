@@ -213,6 +213,11 @@ void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double 
                        const double *wSpt, const double *wSurf, const double *waveSp,
                        const double *dA, double cflFac, double *eleDt,
                        unsigned long long *dtMinBits, cudaStream_t st);
+// The same, the minimum stored straight into *dt by the last block, which
+// then resets *bits (to +inf) and *count (to 0): one launch per time step.
+void launch_element_dt_min(int nS, int nFp, int nPF, int E, const double *detJ, const double *wSpt,
+                           const double *wSurf, const double *waveSp, const double *dA, double cflFac, double *eleDt,
+                           unsigned long long *bits, unsigned int *count, double *dt, cudaStream_t st);
 void launch_reset_min(unsigned long long *bits, cudaStream_t st);
 void launch_store_min(const unsigned long long *bits, double *dt, double *time_acc,
                       cudaStream_t st);

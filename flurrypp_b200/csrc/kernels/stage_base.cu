@@ -44,19 +44,14 @@ __global__ void k_apply_op(int nRows, const int *__restrict__ rp, const int *__r
   out[(long long)r * N + n] = o;
 }
 
-// Interior face points: Rusanov (or 2-D Roe) on the left normal, written to
+// Interior face point i: Rusanov (or 2-D Roe) on the left normal, written to
 // both sides (reference: face.cpp:163-208, intFace.cpp:147-154).
 template <int ND, typename R>
-__global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__restrict__ slotL,
-                                                        const int *__restrict__ slotR, const R *__restrict__ nrm,
-                                                        const R *__restrict__ dAL, const R *__restrict__ dAR,
-                                                        const R *__restrict__ Uf, R *__restrict__ Fn,
-                                                        double *__restrict__ waveSp, R gam, int roe) {
-  pdl_wait();
-  pdl_trigger();
+__device__ __forceinline__ void face_interior(int i, const int *__restrict__ slotL, const int *__restrict__ slotR,
+                                              const R *__restrict__ nrm, const R *__restrict__ dAL,
+                                              const R *__restrict__ dAR, const R *__restrict__ Uf,
+                                              R *__restrict__ Fn, double *__restrict__ waveSp, R gam, int roe) {
   constexpr int NF = ND + 2;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const int sL = slotL[i];
   const int sR = slotR[i];
   R UL[NF], UR[NF], nv[ND], F[NF];
@@ -79,17 +74,14 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
   }
 }
 
-// Boundary face points: ghost state from the BC, then Rusanov (boundaries
+// Boundary face point i: ghost state from the BC, then Rusanov (boundaries
 // always use Rusanov, face.cpp:174-176; ghost states boundFace.cpp:65-314).
 template <int ND, typename R>
-__global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
-                                 const R *__restrict__ nrm, const R *__restrict__ dAL, const R *__restrict__ Uf,
-                                 R *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
-  pdl_wait();
-  pdl_trigger();
+__device__ __forceinline__ void face_boundary(int i, const int *__restrict__ slotL, const int *__restrict__ slotR,
+                                              const R *__restrict__ nrm, const R *__restrict__ dAL,
+                                              const R *__restrict__ Uf, R *__restrict__ Fn,
+                                              double *__restrict__ waveSp, const Phys &ph) {
   constexpr int NF = ND + 2;
-  int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const int sL = slotL[i];
   const int bc = -slotR[i] - 2;
   R UL[NF], UR[NF], nv[ND], F[NF];
@@ -102,6 +94,47 @@ __global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, c
   const R aL = dAL[i];
 #pragma unroll
   for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
+}
+
+// Interior points only (no boundary-condition code, fewer registers).
+template <int ND, typename R>
+__global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__restrict__ slotL,
+                                                        const int *__restrict__ slotR, const R *__restrict__ nrm,
+                                                        const R *__restrict__ dAL, const R *__restrict__ dAR,
+                                                        const R *__restrict__ Uf, R *__restrict__ Fn,
+                                                        double *__restrict__ waveSp, R gam, int roe) {
+  pdl_wait();
+  pdl_trigger();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  face_interior<ND, R>(i, slotL, slotR, nrm, dAL, dAR, Uf, Fn, waveSp, gam, roe);
+}
+
+template <int ND, typename R>
+__global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
+                                 const R *__restrict__ nrm, const R *__restrict__ dAL, const R *__restrict__ Uf,
+                                 R *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
+  int i = n0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  face_boundary<ND, R>(i, slotL, slotR, nrm, dAL, Uf, Fn, waveSp, ph);
+}
+
+// All face points in one launch (small cases, where the launch count
+// dominates): interior points first, then boundary points.
+template <int ND, typename R>
+__global__ void k_faces_all(int nI, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
+                            const R *__restrict__ nrm, const R *__restrict__ dAL, const R *__restrict__ dAR,
+                            const R *__restrict__ Uf, R *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (i < nI)
+    face_interior<ND, R>(i, slotL, slotR, nrm, dAL, dAR, Uf, Fn, waveSp, R(ph.gamma), ND == 2 && ph.riemannType == 1);
+  else
+    face_boundary<ND, R>(i, slotL, slotR, nrm, dAL, Uf, Fn, waveSp, ph);
 }
 
 __device__ __forceinline__ double csr_dot(const Csr &A, int row, const double *__restrict__ x,
@@ -291,6 +324,58 @@ __global__ void k_element_dt(int nS, int nFp, int nPF, int E, const double *__re
     atomicMin(dtMinBits, (unsigned long long)__double_as_longlong(dt));
 }
 
+// Element dt and the global minimum in one launch: each block reduces its
+// elements' dt (bit patterns of non-negative doubles order like the values)
+// and folds it into *bits with atomicMin; the last block to finish stores
+// the minimum in *dt and resets *bits and *count for the next call, so no
+// separate reset or store launch is needed (*bits must start at +inf and
+// *count at 0).
+__global__ void k_element_dt_min(int nS, int nFp, int nPF, int E, const double *__restrict__ detJ,
+                                 const double *__restrict__ wSpt, const double *__restrict__ wSurf,
+                                 const double *__restrict__ waveSp, const double *__restrict__ dA, double cflFac,
+                                 double *__restrict__ eleDt, unsigned long long *bits, unsigned int *count,
+                                 double *dtOut) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ unsigned long long sMin[32];
+  __shared__ bool last;
+  const unsigned long long INF = (unsigned long long)0x7ff0000000000000ull;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long mine = INF;
+  if (e < E) {
+    double vol = 0;
+    for (int s = 0; s < nS; s++) vol += detJ[(long long)s * E + e] * wSpt[s];
+    double intWave = 0;
+    for (int f = 0; f < nFp; f++)
+      intWave += waveSp[(long long)f * E + e] * wSurf[f % nPF] * dA[(long long)f * E + e];
+    double dt = cflFac * 2 * vol / intWave;
+    if (eleDt) eleDt[e] = dt;
+    if (dt >= 0.0 && dt == dt) mine = (unsigned long long)__double_as_longlong(dt);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, mine, o);
+    mine = v < mine ? v : mine;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sMin[w] = mine;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = INF;
+    for (int i = 0; i < (int)((blockDim.x + 31) / 32); i++) m = sMin[i] < m ? sMin[i] : m;
+    if (m != INF) atomicMin(bits, m);
+    __threadfence();
+    last = atomicAdd(count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long m = atomicAdd(bits, 0ull);
+    *dtOut = __longlong_as_double((long long)m);
+    *bits = INF;
+    *count = 0;
+  }
+}
+
 __global__ void k_reset_min(unsigned long long *bits) {
   pdl_wait();
   pdl_trigger();
@@ -420,6 +505,16 @@ void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R
                            const Phys &ph, cudaStream_t st) {
   const int b = 256;
   const int nI = ft.nInterior, nB = ft.n - ft.nInterior;
+  if (nI > 0 && nB > 0 && pdl_enabled()) {  // small case: one launch
+    const int g = (ft.n + b - 1) / b;
+    if (nDims == 2)
+      launch_k(k_faces_all<2, R>, g, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn,
+               waveSp, ph);
+    else
+      launch_k(k_faces_all<3, R>, g, b, 0, st, nI, ft.n, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn,
+               waveSp, ph);
+    return;
+  }
   if (nI > 0) {
     const int g = (nI + b - 1) / b;
     if (nDims == 2)
@@ -476,6 +571,14 @@ void launch_element_dt(int nDims, int nS, int nFp, int nPF, int E, const double 
   if (E <= 0) return;
   launch_k(k_element_dt, (E + 127) / 128, 128, 0, st, nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA,
                                                  cflFac, eleDt, dtMinBits);
+}
+
+void launch_element_dt_min(int nS, int nFp, int nPF, int E, const double *detJ, const double *wSpt,
+                           const double *wSurf, const double *waveSp, const double *dA, double cflFac, double *eleDt,
+                           unsigned long long *bits, unsigned int *count, double *dt, cudaStream_t st) {
+  if (E <= 0) return;
+  launch_k(k_element_dt_min, (E + 127) / 128, 128, 0, st, nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA, cflFac,
+           eleDt, bits, count, dt);
 }
 
 void launch_reset_min(unsigned long long *bits, cudaStream_t st) { launch_k(k_reset_min, 1, 1, 0, st, bits); }

@@ -221,6 +221,10 @@ void fr_server_destroy(fr_server *s);
 
 /* Blocks until the case's stream is idle; returns FR_ERR_CUDA on a sticky error. */
 int fr_synchronize(fr_case *c);
+/* 1 when all work issued on the case's stream has completed, 0 while some is
+ * running, -FR_ERR_CUDA on an error (cudaStreamQuery); no reference
+ * counterpart (used by the solve server to advance cases independently). */
+int fr_stream_idle(fr_case *c);
 
 /* Residual norm that allocates no device memory.  No counterpart in the
  * reference; it computes what fr_residual_norm computes (writeResidual,
