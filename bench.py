@@ -127,6 +127,24 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(values, device):
+    """Each timing as the maximum over all ranks (replicas finish when the
+    slowest does); identity with one process."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_rate(world: int, dof: int, stages: int, steps: int, ms: float) -> float:
+    """DOF x RK stages / s over all ranks: every rank advances its own case
+    of `dof` unknowns by `steps` steps in `ms` (the slowest rank's time)."""
+    return world * dof * stages * steps / (ms / 1e3)
+
+
 def reference_sample(steps: int, warmup: int, threads: int):
     """The reference's own CPU path (oracle/_ref, OpenMP build) on the bounded
     sample: the same Taylor-Green problem on 16^3 hexes (same per-element work,
@@ -603,14 +621,11 @@ def main():
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
 
-    t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], "cuda")
 
     if rank == 0:
-        value = world * dof * nrk * args.steps / (ms / 1e3)
-        e2e = world * dof * nrk * args.e2e_steps / (ms_e2e / 1e3)
+        value = whole_job_rate(world, dof, nrk, args.steps, ms)
+        e2e = whole_job_rate(world, dof, nrk, args.e2e_steps, ms_e2e)
         peak, peak_kind = measured_peak_hbm()
         # algorithmic bytes per launch of the element kernel (intermediate RK
         # stage, FP64): per element read U, U0, acc, Fn (nFpts*nF), JGinv
