@@ -606,17 +606,17 @@ def main():
     # end to end through the C ABI with host buffers (pinned), every step:
     # state H2D, one update, state D2H
     U_host = torch.empty(s.shape, dtype=torch.float64, pin_memory=True).numpy()
-    U_host[...] = s.get_state()
+    s.get_state(out=U_host)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.set_state(U_host)
     s.update()
-    U_host[...] = s.get_state()
+    s.get_state(out=U_host)
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.e2e_steps):
-        s.set_state(U_host)
+        s.set_state(U_host)   # pinned host -> device
         s.update()
-        U_host[...] = s.get_state()
+        s.get_state(out=U_host)  # device -> pinned host
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)

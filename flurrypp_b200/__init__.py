@@ -222,10 +222,15 @@ class Solver:
         U = np.ascontiguousarray(U, dtype=np.float64)
         self._check(lib.fr_set_state(self._c, _dptr(U), U.size))
 
-    def get_state(self) -> np.ndarray:
-        U = np.empty(self.shape, dtype=np.float64)
-        self._check(lib.fr_get_state(self._c, _dptr(U), U.size))
-        return U
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """U_spts [nSpts, nEles, nFields]; into `out` (e.g. pinned host
+        memory, C-contiguous float64 of that shape) when given."""
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float64)
+        elif out.dtype != np.float64 or out.size != self.nSpts * self.nEles * self.nFields or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of the state's size")
+        self._check(lib.fr_get_state(self._c, _dptr(out), out.size))
+        return out
 
     def calc_residual(self, step: int = 0):
         self._check(lib.fr_calc_residual(self._c, step))

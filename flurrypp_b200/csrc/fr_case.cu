@@ -1334,17 +1334,18 @@ int copy_dev(fr_case *c, const T *d, size_t n, void *host, size_t *count) {
   *count = n;
   if (!host) return FR_OK;
   if (cap < n) return FR_ERR_ARG;
-  if (!c->sync()) return FR_ERR_CUDA;
   std::vector<T> tmp;
   void *dst = host;
   if (!std::is_same<T, double>::value) {
     tmp.resize(n);
     dst = tmp.data();
   }
-  if (cudaMemcpy(dst, d, n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess) {
+  // on the case's stream, after the work that produced the array
+  if (cudaMemcpyAsync(dst, d, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) {
     c->err = "cudaMemcpy D2H failed";
     return FR_ERR_CUDA;
   }
+  if (!c->sync()) return FR_ERR_CUDA;
   if (!std::is_same<T, double>::value)
     for (size_t i = 0; i < n; i++) static_cast<double *>(host)[i] = (double)tmp[i];
   return FR_OK;
