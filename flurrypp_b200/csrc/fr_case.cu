@@ -89,6 +89,8 @@ struct fr_case {
   // programmatic dependent launch for cases whose grids fit in about one wave
   // (a solution point per thread: 148 SMs x 1024 threads)
   bool usePdl = false;
+  int variant64 = 0;              // plain form: element tile variant in use
+  std::vector<float> tuneMs64;    // plain form: element-stage ms per tile variant
   struct Fp32 {
     float *U = nullptr, *U0 = nullptr, *acc = nullptr, *comp = nullptr, *Ufpts = nullptr, *Fn = nullptr;
     float *JGinv = nullptr, *detJ = nullptr;
@@ -333,8 +335,9 @@ struct fr_case {
     if (!alloc(devErr, 1)) return false;
     usePdl = !opts.no_pdl && (long long)nS * E <= 148LL * 1024;
     if (!mixed) {
-      useTma = useTp && !opts.no_tma && build_tma();
+      useTma = useTp && !opts.no_tma && build_tma(0);
       if (useTma && in.viscous) EB = frk::tma_elems_per_block<double>(nDims, in.order);
+      if (useTma && !in.viscous && !autotune_tiles64()) return false;
     } else if (useTp && in.viscous && !opts.no_tma && (E * nF) % 4 == 0) {
       // viscous precision form: tile variant 0
       if (build_tma32(0)) {
@@ -766,9 +769,60 @@ struct fr_case {
   double *detTma = nullptr, *jgTma = nullptr;
   float *detTma32 = nullptr, *jgTma32 = nullptr;
 
-  bool build_tma() {
-    return build_maps<double>(tm, frk::tma_elems_per_block<double>(nDims, in.order), U, U0, acc, nullptr, Fn, Ufpts,
-                              detJ, JGinv, detTma, jgTma, dUs, dUc, dUf);
+  bool build_tma(int v) {
+    return build_maps<double>(tm, frk::tma_elems_per_block<double>(nDims, in.order, v), U, U0, acc, nullptr, Fn,
+                              Ufpts, detJ, JGinv, detTma, jgTma, dUs, dUc, dUf);
+  }
+
+  // The plain form's tile autotuner: the same timing as autotune_tiles on
+  // the FP64 arrays; all variants give bit-identical results.
+  bool autotune_tiles64() {
+    const int nv = frk::tma_variants(false);
+    const int forced = opts.tile_variant;
+    if (forced >= nv) return fail(FR_ERR_ARG, "tile_variant out of range for the plain form");
+    tuneMs64.assign(nv, -1.0f);
+    int best = -1;
+    float bestMs = 0.0f;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "event create");
+    for (int v = 0; v < nv; v++) {
+      if (forced >= 0 && v != forced) continue;
+      bool dup = false;
+      for (int w = 0; w < v; w++)
+        if (frk::tma_elems_per_block<double>(nDims, in.order, w) == frk::tma_elems_per_block<double>(nDims, in.order, v))
+          dup = true;
+      if (dup && forced < 0) continue;
+      if (!build_tma(v)) continue;
+      frk::ElemArgs a = elem_args();
+      a.mode = frk::MODE_RK_STAGE;
+      a.stage = 1;
+      a.Ufpts_out = Ufpts;
+      for (int i = 0; i < 2; i++) frk::launch_element_stage_tma<double>(nDims, in.order, a, tp, tm, stream, v);
+      cudaEventRecord(e0, stream);
+      const int reps = 5;
+      for (int i = 0; i < reps; i++) frk::launch_element_stage_tma<double>(nDims, in.order, a, tp, tm, stream, v);
+      cudaEventRecord(e1, stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      tuneMs64[v] = ms / reps;
+      if (best < 0 || tuneMs64[v] < bestMs) {
+        best = v;
+        bestMs = tuneMs64[v];
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!cuda_ok("tile autotune") || !sync()) return false;
+    if (best < 0) best = 0;
+    if (!build_tma(best)) return fail(FR_ERR_CUDA, "tensor map");
+    variant64 = best;
+    const size_t nU = (size_t)nS * E * nF, nUf = (size_t)nFp * E * nF;
+    for (double *p : {U, U0, acc}) cudaMemsetAsync(p, 0, nU * sizeof(double), stream);
+    cudaMemsetAsync(Ufpts, 0, nUf * sizeof(double), stream);
+    cudaMemsetAsync(devErr, 0, sizeof(unsigned), stream);
+    return sync();
   }
   bool build_tma32(int v) {
     return build_maps<float>(f32.tm, frk::tma_elems_per_block<float>(nDims, in.order, v), f32.U, f32.U0, f32.acc,
@@ -1030,7 +1084,7 @@ struct fr_case {
     else if (in.viscous)
       frk::launch_element_stage_tp_visc<double>(nDims, in.order, a, tp, stream);
     else if (useTma)
-      frk::launch_element_stage_tma<double>(nDims, in.order, a, tp, tm, stream);
+      frk::launch_element_stage_tma<double>(nDims, in.order, a, tp, tm, stream, variant64);
     else if (useTp)
       frk::launch_element_stage_tp<double>(nDims, in.order, a, tp, stream);
     else
@@ -1395,7 +1449,7 @@ int fr_get_info(fr_case *c, fr_info *info) {
   info->iter = c->iter;
   info->launches = c->total_launches();
   info->tensor_kernels = (c->mixed ? c->f32.useTma : c->useTma) ? 2 : (c->useTp ? 1 : 0);
-  info->tile_variant = c->mixed && c->f32.useTma ? c->f32.variant : -1;
+  info->tile_variant = c->mixed ? (c->f32.useTma ? c->f32.variant : -1) : (c->useTma ? c->variant64 : -1);
   info->elems_per_block = c->EB;
   if (c->U && !c->hostOnly) {
     if (!c->sync()) return FR_ERR_CUDA;
@@ -1672,7 +1726,8 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count) {
     return copy_dev(c, c->divF[s], nU, host, count);
   }
   if (n == "tile_ms") {  // precision form: element-stage ms per tile variant timed by the autotuner (-1: not run)
-    std::vector<double> v(c->f32.tuneMs.begin(), c->f32.tuneMs.end());
+    const std::vector<float> &t = c->mixed ? c->f32.tuneMs : c->tuneMs64;
+    std::vector<double> v(t.begin(), t.end());
     return copy_out(c, v, host, count);
   }
   if (n == "pos_spts") return copy_out(c, c->geo.pos_spts, host, count);

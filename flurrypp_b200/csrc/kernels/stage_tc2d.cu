@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
   const bool needAcc = (a.mode == MODE_RK_STAGE && a.stage > 0) || (a.mode == MODE_RK_FINAL && a.nRK > 1);
   const bool needCmp = finalStage;
   const bool needDet = a.mode != MODE_RESIDUAL;
+  const double dtIn = a.mode == MODE_RESIDUAL ? 0.0 : (a.eleDt ? (rvalid ? a.eleDt[e0 + re] : 0.0) : *a.dt);
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -256,8 +257,7 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
     tc_fence_after();
     // divergence + correction (TMEM columns 0 ..): RK update, new state into
     // the tiles and into the third A operand
-    const int e = e0 + re;
-    const float dt = float(a.mode == MODE_RESIDUAL ? 0.0 : (a.eleDt ? (rvalid ? a.eleDt[e] : 0.0) : *a.dt));
+    const float dt = float(dtIn);
     const float rka = float(a.rka_next), rkb = float(a.rkb);
     for (int c = 0; c < NS; c += 8) {
       float v[8];

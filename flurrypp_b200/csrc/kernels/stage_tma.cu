@@ -28,6 +28,7 @@ constexpr int ipow2(int b, int e) { return e == 0 ? 1 : b * ipow2(b, e - 1); }
 constexpr int pow2_floor(int x) { return x >= 2 ? 2 * pow2_floor(x / 2) : 1; }
 
 constexpr int kFp32Variants = 3;
+constexpr int kFp64Variants = 2;
 constexpr size_t kMaxSmem = 227 * 1024;
 
 template <int ND, int P, typename R, int V>
@@ -49,19 +50,22 @@ struct Tm {
            128;
   }
   static constexpr bool fits(int eb) { return NS * eb <= 1024 && smem_for(eb) <= kMaxSmem && eb * NF <= 256; }
-  // FP64: largest power of two <= 32 with NS*EB <= 160, at least 2.
+  // FP64: largest power of two <= 32 with NS*EB <= 160, at least 2, times
+  // 2^V (at most 32, halved until it fits).
   // FP32: 128/NS rounded down to a power of two, at least 4 (16-byte
   // offsets), times 2^V, at most 32, halved until it fits.
-  static constexpr int eb64() {
+  static constexpr int eb64_base() {
     return NS * 32 <= 160 ? 32 : NS * 16 <= 160 ? 16 : NS * 8 <= 160 ? 8 : NS * 4 <= 160 ? 4 : 2;
   }
+  static constexpr int eb64() { return (eb64_base() << V) > 32 ? 32 : (eb64_base() << V); }
   static constexpr int eb32_want() {
     return (pow2_floor(128 / NS) < 4 ? 4 : pow2_floor(128 / NS)) << V > 32
                ? 32
                : (pow2_floor(128 / NS) < 4 ? 4 : pow2_floor(128 / NS)) << V;
   }
   static constexpr int shrink(int eb) { return (eb <= 4 || fits(eb)) ? eb : shrink(eb / 2); }
-  static constexpr int EB = F32 ? shrink(eb32_want()) : eb64();
+  static constexpr int shrink64(int eb) { return (eb <= 2 || fits(eb)) ? eb : shrink64(eb / 2); }
+  static constexpr int EB = F32 ? shrink(eb32_want()) : shrink64(eb64());
   static constexpr int NT = NS * EB;
   static constexpr int ROW = EB * NF;
   static constexpr int O_U = 0;
@@ -133,6 +137,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
   const bool needAcc = (a.mode == MODE_RK_STAGE && a.stage > 0) || (a.mode == MODE_RK_FINAL && a.nRK > 1);
   const bool needCmp = F32 && finalStage;
   const bool needDet = a.mode != MODE_RESIDUAL;
+  // the time step, loaded now so its latency hides behind the tile loads
+  const double dtIn = a.mode == MODE_RESIDUAL ? 0.0 : (a.eleDt ? (valid ? a.eleDt[e] : 0.0) : *a.dt);
 
   // two transaction barriers: bar[0] for what the flux needs (U, JGinv),
   // bar[1] for what the correction and update need, so the second batch
@@ -301,7 +307,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     }
     // one reciprocal per point instead of a division per update term
     const R rdJ = needDet ? R(1.0) / sDet[s * EB + el] : R(1.0);
-    const R dt = R(a.mode == MODE_RESIDUAL ? 0.0 : (a.eleDt ? (valid ? a.eleDt[e] : 0.0) : *a.dt));
+    const R dt = R(dtIn);
     const R rka = R(a.rka_next), rkb = R(a.rkb);
 #pragma unroll
     for (int k = 0; k < NF; k++) {
@@ -645,11 +651,11 @@ template void launch_elem_grad_tma<double>(int, int, int, const TpTablesT<double
 template void launch_elem_grad_tma<float>(int, int, int, const TpTablesT<float> &, const TmaMaps &, unsigned int *,
                                           cudaStream_t);
 
-int tma_variants(bool fp32) { return fp32 ? kFp32Variants : 1; }
+int tma_variants(bool fp32) { return fp32 ? kFp32Variants : kFp64Variants; }
 
 template <>
-int tma_elems_per_block<double>(int nDims, int order, int) {
-  return eb_of<double, 0>(nDims, order);
+int tma_elems_per_block<double>(int nDims, int order, int v) {
+  return v == 0 ? eb_of<double, 0>(nDims, order) : eb_of<double, 1>(nDims, order);
 }
 template <>
 int tma_elems_per_block<float>(int nDims, int order, int v) {
@@ -657,8 +663,8 @@ int tma_elems_per_block<float>(int nDims, int order, int v) {
   return v == 0 ? eb_of<float, 0>(nDims, order) : v == 1 ? eb_of<float, 1>(nDims, order) : eb_of<float, 2>(nDims, order);
 }
 template <>
-size_t tma_smem_bytes<double>(int nDims, int order, int) {
-  return smem_of<double, 0>(nDims, order);
+size_t tma_smem_bytes<double>(int nDims, int order, int v) {
+  return v == 0 ? smem_of<double, 0>(nDims, order) : smem_of<double, 1>(nDims, order);
 }
 template <>
 size_t tma_smem_bytes<float>(int nDims, int order, int v) {
@@ -667,9 +673,12 @@ size_t tma_smem_bytes<float>(int nDims, int order, int v) {
 
 template <>
 void launch_element_stage_tma<double>(int nDims, int order, const ElemArgsT<double> &a, const TpTablesT<double> &t,
-                                      const TmaMaps &m, cudaStream_t st, int) {
+                                      const TmaMaps &m, cudaStream_t st, int v) {
   if (a.E <= 0) return;
-  launch_v<double, 0>(nDims, order, a, t, m, st);
+  if (v == 0)
+    launch_v<double, 0>(nDims, order, a, t, m, st);
+  else
+    launch_v<double, 1>(nDims, order, a, t, m, st);
 }
 template <>
 void launch_element_stage_tma<float>(int nDims, int order, const ElemArgsT<float> &a, const TpTablesT<float> &t,

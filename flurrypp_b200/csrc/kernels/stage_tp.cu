@@ -62,6 +62,8 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
   const int s = tid / EB, el = tid - (tid / EB) * EB;
   const int e = e0 + el;
   const bool valid = el < nValid;
+  // the time step, loaded early so its latency overlaps the tile loads
+  const double dtIn = a.eleDt ? (valid ? a.eleDt[e] : 0.0) : (a.mode != MODE_RESIDUAL ? *a.dt : 0.0);
 
   for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
   for (int i = tid; i < 2 * N; i += NT) {
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
       for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
     }
     const R rdJ = R(1.0) / a.detJ[(long long)s * E + e];  // one reciprocal per point
-    const R dt = R(a.eleDt ? a.eleDt[e] : (a.mode != MODE_RESIDUAL ? *a.dt : 0.0));
+    const R dt = R(dtIn);
     const R rka = R(a.rka_next), rkb = R(a.rkb);
     const bool finalStage = a.mode == MODE_RK_FINAL || (a.mode == MODE_JAMESON && a.stage == a.nRK - 1);
 #pragma unroll

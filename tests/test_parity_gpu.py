@@ -193,3 +193,21 @@ def test_cpp_driver_matches_python_binding():
         s.update()
     res_py = s.residual_norm(2)
     assert np.allclose(res_cpp, res_py, rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "p5_2d", "channel2d_p2"])
+def test_plain_tile_variants_bit_identical(case):
+    """The plain form's autotuner chooses between element tile shapes that
+    compute every point with the same operations: bit-identical states."""
+    a, meta = load_golden(case)
+    outs = []
+    for v in (0, 1):
+        s = gpu_case(meta, tile_variant=v)
+        inf = s.info()
+        if inf.tile_variant != v:
+            pytest.skip("no TMA tiles for this case")
+        s.set_state(a["U_init"])
+        s.run(meta["steps"])
+        outs.append(s.get_state())
+    assert np.array_equal(outs[0], outs[1])
+    assert rel_err(outs[0], a["U_final"]) < STEP_TOL
