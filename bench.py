@@ -464,6 +464,7 @@ PROFILE_CASES = {
     "fp32_vortex256_p3": ("vortex", 3, 256, 1, -1),
     "tc_vortex256_p3": ("vortex", 3, 256, 1, 3),
     "fp32_ns_tgv24_p4": ("ns", 4, 24, 1, -1),
+    "fp64_ns_tgv24_p4": ("ns", 4, 24, 0, -1),
 }
 
 

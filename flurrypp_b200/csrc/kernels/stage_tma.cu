@@ -447,13 +447,16 @@ struct Tg2 {
   static constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
   static constexpr int AL = T::AL;
   static constexpr int al(int n) { return (n + AL - 1) / AL * AL; }
+  // the flux-point gradient tile reuses the input tiles (U, dUc, JGinv,
+  // detJ), dead once the gradient at the solution points is formed
   static constexpr int O_U = 0;
   static constexpr int O_C = O_U + al(NS * ROW);
   static constexpr int O_J = O_C + al(NFP * ROW);
   static constexpr int O_DET = O_J + al(ND * NS * EB * ND);
-  static constexpr int O_G = O_DET + al(NS * EB);
-  static constexpr int O_GF = O_G + al(ND * NS * ROW);
-  static constexpr int O_TAB = O_GF + al(ND * NFP * ROW);
+  static constexpr int IN_END = O_DET + al(NS * EB);
+  static constexpr int O_GF = O_U;
+  static constexpr int O_G = IN_END > al(ND * NFP * ROW) ? IN_END : al(ND * NFP * ROW);
+  static constexpr int O_TAB = O_G + al(ND * NS * ROW);
   static constexpr int O_CV = O_TAB + al(N * N + 2 * N);
   static constexpr int O_IDX = O_CV + al(NS * 2 * ND);
   static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1);
@@ -569,7 +572,7 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
       sG[(d2 * NS + s) * ROW + el * NF + k] = v;
     }
   fence_async_smem();
-  __syncthreads();
+  __syncthreads();  // the input tiles are dead from here on (sGf reuses them)
   if (tid == 0) {
     tma_store_3d(&mp.dUs, e0 * NF, 0, 0, sG);
     tma_commit();

@@ -24,6 +24,9 @@ __device__ __forceinline__ R ldg_pen(const R *n, R penFact) {
   return (n[0] + n[1] + sqrt(R(2.)) * n[ND - 1] < 0) ? -penFact : penFact;
 }
 
+// One thread per (interior face point, field): the jumps of one field need
+// only that field's two traces, so consecutive threads read and write
+// consecutive words.
 template <int ND, typename R>
 __global__ void k_faces_ldg_interior(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
                                      const R *__restrict__ nrm, const R *__restrict__ Uf,
@@ -31,20 +34,18 @@ __global__ void k_faces_ldg_interior(int n, const int *__restrict__ slotL, const
   pdl_wait();
   pdl_trigger();
   constexpr int NF = ND + 2;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * NF) return;
+  const int i = (int)(t / NF), k = (int)(t - (long long)i * NF);
   const int sL = slotL[i], sR = slotR[i];
   R nv[ND];
 #pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
   const R pen = ldg_pen<ND, R>(nv, penFact);
-#pragma unroll
-  for (int k = 0; k < NF; k++) {
-    const R ul = Uf[(long long)sL * NF + k], ur = Uf[(long long)sR * NF + k];
-    const R uc = R(0.5) * (ul + ur) - pen * (ul - ur);
-    dUc[(long long)sL * NF + k] = uc - ul;
-    dUc[(long long)sR * NF + k] = uc - ur;
-  }
+  const R ul = Uf[(long long)sL * NF + k], ur = Uf[(long long)sR * NF + k];
+  const R uc = R(0.5) * (ul + ur) - pen * (ul - ur);
+  dUc[(long long)sL * NF + k] = uc - ul;
+  dUc[(long long)sR * NF + k] = uc - ur;
 }
 
 template <int ND, typename R>
@@ -354,10 +355,12 @@ template <typename R>
 void launch_faces_ldg(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *dUc, const Phys &ph, cudaStream_t st) {
   const int b = 256, nI = ft.nInterior, nB = ft.n - ft.nInterior;
   if (nI > 0) {
+    const long long nt = (long long)nI * (nDims + 2);
+    const unsigned g = (unsigned)((nt + b - 1) / b);
     if (nDims == 2)
-      launch_k(k_faces_ldg_interior<2, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
+      launch_k(k_faces_ldg_interior<2, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
     else
-      launch_k(k_faces_ldg_interior<3, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
+      launch_k(k_faces_ldg_interior<3, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, Ufpts, dUc, ph.penFact);
   }
   if (nB > 0) {
     if (nDims == 2)
