@@ -1024,6 +1024,10 @@ struct fr_case {
       frk::launch_wavesp_init<double>(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
   }
 
+  // the face kernels' wave speeds feed only the CFL time step: a batch group
+  // (fixed dt per member) does not store them
+  double *wave_out() { return perElementDt && in.dtType == 0 ? nullptr : waveSp; }
+
   void faces_pass() {
     const int nk = (ft.nInterior > 0 ? 1 : 0) + (ft.n > ft.nInterior ? 1 : 0);
     const int nkInv = (nk == 2 && frk::pdl_enabled()) ? 1 : nk;  // small cases: one face launch
@@ -1032,7 +1036,7 @@ struct fr_case {
       return;
     }
     if (!in.viscous) {
-      frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, waveSp, ph, stream);
+      frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, wave_out(), ph, stream);
       launches += nkInv;
       return;
     }
@@ -1051,12 +1055,12 @@ struct fr_case {
       frk::launch_elem_grad_tma<double>(nDims, in.order, E, tp, tm, devErr, stream);
     else
       frk::launch_elem_grad(nDims, in.order, g, tp, stream);
-    frk::launch_faces_visc(nDims, ft, Ufpts, dUf, g.fStride, Fn, waveSp, ph, stream);
+    frk::launch_faces_visc(nDims, ft, Ufpts, dUf, g.fStride, Fn, wave_out(), ph, stream);
     launches += 2 * nk + 1;
   }
   void faces_pass32(int nk) {
     if (!in.viscous) {
-      frk::launch_faces_inviscid<float>(nDims, f32.ft, f32.Ufpts, f32.Fn, waveSp, ph, stream);
+      frk::launch_faces_inviscid<float>(nDims, f32.ft, f32.Ufpts, f32.Fn, wave_out(), ph, stream);
       launches += (nk == 2 && frk::pdl_enabled()) ? 1 : nk;
       return;
     }
@@ -1075,7 +1079,7 @@ struct fr_case {
       frk::launch_elem_grad_tma<float>(nDims, in.order, E, f32.tp, f32.tm, devErr, stream);
     else
       frk::launch_elem_grad<float>(nDims, in.order, g, f32.tp, stream);
-    frk::launch_faces_visc<float>(nDims, f32.ft, f32.Ufpts, f32.dUf, g.fStride, f32.Fn, waveSp, ph, stream);
+    frk::launch_faces_visc<float>(nDims, f32.ft, f32.Ufpts, f32.dUf, g.fStride, f32.Fn, wave_out(), ph, stream);
     launches += 2 * nk + 1;
   }
   void element(const frk::ElemArgs &a) {

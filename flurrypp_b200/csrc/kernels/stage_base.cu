@@ -64,7 +64,8 @@ __device__ __forceinline__ void face_interior(int i, const int *__restrict__ slo
   if (ND == 2 && roe) {
     roe2d<R>(UL, UR, nv, gam, F);
   } else {
-    waveSp[sL] = rusanov<ND, R>(UL, UR, nv, gam, F);
+    const R ws = rusanov<ND, R>(UL, UR, nv, gam, F);
+    if (waveSp) waveSp[sL] = ws;  // null when no CFL time step reads it
   }
   const R aL = dAL[i], aR = dAR[i];
 #pragma unroll
@@ -90,7 +91,8 @@ __device__ __forceinline__ void face_boundary(int i, const int *__restrict__ slo
 #pragma unroll
   for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
   boundary_state<ND, R>(bc, UL, nv, ph, UR);
-  waveSp[sL] = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  const R ws = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  if (waveSp) waveSp[sL] = ws;
   const R aL = dAL[i];
 #pragma unroll
   for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;

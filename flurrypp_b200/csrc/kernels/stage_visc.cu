@@ -135,10 +135,12 @@ __global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, cons
       gR[d][k] = dUf[d * dStride + (long long)sR * NF + k];
     }
   }
-  if (ND == 2 && ph.riemannType == 1)
+  if (ND == 2 && ph.riemannType == 1) {
     roe2d<R>(UL, UR, nv, R(ph.gamma), F);
-  else
-    waveSp[sL] = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  } else {
+    const R ws = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+    if (waveSp) waveSp[sL] = ws;  // null when no CFL time step reads it
+  }
   ldg_interior_flux<ND, R>(UL, UR, gL, gR, nv, ph, F);
   const R aL = dAL[i], aR = dAR[i];
 #pragma unroll
@@ -171,7 +173,8 @@ __global__ void k_faces_visc_boundary(int n0, int n, const int *__restrict__ slo
     for (int k = 0; k < NF; k++) g[d][k] = dUf[d * dStride + (long long)sL * NF + k];
   }
   boundary_state<ND, R>(bc, UL, nv, ph, UR);
-  waveSp[sL] = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  const R ws = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
+  if (waveSp) waveSp[sL] = ws;
   R Fv[ND][NF];
   if (bc == BC_ADI_NOSLIP) {
     // adiabatic wall: right gradient with the temperature gradient removed
