@@ -94,6 +94,36 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
+// One point's NF values of a tile row.  With 4 fields (2-D) the record is
+// 16-byte aligned and moves as one 128-bit shared-memory access (two for
+// FP64): four times fewer instructions than per-field accesses and no bank
+// conflicts; otherwise per field.
+template <int NF, typename R>
+__device__ __forceinline__ void ldp(const R *p, R (&v)[NF]) {
+  if constexpr (NF == 4 && std::is_same<R, float>::value) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else if constexpr (NF == 4 && std::is_same<R, double>::value) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; k++) v[k] = p[k];
+  }
+}
+template <int NF, typename R>
+__device__ __forceinline__ void stp(R *p, const R (&v)[NF]) {
+  if constexpr (NF == 4 && std::is_same<R, float>::value) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (NF == 4 && std::is_same<R, double>::value) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; k++) p[k] = v[k];
+  }
+}
+
 template <int ND, int P, typename R, int V, bool VISC>
 __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a, TpTablesT<R> t,
                                                                   const __grid_constant__ TmaMaps mp) {
@@ -196,7 +226,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
   // B: reference-space flux at (s, el)
   {
     R Fp[ND][NF];
-    const R *u = &sU[s * ROW + el * NF];
+    R u[NF];
+    ldp<NF, R>(&sU[s * ROW + el * NF], u);
     if (valid) {
       inviscid_flux<ND, R>(u, Fp, R(a.gamma));
       if (VISC) {
@@ -204,9 +235,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
         // (reference: solver.cpp:777-811)
         R gU[ND][NF], Fv[ND][NF];
 #pragma unroll
-        for (int d = 0; d < ND; d++)
-#pragma unroll
-          for (int k = 0; k < NF; k++) gU[d][k] = sF[(d * NS + s) * ROW + el * NF + k];
+        for (int d = 0; d < ND; d++) ldp<NF, R>(&sF[(d * NS + s) * ROW + el * NF], gU[d]);
         viscous_flux<ND, R>(u, gU, a.ph, Fv);
 #pragma unroll
         for (int d = 0; d < ND; d++)
@@ -222,14 +251,16 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
 #pragma unroll
     for (int d1 = 0; d1 < ND; d1++) {
       const R *Jr = &sJ[(d1 * NS + s) * EB * ND + el * ND];
+      R fk[NF];
 #pragma unroll
       for (int k = 0; k < NF; k++) {
         R f = R(0);
 #pragma unroll
         for (int d2 = 0; d2 < ND; d2++) f += Jr[d2] * Fp[d2][k];
-        sF[(d1 * NS + s) * ROW + el * NF + k] = f;
+        fk[k] = f;
         if (a.F_dbg && valid) a.F_dbg[(((long long)d1 * NS + s) * E + e) * NF + k] = f;
       }
+      stp<NF, R>(&sF[(d1 * NS + s) * ROW + el * NF], fk);
     }
   }
   __syncthreads();
@@ -251,7 +282,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
 #pragma unroll
     for (int m = 0; m < N; m++) {
       const R dv = Dr[m];
-      const R *x = &sF[(d * NS + base + m * stride) * ROW + el * NF];
+      R x[NF];
+      ldp<NF, R>(&sF[(d * NS + base + m * stride) * ROW + el * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
     }
@@ -278,16 +310,20 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
 #pragma unroll
     for (int m = 0; m < N; m++) {
       const R ev = sEF[side * N + m];
-      const R *x = &sF[(dn * NS + base + m * stride) * ROW + fe * NF];
+      R x[NF];
+      ldp<NF, R>(&sF[(dn * NS + base + m * stride) * ROW + fe * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
     }
     R *q = &sFn[f * ROW + fe * NF];
+    R qv[NF];
+    ldp<NF, R>(q, qv);
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      q[k] = q[k] - acc[k];
-      if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = q[k];
+      qv[k] = qv[k] - acc[k];
+      if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = qv[k];
     }
+    stp<NF, R>(q, qv);
   }
   if (tid == 0) tma_wait_read_all();  // the U0 store has read sU
   __syncthreads();
@@ -301,7 +337,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     for (int fc = 0; fc < 2 * ND; fc++) {
       const int fp = sCF[s * 2 * ND + fc];
       const R cv = sCV[s * 2 * ND + fc];
-      const R *x = &sFn[fp * ROW + el * NF];
+      R x[NF];
+      ldp<NF, R>(&sFn[fp * ROW + el * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) cq[k] += cv * x[k];
     }
@@ -309,47 +346,59 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     const R rdJ = needDet ? R(1.0) / sDet[s * EB + el] : R(1.0);
     const R dt = R(dtIn);
     const R rka = R(a.rka_next), rkb = R(a.rkb);
+    const int l0 = s * ROW + el * NF;
+    R vU[NF], vU0[NF], vAcc[NF], vCmp[NF];
+    if (a.mode != MODE_RESIDUAL) {
+      ldp<NF, R>(&sU[l0], vU);
+      if (needU0) ldp<NF, R>(&sU0[l0], vU0);
+      if (needAcc) ldp<NF, R>(&sAcc[l0], vAcc);
+      if (needCmp) ldp<NF, R>(&sCmp[l0], vCmp);
+    }
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      const int li = s * ROW + el * NF + k;
       const long long gi = ((long long)s * E + e) * NF + k;
       R dv = cq[k] + div[k];
       if (a.divF_out && valid) a.divF_out[gi] = dv;
       if (a.mode == MODE_RESIDUAL) continue;
       if (a.src && valid) dv = dv + a.src[gi];
-      const R u = sU[li];
+      const R u = vU[k];
       R unew;
       if constexpr (!F32) {
         if (a.mode == MODE_RK_STAGE) {
-          const R u0 = a.stage == 0 ? u : sU0[li];
+          const R u0 = a.stage == 0 ? u : vU0[k];
           unew = u0 - rka * dv * rdJ * dt;
-          const R base = a.stage == 0 ? u0 : sAcc[li];
-          sAcc[li] = base - rkb * dv * rdJ * dt;
+          const R base = a.stage == 0 ? u0 : vAcc[k];
+          vAcc[k] = base - rkb * dv * rdJ * dt;
         } else if (a.mode == MODE_RK_FINAL) {
-          const R base = a.nRK == 1 ? u : sAcc[li];
+          const R base = a.nRK == 1 ? u : vAcc[k];
           unew = base - rkb * dv * rdJ * dt;
         } else {
-          const R u0 = a.stage == 0 ? u : sU0[li];
+          const R u0 = a.stage == 0 ? u : vU0[k];
           unew = u0 - rka * dv * rdJ * dt;
         }
       } else {
         const R inc = dv * rdJ * dt;
         if (a.mode == MODE_RK_STAGE) {
-          const R u0 = a.stage == 0 ? u : sU0[li];
+          const R u0 = a.stage == 0 ? u : vU0[k];
           unew = u0 - rka * inc;
-          sAcc[li] = (a.stage == 0 ? R(0) : sAcc[li]) - rkb * inc;
+          vAcc[k] = (a.stage == 0 ? R(0) : vAcc[k]) - rkb * inc;
         } else if (finalStage) {
-          const R u0 = (a.mode == MODE_RK_FINAL && a.nRK > 1) || (a.mode == MODE_JAMESON && a.stage > 0) ? sU0[li] : u;
-          const R sum = a.mode == MODE_RK_FINAL ? (a.nRK > 1 ? sAcc[li] : R(0)) - rkb * inc : -(rka * inc);
+          const R u0 = (a.mode == MODE_RK_FINAL && a.nRK > 1) || (a.mode == MODE_JAMESON && a.stage > 0) ? vU0[k] : u;
+          const R sum = a.mode == MODE_RK_FINAL ? (a.nRK > 1 ? vAcc[k] : R(0)) - rkb * inc : -(rka * inc);
           R c;
-          two_sum(u0, sCmp[li] + sum, unew, c);
-          sCmp[li] = c;
+          two_sum(u0, vCmp[k] + sum, unew, c);
+          vCmp[k] = c;
         } else {
-          const R u0 = a.stage == 0 ? u : sU0[li];
+          const R u0 = a.stage == 0 ? u : vU0[k];
           unew = u0 - rka * inc;
         }
       }
-      sU[li] = unew;
+      vU[k] = unew;
+    }
+    if (a.mode != MODE_RESIDUAL) {
+      stp<NF, R>(&sU[l0], vU);
+      if (a.mode == MODE_RK_STAGE) stp<NF, R>(&sAcc[l0], vAcc);
+      if (needCmp) stp<NF, R>(&sCmp[l0], vCmp);
     }
   }
   if (a.mode == MODE_RESIDUAL) return;
@@ -378,13 +427,12 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
 #pragma unroll
     for (int m = 0; m < N; m++) {
       const R ev = sE[side * N + m];
-      const R *x = &sU[(base + m * stride) * ROW + fe * NF];
+      R x[NF];
+      ldp<NF, R>(&sU[(base + m * stride) * ROW + fe * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
     }
-    R *o = &sFn[f * ROW + fe * NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) o[k] = acc[k];
+    stp<NF, R>(&sFn[f * ROW + fe * NF], acc);
   }
   fence_async_smem();
   __syncthreads();
