@@ -32,6 +32,9 @@ struct DevBuf {
 
 }  // namespace
 
+// cases with fewer solution points than this do not time tile variants
+constexpr long long kTuneMinPoints = 1LL << 18;
+
 struct fr_case {
   std::string err;
   fr_setup_opts opts;
@@ -642,6 +645,9 @@ struct fr_case {
     int forced = opts.tile_variant;
     f32.tuneMs.assign(nv, -1.0f);
     if (forced >= nv) return fail(FR_ERR_ARG, "tile_variant out of range");
+    // small cases: launches of a few microseconds time as noise, so the
+    // choice is fixed (the first shape) and identical cases stay identical
+    if (forced < 0 && (long long)nS * E < kTuneMinPoints) forced = 0;
     int best = -1;
     float bestMs = 0.0f;
     const int tpEB = EB;
@@ -672,7 +678,10 @@ struct fr_case {
       cudaEventElapsedTime(&ms, e0, e1);
       ms /= reps;
       f32.tuneMs[v] = ms;
-      if (best < 0 || ms < bestMs) {
+      // the tensor-core variant differs from the CUDA-core ones by FP32
+      // round-off: it must win clearly, not by timing noise
+      const bool tcv = v == frk::tma_variants(true);
+      if (best < 0 || (tcv ? ms < 0.9f * bestMs : ms < bestMs)) {
         best = v;
         bestMs = ms;
       }
@@ -778,8 +787,9 @@ struct fr_case {
   // the FP64 arrays; all variants give bit-identical results.
   bool autotune_tiles64() {
     const int nv = frk::tma_variants(false);
-    const int forced = opts.tile_variant;
+    int forced = opts.tile_variant;
     if (forced >= nv) return fail(FR_ERR_ARG, "tile_variant out of range for the plain form");
+    if (forced < 0 && (long long)nS * E < kTuneMinPoints) forced = 0;  // small: fixed choice
     tuneMs64.assign(nv, -1.0f);
     int best = -1;
     float bestMs = 0.0f;

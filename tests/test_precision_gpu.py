@@ -84,11 +84,28 @@ def test_tile_variants_bit_identical(case):
         assert np.array_equal(o, outs[0])
 
 
-def test_autotuner_picks_a_variant():
+def test_autotuner_fixed_choice_on_a_small_case():
     a, meta = load_golden("tgv3d_p3_4")
     s = mixed_case(meta)
     inf = s.info()
-    assert inf.tensor_kernels == 2 and 0 <= inf.tile_variant < 3 and inf.elems_per_block % 4 == 0
+    assert inf.tensor_kernels == 2 and inf.tile_variant == 0 and inf.elems_per_block % 4 == 0
+
+
+def test_autotuner_times_variants_on_a_large_case(tmp_path):
+    """2-D P3, 128^2 elements (2^18 solution points): every tile variant is
+    timed at setup (the tensor-core one included) and the fastest CUDA-core
+    shape is kept unless the tensor-core kernel is clearly faster."""
+    from flurrypp_b200.decks import vortex_case
+
+    s = fb.Solver(vortex_case(str(tmp_path / "v.deck"), 128, 3, 0.5), precision=fb.FR_PREC_MIXED)
+    ms = s.get_array("tile_ms")
+    v = s.info().tile_variant
+    assert len(ms) == 4 and ms[3] > 0 and (ms[:3] > 0).sum() >= 2
+    cuda_core = [m for m in ms[:3] if m > 0]
+    if v == 3:
+        assert ms[3] < 0.9 * min(cuda_core)
+    else:
+        assert ms[v] == min(cuda_core)
 
 
 @pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "jameson5_2d_p2", "euler_fwd2d_p1"])
