@@ -13,6 +13,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <utility>
 
 namespace frk {
@@ -24,6 +25,19 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 // launch sequences, graph captures included).
 void set_pdl(bool on);
 bool pdl_enabled();
+
+// Opts kernel k into `bytes` of dynamic shared memory on the current device.
+// The attribute belongs to the device's context, so it is set once per
+// device; `done` (one per kernel, at the call site) records the devices.
+template <typename... KArgs>
+inline void smem_attr(void (*k)(KArgs...), int bytes, std::atomic<unsigned long long> &done) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done.fetch_or(bit, std::memory_order_acq_rel);
+}
 
 template <typename... KArgs, typename... Args>
 inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args &&...args) {

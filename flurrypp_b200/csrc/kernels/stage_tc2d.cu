@@ -354,11 +354,8 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
 template <int P>
 void launch_tc(const ElemArgsT<float> &a, const float *ops, const TmaMaps &m, cudaStream_t st) {
   using T = Tc<P>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_elem_tc2d<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attrDev{0};
+  smem_attr(k_elem_tc2d<P>, (int)T::SMEM, attrDev);
   launch_k(k_elem_tc2d<P>, (a.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, a, ops, m);
 }
 

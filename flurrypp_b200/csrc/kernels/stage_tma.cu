@@ -446,11 +446,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
 template <int ND, int P, typename R, int V, bool VISC = false>
 void launch_tma(const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m, cudaStream_t st) {
   using T = Tm<ND, P, R, V>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_elem_tma<ND, P, R, V, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attrDev{0};
+  smem_attr(k_elem_tma<ND, P, R, V, VISC>, (int)T::SMEM, attrDev);
   int g = (a.E + T::EB - 1) / T::EB;
   launch_k(k_elem_tma<ND, P, R, V, VISC>, g, T::NT, T::SMEM, st, a, t, m);
 }
@@ -658,11 +655,8 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
 template <int ND, int P, typename R>
 void launch_grad(int E, const TpTablesT<R> &t, const TmaMaps &m, unsigned int *err, cudaStream_t st) {
   using T = Tg2<ND, P, R>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_grad_tma<ND, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attrDev{0};
+  smem_attr(k_grad_tma<ND, P, R>, (int)T::SMEM, attrDev);
   launch_k(k_grad_tma<ND, P, R>, (E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, E, t, err, m);
 }
 

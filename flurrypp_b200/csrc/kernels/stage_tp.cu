@@ -267,11 +267,8 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
 template <int ND, int P, typename R, bool VISC = false>
 void launch_tp(const ElemArgsT<R> &a, const TpTablesT<R> &t, cudaStream_t st) {
   using T = Tp<ND, P, R>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_elem_tp<ND, P, VISC, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attrDev{0};
+  smem_attr(k_elem_tp<ND, P, VISC, R>, (int)T::SMEM, attrDev);
   int g = (a.E + T::EB - 1) / T::EB;
   launch_k(k_elem_tp<ND, P, VISC, R>, g, T::NT, T::SMEM, st, a, t);
 }

@@ -344,11 +344,8 @@ __global__ void __launch_bounds__(Tg<ND, P, R>::NT) k_elem_grad(GradArgsT<R> g, 
 template <int ND, int P, typename R>
 void launch_grad(const GradArgsT<R> &g, const TpTablesT<R> &t, cudaStream_t st) {
   using T = Tg<ND, P, R>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_elem_grad<ND, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attrDev{0};
+  smem_attr(k_elem_grad<ND, P, R>, (int)T::SMEM, attrDev);
   launch_k(k_elem_grad<ND, P, R>, (g.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, g, t);
 }
 

@@ -211,3 +211,30 @@ def test_plain_tile_variants_bit_identical(case):
         outs.append(s.get_state())
     assert np.array_equal(outs[0], outs[1])
     assert rel_err(outs[0], a["U_final"]) < STEP_TOL
+
+
+@pytest.mark.parametrize("precision", [fb.FR_PREC_FP64, fb.FR_PREC_MIXED])
+@pytest.mark.parametrize("case", ["vortex2d_p3_8", "pmg_vortex2d_p3_8", "ns_vortex2d_p3_6", "tgv3d_p3_4_perturbed"])
+def test_programmatic_launch_overlap_changes_nothing(case, precision):
+    """Small cases chain their launches with programmatic dependent launch
+    (each kernel's prologue overlaps the previous kernel's tail).  The same
+    steps with plain stream order give bit-identical states, in the
+    graph-replayed and the step-by-step loop."""
+    a, meta = load_golden(case)
+    if precision == fb.FR_PREC_MIXED and has_pmg(meta):
+        pytest.skip("P-multigrid runs in the plain form only")
+    outs = []
+    for no_pdl in (0, 1):
+        for graph in (True, False):
+            s = gpu_case(meta, precision=precision, no_pdl=no_pdl)
+            s.set_state(a["U_init"])
+            if graph:
+                s.run(4)
+            else:
+                for _ in range(4):
+                    s.update()
+                    if has_pmg(meta):  # fr_run's step: update, then the V-cycle
+                        s.pmg_cycle()
+            outs.append(s.get_state())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
