@@ -1308,7 +1308,7 @@ int create_common(const char *deck, const fr_mesh *mesh, const fr_setup_opts *op
     return e.find("open") != std::string::npos ? FR_ERR_ARG : FR_ERR_UNSUPPORTED;
   }
   if (mesh) {
-    if (mesh->nDims != c->in.nDims || (mesh->nNodes != (mesh->nDims == 2 ? 4 : 8)) || mesh->nEles <= 0 ||
+    if (mesh->nDims != c->in.nDims || !fr::shape_supported(mesh->nDims, mesh->nNodes) || mesh->nEles <= 0 ||
         !mesh->xv || !mesh->c2v) {
       c->err = "mesh does not match the deck (nDims / nNodes) or is empty";
       *out = c.release();

@@ -136,7 +136,9 @@ struct Operators {
 void build_operators(int nDims, int order, int ptsType, int vcjh, Operators &op);
 
 // --- mesh -------------------------------------------------------------------
-// Linear quads (4 nodes) or hexes (8 nodes), reference node ordering.
+// Quads or hexes of any geometric order the reference reads: Lagrange quads
+// of (n+1)^2 nodes, Lagrange hexes of (n+1)^3 nodes and the 20-node
+// serendipity hex, in Gmsh's node numbering (the first 4 or 8 are corners).
 struct Mesh {
   int nDims = 2;
   int nVerts = 0;
@@ -156,10 +158,11 @@ struct Mesh {
   std::vector<int> bndPointBc;
 };
 
-// Gmsh 2.x ASCII reader for linear quads (type 3) and hexes (type 5), with
-// $PhysicalNames boundaries mapped through the deck's mesh_bound entries
-// (reference: src/geo.cpp:1021-1475).  Higher-order (curved) elements are
-// rejected.
+// Gmsh 2.x ASCII reader for quads (types 3, 10, 36-38, 47-51) and hexes
+// (types 5, 12, 17, 92-94), with $PhysicalNames boundaries mapped through the
+// deck's mesh_bound entries (reference: src/geo.cpp:1021-1475).  Triangles,
+// tets and prisms (which the reference reads as collapsed quads and hexes) and
+// meshes mixing node counts are refused.
 bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err);
 
 // Cartesian generator (reference: src/geo.cpp:1477-1762): same vertex and
@@ -196,6 +199,8 @@ struct Geometry {
   std::vector<double> detJac_fpts;  // [nFpts][nEles]
 };
 bool build_geometry(const Mesh &m, int order, int ptsType, Geometry &g, std::string &err);
+// True when nNodes names a quad (nDims 2) or hex (nDims 3) shape above.
+bool shape_supported(int nDims, int nNodes);
 
 // Initial conditions.  kinds: 0 = reference icType of the deck
 // (src/ele.cpp:733-832), 1 = vortex (eps, xc, yc, Mach), 2 = Taylor-Green

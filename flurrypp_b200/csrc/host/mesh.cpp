@@ -141,6 +141,64 @@ void perturb_interior_vertices(const Input &in, Mesh &m, uint64_t seed, double f
   }
 }
 
+namespace {
+
+// Nodes of a Gmsh volume cell on the path: Lagrange quads (4, 9, 16, ...,
+// 121 nodes), Lagrange hexes (8, 27, 64, 125, 216) and the 20-node
+// serendipity hex (reference: src/geo.cpp:1160-1353).  -2: a simplex or prism
+// that the reference reads as a collapsed quad or hex; -1: unknown.
+int gmsh_cell_nodes(int type, int nd) {
+  if (nd == 2) {
+    switch (type) {
+      case 3: return 4;
+      case 10: return 9;
+      case 16: return 8;  // serendipity quad: refused by the shape functions
+      case 36: return 16;
+      case 37: return 25;
+      case 38: return 36;
+      case 47: return 49;
+      case 48: return 64;
+      case 49: return 81;
+      case 50: return 100;
+      case 51: return 121;
+      case 2: case 9: return -2;
+    }
+  } else {
+    switch (type) {
+      case 5: return 8;
+      case 17: return 20;
+      case 12: return 27;
+      case 92: return 64;
+      case 93: return 125;
+      case 94: return 216;
+      case 4: case 6: return -2;
+    }
+  }
+  return -1;
+}
+
+// Nodes of a boundary element that join its boundary's point set: every node
+// of an edge, the corners of a quad face (reference: src/geo.cpp:1388-1436).
+int gmsh_face_points(int type) {
+  switch (type) {
+    case 1: return 2;
+    case 2: return 3;
+    case 3: case 10: case 16: case 36: case 37: case 38: return 4;
+    case 8: return 3;
+    case 26: return 4;
+    case 27: return 5;
+    case 28: return 6;
+    case 62: return 7;
+    case 63: return 8;
+    case 64: return 9;
+    case 65: return 10;
+    case 66: return 11;
+  }
+  return -1;
+}
+
+}  // namespace
+
 bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err) {
   std::ifstream f(path);
   if (!f.is_open()) {
@@ -219,7 +277,7 @@ bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err) {
   f >> nEl;
   std::getline(f, line);
   std::vector<std::set<int>> pts(bndBc.size());
-  m.nNodes = nd == 2 ? 4 : 8;
+  m.nNodes = 0;
   m.c2v.clear();
   m.nEles = 0;
   for (long long k = 0; k < nEl; k++) {
@@ -235,20 +293,40 @@ bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err) {
       return false;
     }
     if (it->second == -1) {
-      int nv = type == 3 ? 4 : (type == 5 ? 8 : -1);
-      if (nv < 0 || nv != m.nNodes) {
+      const int nv = gmsh_cell_nodes(type, nd);
+      if (nv == -2) {
         err = "Gmsh element type " + std::to_string(type) +
-              " not on the B200 path (linear quads and hexes only)";
+              " (triangle, tetrahedron or prism read as a collapsed quad or hex) is not on the B200 path";
         return false;
       }
-      for (int v = 0; v < nv; v++) {
-        int g;
-        ss >> g;
-        m.c2v.push_back(g - 1);
+      if (nv < 0) {
+        err = "Gmsh element ID " + std::to_string(k) + ", type " + std::to_string(type) +
+              ": element type not recognized";
+        return false;
       }
+      if (m.nNodes == 0) m.nNodes = nv;
+      if (nv != m.nNodes) {
+        err = "elements with different node counts in one mesh (" + std::to_string(m.nNodes) + " and " +
+              std::to_string(nv) + ")";
+        return false;
+      }
+      int g[216];
+      for (int v = 0; v < nv; v++) ss >> g[v];
+      if (type == 17) {
+        // Gmsh lists the 20-node hex's mid-edge nodes by edge 0-1, 0-3, 0-4,
+        // 1-2, 1-5, 2-3, 2-6, 3-7, 4-5, 4-7, 5-6, 6-7; the serendipity shape
+        // functions number them 0-1, 1-2, 2-3, 3-0, 0-4, 1-5, 2-6, 3-7, 4-5,
+        // 5-6, 6-7, 7-4 (reference: src/geo.cpp:1284-1294)
+        static const int slot[12] = {8, 11, 12, 9, 13, 10, 14, 15, 16, 19, 17, 18};
+        int h[20];
+        for (int v = 0; v < 8; v++) h[v] = g[v];
+        for (int v = 0; v < 12; v++) h[slot[v]] = g[8 + v];
+        for (int v = 0; v < 20; v++) g[v] = h[v];
+      }
+      for (int v = 0; v < nv; v++) m.c2v.push_back(g[v] - 1);
       m.nEles++;
     } else {
-      int np = type == 1 ? 2 : (type == 3 ? 4 : (type == 8 ? 3 : (type == 10 || type == 16 ? 4 : -1)));
+      const int np = gmsh_face_points(type);
       if (np < 0) {
         err = "Boundary Element (Face) Type Not Recognized!";
         return false;
@@ -259,6 +337,10 @@ bool read_gmsh(const std::string &path, Input &in, Mesh &m, std::string &err) {
         pts[it->second].insert(g - 1);
       }
     }
+  }
+  if (m.nEles == 0) {
+    err = "no fluid elements in the Gmsh file";
+    return false;
   }
   m.bndFaceVerts.clear();
   m.bndFaceBc.clear();
@@ -308,48 +390,169 @@ Key4 face_key(const Mesh &m, int e, int f) {
   return k;
 }
 
-// Linear shape functions and derivatives (reference: src/funcs.cpp:145-600,
-// the Lagrange construction for 4-node quads and 8-node hexes).
+// Geometric shape functions (reference: src/funcs.cpp:145-1015).  Lagrange
+// quads of (n+1)^2 nodes and hexes of (n+1)^3 nodes interpolate on n+1
+// equidistant points per direction; their nodes are numbered shell by shell
+// from the outside in: corners, then the points inside each edge, then (hexes)
+// the points inside each face, each face numbered like a quad, then the next
+// shell; an odd count ends with the centre.  This is Gmsh's numbering, which
+// the reference reads unchanged.  The 20-node serendipity hex has corners
+// 0-7, then the mid-edge nodes of the bottom ring (8-11: edges 0-1, 1-2, 2-3,
+// 3-0), the vertical edges (12-15: above nodes 0-3) and the top ring (16-19).
 const double kHexXi[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
 const double kHexEta[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
 const double kHexMu[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
 
-inline double L1(double side, double x) { return side < 0 ? (x - 1.0) / (-2.0) : (x + 1.0) / 2.0; }
-inline double dL1(double side) { return side < 0 ? -0.5 : 0.5; }
+struct ShapeFn {
+  int nd = 2, nNodes = 4;
+  bool serendipity = false;
+  std::vector<double> xl;              // equidistant 1-D nodes on [-1, 1]
+  std::vector<std::array<int, 3>> ijk;  // per node: 1-D index along xi, eta, mu
 
-void shape(int nDims, const Pt &p, double *N) {
-  if (nDims == 2) {
-    for (int n = 0; n < 4; n++) N[n] = L1(kHexXi[n], p.x) * L1(kHexEta[n], p.y);
-  } else {
-    for (int n = 0; n < 8; n++) N[n] = L1(kHexXi[n], p.x) * L1(kHexEta[n], p.y) * L1(kHexMu[n], p.z);
-  }
-}
-
-void dshape(int nDims, const Pt &p, double *dN /*[nNodes][nDims]*/) {
-  if (nDims == 2) {
-    for (int n = 0; n < 4; n++) {
-      dN[2 * n + 0] = dL1(kHexXi[n]) * L1(kHexEta[n], p.y);
-      dN[2 * n + 1] = L1(kHexXi[n], p.x) * dL1(kHexEta[n]);
+  // (a, b) pairs of a quad's nodes whose 1-D indices run over [lo, hi]
+  static void quad_rings(int lo, int hi, std::vector<std::array<int, 2>> &out) {
+    const int n = hi - lo + 1;
+    for (int l = 0; l < n / 2; l++) {
+      const int a = lo + l, b = hi - l, m = n - 2 * (l + 1);
+      out.push_back({a, a});
+      out.push_back({b, a});
+      out.push_back({b, b});
+      out.push_back({a, b});
+      for (int k = 0; k < m; k++) out.push_back({a + 1 + k, a});
+      for (int k = 0; k < m; k++) out.push_back({b, a + 1 + k});
+      for (int k = 0; k < m; k++) out.push_back({b - 1 - k, b});
+      for (int k = 0; k < m; k++) out.push_back({a, b - 1 - k});
     }
-  } else {
-    for (int n = 0; n < 8; n++) {
-      dN[3 * n + 0] = dL1(kHexXi[n]) * L1(kHexEta[n], p.y) * L1(kHexMu[n], p.z);
-      dN[3 * n + 1] = L1(kHexXi[n], p.x) * dL1(kHexEta[n]) * L1(kHexMu[n], p.z);
-      dN[3 * n + 2] = L1(kHexXi[n], p.x) * L1(kHexEta[n], p.y) * dL1(kHexMu[n]);
+    if (n % 2) out.push_back({lo + n / 2, lo + n / 2});
+  }
+
+  bool init(int nDims, int nodes, std::string &err) {
+    nd = nDims;
+    nNodes = nodes;
+    serendipity = nd == 3 && nodes == 20;
+    ijk.clear();
+    if (serendipity) return true;
+    int nSide = 1;
+    while (nSide * nSide * (nd == 3 ? nSide : 1) < nodes) nSide++;
+    if (nSide < 2 || nSide * nSide * (nd == 3 ? nSide : 1) != nodes) {
+      err = nd == 2 ? "For Lagrange quad of order N, must have (N+1)^2 shape points."
+                    : "For Lagrange hex of order N, must have (N+1)^3 shape points.";
+      return false;
+    }
+    xl.resize(nSide);
+    const double dxi = 2. / (nSide - 1);
+    for (int i = 0; i < nSide; i++) xl[i] = -1. + i * dxi;
+    if (nd == 2) {
+      std::vector<std::array<int, 2>> q;
+      quad_rings(0, nSide - 1, q);
+      for (auto &ab : q) ijk.push_back({ab[0], ab[1], 0});
+      return true;
+    }
+    for (int l = 0; l < nSide / 2; l++) {
+      const int i = l, i2 = nSide - 1 - l, m = nSide - 2 * (l + 1);
+      const int c[8][3] = {{i, i, i},   {i2, i, i},   {i2, i2, i},   {i, i2, i},
+                           {i, i, i2},  {i2, i, i2},  {i2, i2, i2},  {i, i2, i2}};
+      for (auto &v : c) ijk.push_back({v[0], v[1], v[2]});
+      // edges 0-1, 0-3, 0-4, 1-2, 1-5, 2-3, 2-6, 3-7, 4-5, 4-7, 5-6, 6-7
+      for (int e = 0; e < 12; e++)
+        for (int k = 0; k < m; k++) {
+          const int r = i + 1 + k, rr = i2 - 1 - k;
+          const int t[12][3] = {{r, i, i},  {i, r, i},   {i, i, r},  {i2, r, i},  {i2, i, r},  {rr, i2, i},
+                                {i2, i2, r}, {i, i2, r}, {r, i, i2}, {i, r, i2}, {i2, r, i2}, {rr, i2, i2}};
+          ijk.push_back({t[e][0], t[e][1], t[e][2]});
+        }
+      // faces mu=lo, eta=lo, xi=lo, xi=hi, eta=hi, mu=hi, each a quad's rings
+      std::vector<std::array<int, 2>> q;
+      quad_rings(i + 1, i2 - 1, q);
+      for (auto &ab : q) ijk.push_back({ab[1], ab[0], i});
+      for (auto &ab : q) ijk.push_back({ab[0], i, ab[1]});
+      for (auto &ab : q) ijk.push_back({i, ab[1], ab[0]});
+      for (auto &ab : q) ijk.push_back({i2, ab[0], ab[1]});
+      for (auto &ab : q) ijk.push_back({nSide - 1 - ab[0], i2, ab[1]});
+      for (auto &ab : q) ijk.push_back({ab[0], ab[1], i2});
+    }
+    if (nSide % 2) ijk.push_back({nSide / 2, nSide / 2, nSide / 2});
+    return (int)ijk.size() == nodes;
+  }
+
+  // mid-edge node n of the serendipity hex: the varying direction and the
+  // sides of the other two (in xi, eta, mu order with the varying one skipped)
+  static void ser_edge(int n, int &axis, double &s1, double &s2) {
+    static const int ax[12] = {0, 1, 0, 1, 2, 2, 2, 2, 0, 1, 0, 1};
+    static const double a1[12] = {-1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1};
+    static const double a2[12] = {-1, -1, -1, -1, -1, -1, 1, 1, 1, 1, 1, 1};
+    axis = ax[n - 8];
+    s1 = a1[n - 8];
+    s2 = a2[n - 8];
+  }
+
+  void eval(const Pt &p, double *N) const {
+    const double x[3] = {p.x, p.y, p.z};
+    if (serendipity) {
+      for (int n = 0; n < 8; n++) {
+        const double sx = kHexXi[n], sy = kHexEta[n], sz = kHexMu[n];
+        N[n] = .125 * (1 + x[0] * sx) * (1 + x[1] * sy) * (1 + x[2] * sz) * (x[0] * sx + x[1] * sy + x[2] * sz - 2);
+      }
+      for (int n = 8; n < 20; n++) {
+        int a;
+        double s1, s2;
+        ser_edge(n, a, s1, s2);
+        const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+        N[n] = .25 * (1 - x[a] * x[a]) * (1 + x[b] * s1) * (1 + x[c] * s2);
+      }
+      return;
+    }
+    for (int n = 0; n < nNodes; n++) {
+      double v = lagrange(xl, x[0], ijk[n][0]) * lagrange(xl, x[1], ijk[n][1]);
+      if (nd == 3) v *= lagrange(xl, x[2], ijk[n][2]);
+      N[n] = v;
     }
   }
-}
 
-void point_pos(const Mesh &m, int e, const Pt &p, double *x) {
-  double N[8];
-  shape(m.nDims, p, N);
-  for (int d = 0; d < m.nDims; d++) {
-    x[d] = 0.0;
-    for (int n = 0; n < m.nNodes; n++) x[d] += N[n] * m.xv[(size_t)m.c2v[(size_t)e * m.nNodes + n] * m.nDims + d];
+  void deval(const Pt &p, double *dN /*[nNodes][nd]*/) const {
+    const double x[3] = {p.x, p.y, p.z};
+    if (serendipity) {
+      for (int n = 0; n < 8; n++) {
+        const double s[3] = {kHexXi[n], kHexEta[n], kHexMu[n]};
+        for (int d = 0; d < 3; d++) {
+          const int b = d == 0 ? 1 : 0, c = d == 2 ? 1 : 2;
+          dN[3 * n + d] = .125 * s[d] * (1 + x[b] * s[b]) * (1 + x[c] * s[c]) *
+                          (2 * x[d] * s[d] + x[b] * s[b] + x[c] * s[c] - 1);
+        }
+      }
+      for (int n = 8; n < 20; n++) {
+        int a;
+        double s1, s2;
+        ser_edge(n, a, s1, s2);
+        const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+        dN[3 * n + a] = -.5 * x[a] * (1 + x[b] * s1) * (1 + x[c] * s2);
+        dN[3 * n + b] = .25 * (1 - x[a] * x[a]) * s1 * (1 + x[c] * s2);
+        dN[3 * n + c] = .25 * (1 - x[a] * x[a]) * (1 + x[b] * s1) * s2;
+      }
+      return;
+    }
+    for (int n = 0; n < nNodes; n++) {
+      const double L0 = lagrange(xl, x[0], ijk[n][0]), L1 = lagrange(xl, x[1], ijk[n][1]);
+      const double D0 = dlagrange(xl, x[0], ijk[n][0]), D1 = dlagrange(xl, x[1], ijk[n][1]);
+      if (nd == 2) {
+        dN[2 * n + 0] = D0 * L1;
+        dN[2 * n + 1] = L0 * D1;
+      } else {
+        const double L2 = lagrange(xl, x[2], ijk[n][2]), D2 = dlagrange(xl, x[2], ijk[n][2]);
+        dN[3 * n + 0] = D0 * L1 * L2;
+        dN[3 * n + 1] = L0 * D1 * L2;
+        dN[3 * n + 2] = L0 * L1 * D2;
+      }
+    }
   }
-}
-
+};
 }  // namespace
+
+bool shape_supported(int nDims, int nNodes) {
+  ShapeFn sf;
+  std::string err;
+  return (nDims == 2 || nDims == 3) && nNodes >= 4 && nNodes <= 216 && sf.init(nDims, nNodes, err);
+}
 
 bool build_faces(const Mesh &m, int order, int ptsType, std::vector<Face> &faces, std::string &err) {
   const int nd = m.nDims;
@@ -357,6 +560,18 @@ bool build_faces(const Mesh &m, int order, int ptsType, std::vector<Face> &faces
   const int n1 = order + 1;
   const int nPF = nd == 2 ? n1 : n1 * n1;
   faces.clear();
+  if ((int)m.xv.size() < m.nVerts * nd || m.c2v.size() != (size_t)m.nEles * m.nNodes) {
+    err = "mesh arrays do not match their sizes";
+    return false;
+  }
+  for (int v : m.c2v)
+    if (v < 0 || v >= m.nVerts) {
+      err = "element node index out of range";
+      return false;
+    }
+  ShapeFn sf;
+  if (!sf.init(nd, m.nNodes, err)) return false;
+  const int nN = m.nNodes;
 
   // Boundary-face BC lookup by sorted vertex list.
   std::unordered_map<Key4, int, Key4Hash> bndBc;
@@ -470,12 +685,18 @@ bool build_faces(const Mesh &m, int order, int ptsType, std::vector<Face> &faces
 
   // Flux-point positions for orientation matching.
   auto fp = loc_fpts(nd, order, ptsType);
+  std::vector<double> Nf(fp.size() * nN);
+  for (size_t q = 0; q < fp.size(); q++) sf.eval(fp[q], &Nf[q * nN]);
   auto facePos = [&](int e, int f, std::vector<double> &out) {
-    out.resize((size_t)nPF * 3);
+    out.assign((size_t)nPF * 3, 0.0);
+    const int *cv = &m.c2v[(size_t)e * nN];
     for (int j = 0; j < nPF; j++) {
-      double x[3] = {0, 0, 0};
-      point_pos(m, e, fp[f * nPF + j], x);
-      for (int d = 0; d < 3; d++) out[(size_t)j * 3 + d] = x[d];
+      const double *N = &Nf[(size_t)(f * nPF + j) * nN];
+      for (int d = 0; d < nd; d++) {
+        double x = 0.0;
+        for (int n = 0; n < nN; n++) x += N[n] * m.xv[(size_t)cv[n] * nd + d];
+        out[(size_t)j * 3 + d] = x;
+      }
     }
   };
 
@@ -561,33 +782,36 @@ bool build_geometry(const Mesh &m, int order, int ptsType, Geometry &g, std::str
   g.norm_fpts.assign((size_t)nF * E * nd, 0.0);
   g.dA_fpts.assign((size_t)nF * E, 0.0);
 
-  std::vector<double> Ns((size_t)nS * 8), dNs((size_t)nS * 8 * 3), Nf((size_t)nF * 8), dNf((size_t)nF * 8 * 3);
+  ShapeFn sf;
+  if (!sf.init(nd, m.nNodes, err)) return false;
+  const int nN = m.nNodes;
+  std::vector<double> Ns((size_t)nS * nN), dNs((size_t)nS * nN * nd), Nf((size_t)nF * nN), dNf((size_t)nF * nN * nd);
   for (int s = 0; s < nS; s++) {
-    shape(nd, sp[s], &Ns[(size_t)s * 8]);
-    dshape(nd, sp[s], &dNs[(size_t)s * 24]);
+    sf.eval(sp[s], &Ns[(size_t)s * nN]);
+    sf.deval(sp[s], &dNs[(size_t)s * nN * nd]);
   }
   for (int f = 0; f < nF; f++) {
-    shape(nd, fp[f], &Nf[(size_t)f * 8]);
-    dshape(nd, fp[f], &dNf[(size_t)f * 24]);
+    sf.eval(fp[f], &Nf[(size_t)f * nN]);
+    sf.deval(fp[f], &dNf[(size_t)f * nN * nd]);
   }
+  std::vector<std::array<double, 3>> X(nN);
   static const double tq[4][2] = {{0, -1}, {1, 0}, {0, 1}, {-1, 0}};
   static const double th[6][3] = {{0, 0, -1}, {0, 0, 1}, {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}};
 
   for (int e = 0; e < E; e++) {
-    double X[8][3];
     for (int n = 0; n < m.nNodes; n++)
       for (int d = 0; d < nd; d++) X[n][d] = m.xv[(size_t)m.c2v[(size_t)e * m.nNodes + n] * nd + d];
     for (int s = 0; s < nS; s++) {
       double J[3][3] = {{0}};  // J[dref][dphys] = Jac_spts(dref, s, e, dphys)
       for (int d = 0; d < nd; d++) {
         double x = 0;
-        for (int n = 0; n < m.nNodes; n++) x += Ns[(size_t)s * 8 + n] * X[n][d];
+        for (int n = 0; n < m.nNodes; n++) x += Ns[(size_t)s * nN + n] * X[n][d];
         g.pos_spts[((size_t)s * E + e) * nd + d] = x;
       }
       for (int r = 0; r < nd; r++)
         for (int d = 0; d < nd; d++) {
           double v = 0;
-          for (int n = 0; n < m.nNodes; n++) v += dNs[(size_t)s * 24 + n * nd + r] * X[n][d];
+          for (int n = 0; n < m.nNodes; n++) v += dNs[((size_t)s * nN + n) * nd + r] * X[n][d];
           J[r][d] = v;
         }
       double det;
@@ -619,13 +843,13 @@ bool build_geometry(const Mesh &m, int order, int ptsType, Geometry &g, std::str
       double J[3][3] = {{0}};
       for (int d = 0; d < nd; d++) {
         double x = 0;
-        for (int n = 0; n < m.nNodes; n++) x += Nf[(size_t)f * 8 + n] * X[n][d];
+        for (int n = 0; n < m.nNodes; n++) x += Nf[(size_t)f * nN + n] * X[n][d];
         g.pos_fpts[((size_t)f * E + e) * nd + d] = x;
       }
       for (int r = 0; r < nd; r++)
         for (int d = 0; d < nd; d++) {
           double v = 0;
-          for (int n = 0; n < m.nNodes; n++) v += dNf[(size_t)f * 24 + n * nd + r] * X[n][d];
+          for (int n = 0; n < m.nNodes; n++) v += dNf[((size_t)f * nN + n) * nd + r] * X[n][d];
           J[r][d] = v;
         }
       double det, A[3][3];

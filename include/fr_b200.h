@@ -76,8 +76,8 @@ typedef struct fr_mesh {
   int nVerts;
   const double *xv;       /* [nVerts][nDims] */
   int nEles;
-  int nNodes;             /* 4 (quad) or 8 (hex) */
-  const int *c2v;         /* [nEles][nNodes] */
+  int nNodes;             /* quads: 4, 9, 16, ... (n+1)^2; hexes: 8, 20, 27, ... (n+1)^3 */
+  const int *c2v;         /* [nEles][nNodes], Gmsh node order (corners first) */
   int nBndFaces;
   const int *bndFaceVerts; /* [nBndFaces][4] (2-D: last two entries ignored) */
   const int *bndFaceBc;    /* [nBndFaces] */

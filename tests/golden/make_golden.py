@@ -11,11 +11,22 @@ disFn_fpts, divF) and the state after N time steps.
 
 Requires the reference build (this container); the committed .npz files are
 what the tests read.
+
+Meshes: the curved (high-order) meshes are generated here by
+``flurrypp_b200.meshgen.curved_box``; three of the reference's own test meshes
+(``tests/euler/cylinder/cylinder2D.msh``, ``cylinder3D.msh`` and
+``tests/euler/naca/naca0012_structured_coarse.msh``) are copied unchanged as
+parity inputs, the two large ones gzip-compressed.  Cases on the large meshes
+keep a per-element summary of the setup arrays and the full face table
+("summary" cases) instead of full arrays.
 """
 from __future__ import annotations
 
+import gzip
 import json
+import math
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -75,7 +86,78 @@ CASES = {
     "chbump_p2_pmg": ("chbump_p2_pmg", [], 5, "all"),
     "chbump_p3": ("chbump_p3", [], 10, "all"),
     "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5"], 5, "all"),
+    "curved2d_q2_p3": ("curved2d_q2_p3", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),
+    "curved2d_q4_p2": ("curved2d_q4_p2", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),
+    "curved3d_q2_p2": ("curved3d_q2_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 4, "all"),
+    "curved3d_s20_p2": ("curved3d_s20_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 4, "all"),
+    "curved3d_q3_p3": ("curved3d_q3_p3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 3, "all"),
+    "cyl2d_p2": ("cyl2d_p2", [], 10, "all"),
+    "naca_p4": ("naca_p4", [], 0, "summary"),
+    "cyl3d_p2": ("cyl3d_p2", [], 0, "summary"),
 }
+
+DECKS = os.path.join(HERE, "decks")
+REFERENCE = "/root/reference"
+# generated curved meshes: file -> (nDims, n per direction, geometric order, box length, serendipity)
+CURVED = {
+    "curved2d_q2.msh": (2, 6, 2, 10.0, False),
+    "curved2d_q4.msh": (2, 3, 4, 10.0, False),
+    "curved3d_q2.msh": (3, 3, 2, 2 * math.pi, False),
+    "curved3d_s20.msh": (3, 3, 2, 2 * math.pi, True),
+    "curved3d_q3.msh": (3, 2, 3, 2 * math.pi, False),
+}
+# the reference's own test meshes: file here -> path in the reference tree
+REF_MESHES = {
+    "cylinder2D.msh": "tests/euler/cylinder/cylinder2D.msh",
+    "cylinder3D.msh.gz": "tests/euler/cylinder/cylinder3D.msh",
+    "naca0012_structured_coarse.msh.gz": "tests/euler/naca/naca0012_structured_coarse.msh",
+}
+
+
+def write_meshes() -> None:
+    sys.path.insert(0, ROOT)
+    from flurrypp_b200.meshgen import curved_box, write_gmsh_ho
+    for name, (nd, n, q, length, ser) in CURVED.items():
+        write_gmsh_ho(os.path.join(DECKS, name), curved_box(nd, n, q, length, serendipity=ser))
+    for name, rel in REF_MESHES.items():
+        src = os.path.join(REFERENCE, rel)
+        if name.endswith(".gz"):
+            with open(src, "rb") as fi, gzip.GzipFile(os.path.join(DECKS, name), "wb", 9, mtime=0) as fo:
+                shutil.copyfileobj(fi, fo)
+        else:
+            shutil.copyfile(src, os.path.join(DECKS, name))
+
+
+def stage_deck(deck: str, where: str) -> str:
+    """Copy a deck and its mesh (decompressed) into `where`; returns the deck path."""
+    dst = os.path.join(where, deck + ".deck")
+    shutil.copyfile(os.path.join(DECKS, deck + ".deck"), dst)
+    mesh = None
+    for line in open(dst):
+        t = line.split()
+        if len(t) > 1 and t[0] == "meshFileName":
+            mesh = t[1]
+    if mesh:
+        if os.path.exists(os.path.join(DECKS, mesh)):
+            shutil.copyfile(os.path.join(DECKS, mesh), os.path.join(where, mesh))
+        else:
+            with gzip.open(os.path.join(DECKS, mesh + ".gz"), "rb") as fi, open(os.path.join(where, mesh), "wb") as fo:
+                shutil.copyfileobj(fi, fo)
+    return dst
+
+
+def setup_summary(a: dict) -> dict:
+    """Per-element reductions of the setup arrays plus the face table: what the
+    summary cases keep (also computed by the tests from the product's arrays)."""
+    E = a["detJac_spts"].shape[1]
+    nd = a["norm_fpts"].shape[-1]
+    return {
+        "sum_detJac_spts": a["detJac_spts"].sum(axis=0),
+        "sum_dA_fpts": a["dA_fpts"].reshape(-1, E).sum(axis=0),
+        "sum_norm_fpts": a["norm_fpts"].reshape(-1, E, nd).sum(axis=0),
+        "sum_pos_spts": a["pos_spts"].reshape(-1, E, nd).sum(axis=0),
+        "sum_JGinv_spts": a["JGinv_spts"].reshape(nd, -1, E, nd).sum(axis=1),
+    }
 
 
 def read_dump(d: str) -> tuple[dict, dict]:
@@ -98,14 +180,19 @@ def read_dump(d: str) -> tuple[dict, dict]:
 
 def run_case(name: str) -> None:
     deck, args, steps, keep = CASES[name]
-    deck_path = os.path.join(HERE, "decks", deck + ".deck")
-    with tempfile.TemporaryDirectory() as td:
+    with tempfile.TemporaryDirectory() as td, tempfile.TemporaryDirectory() as wd:
+        deck_path = stage_deck(deck, wd)
         cmd = [HARNESS, deck_path, td] + args + ["--steps", str(steps)]
         # mesh files named in a deck are relative to the deck's directory
-        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=os.path.join(HERE, "decks"))
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=wd)
         arrays, meta = read_dump(td)
-    names = SETUP + RESID + FINAL if keep == "all" else keep
-    out = {k: arrays[k] for k in names if k in arrays}
+    if keep == "summary":
+        out = setup_summary(arrays)
+        for k in ["face_eL", "face_locL", "face_eR", "face_locR", "face_bc", "face_fptR"]:
+            out["ref_" + k] = arrays[k]
+    else:
+        names = SETUP + RESID + FINAL if keep == "all" else keep
+        out = {k: arrays[k] for k in names if k in arrays}
     meta.update({"case": name, "deck": deck, "harness_args": args, "steps": steps})
     out["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
@@ -115,6 +202,7 @@ def run_case(name: str) -> None:
 def main(argv: list[str]) -> None:
     if not os.path.exists(HARNESS):
         sys.exit(f"{HARNESS} missing: run `make -C oracle` first")
+    write_meshes()
     for name in argv or list(CASES):
         run_case(name)
 
