@@ -135,6 +135,9 @@ def _load() -> ctypes.CDLL:
         "fr_get_array": (i, [P, ctypes.c_char_p, P, ctypes.POINTER(sz)]),
         "fr_device_ptr": (i, [P, ctypes.c_char_p, ctypes.POINTER(P), ctypes.POINTER(sz)]),
         "fr_synchronize": (i, [P]),
+        "fr_checkpoint": (i, [P]),
+        "fr_write_data": (i, [P, ctypes.c_char_p]),
+        "fr_read_restart": (i, [P, ctypes.c_char_p]),
         "fr_bench_kernel": (i, [P, ctypes.c_char_p, i]),
         "fr_batch_create": (i, [ctypes.POINTER(P), i, ctypes.POINTER(P)]),
         "fr_batch_run": (i, [P, i]),
@@ -249,6 +252,18 @@ class Solver:
 
     def pmg_cycle(self):
         self._check(lib.fr_pmg_cycle(self._c))
+
+    def checkpoint(self):
+        """Snapshot for output; the copy to the host overlaps later steps."""
+        self._check(lib.fr_checkpoint(self._c))
+
+    def write_data(self, path: str | None = None):
+        """writeData: ParaView .vtu (plotType 1) or CSV (plotType 0)."""
+        self._check(lib.fr_write_data(self._c, path.encode() if path else None))
+
+    def read_restart(self, path: str | None = None):
+        """readRestartFile: state and time from a .vtu (deck name if None)."""
+        self._check(lib.fr_read_restart(self._c, path.encode() if path else None))
 
     def calc_dt(self) -> float:
         d = ctypes.c_double()

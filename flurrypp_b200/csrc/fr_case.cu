@@ -108,7 +108,26 @@ struct fr_case {
     std::vector<float> tuneMs;  // element-stage time per tile variant (autotuner)
   } f32;
 
+  // solution output: primitive variables at the plot points, copied to a
+  // pinned host buffer on a side stream so that stepping goes on meanwhile
+  struct Checkpoint {
+    double *opp = nullptr;   // [nPpts][nSpts] spts -> plot points
+    double *Vp = nullptr;    // [nPpts][E][nF], then the time
+    double *host = nullptr;  // pinned copy of Vp
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ready = nullptr, done = nullptr;
+    bool pending = false;
+    long long iter = 0;
+    int nP = 0;
+    std::vector<double> pos;  // plot-point positions [nPpts][E][nDims]
+  } cp;
+
   ~fr_case() {
+    if (cp.copy) cudaStreamSynchronize(cp.copy);
+    if (cp.host) cudaFreeHost(cp.host);
+    if (cp.ready) cudaEventDestroy(cp.ready);
+    if (cp.done) cudaEventDestroy(cp.done);
+    if (cp.copy) cudaStreamDestroy(cp.copy);
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
     levels.clear();  // coarse levels use this case's stream: release them first
@@ -1490,6 +1509,9 @@ int fr_init_solution(fr_case *c, int kind, const double *prm, int nprm) {
     c->err = "host-only case: no device state";
     return FR_ERR_STATE;
   }
+  // solver::initializeSolution (src/solver.cpp:1896-1899): a restart deck
+  // reads its state from the restart file
+  if (kind == fr::IC_DECK && c->in.restart) return fr_read_restart(c, nullptr);
   std::vector<double> U;
   std::string e;
   if (!fr::initial_condition(c->in, c->geo, c->nS, c->E, kind, prm, nprm, U, e)) {
@@ -1984,6 +2006,128 @@ int fr_stream_idle(fr_case *c) {
   cudaGetLastError();
   c->err = std::string("stream query: ") + cudaGetErrorString(e);
   return -FR_ERR_CUDA;
+}
+
+int fr_checkpoint(fr_case *c) {
+  PdlScope pdlScope(c);
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = c->hostOnly ? "host-only case: no device state" : "no state set";
+    return FR_ERR_STATE;
+  }
+  auto &k = c->cp;
+  const int n3 = c->in.order + 3;
+  const size_t nV = (size_t)(c->nDims == 2 ? n3 * n3 : n3 * n3 * n3) * c->E * c->nF + 1;
+  if (!k.Vp) {
+    k.nP = c->nDims == 2 ? n3 * n3 : n3 * n3 * n3;
+    if (!c->upload(k.opp, fr::spts_to_ppts(c->nDims, c->in.order, c->in.sptsTypeQuad)) || !c->alloc(k.Vp, nV))
+      return FR_ERR_CUDA;
+    if (cudaMallocHost(&k.host, nV * sizeof(double)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&k.copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&k.ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      c->err = "cannot allocate the checkpoint buffers";
+      return FR_ERR_CUDA;
+    }
+  }
+  // the previous copy must have left Vp before the kernel overwrites it
+  if (k.pending) cudaStreamWaitEvent(c->stream, k.done, 0);
+  if (c->mixed) c->join_state();
+  frk::launch_plot_primitives(c->nDims, c->U, k.opp, k.Vp, c->nS, k.nP, c->E, c->in.gamma, c->stream);
+  c->launches++;
+  cudaMemcpyAsync(k.Vp + nV - 1, c->timeAcc, sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  cudaEventRecord(k.ready, c->stream);
+  cudaStreamWaitEvent(k.copy, k.ready, 0);
+  cudaMemcpyAsync(k.host, k.Vp, nV * sizeof(double), cudaMemcpyDeviceToHost, k.copy);
+  cudaEventRecord(k.done, k.copy);
+  k.pending = true;
+  k.iter = c->iter;
+  return c->cuda_ok("checkpoint") ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_write_data(fr_case *c, const char *path) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = c->hostOnly ? "host-only case: no device state" : "no state set";
+    return FR_ERR_STATE;
+  }
+  std::string e;
+  char name[64];
+  if (c->in.plotType == 0) {
+    // src/output.cpp:60-135: primitives at the solution and flux points
+    const size_t nU = (size_t)c->nS * c->E * c->nF, nUf = (size_t)c->nFp * c->E * c->nF;
+    std::vector<double> U(nU), Uf(nUf);
+    size_t cnt = nU;
+    int st = fr_get_array(c, "U_spts", U.data(), &cnt);
+    if (st != FR_OK) return st;
+    if (!c->fptsFresh) c->extrapolate();
+    cnt = nUf;
+    if ((st = fr_get_array(c, "U_fpts", Uf.data(), &cnt)) != FR_OK) return st;
+    std::snprintf(name, sizeof name, ".csv.%.09lld", c->iter);
+    const std::string out = path ? std::string(path) : c->in.dataFileName + name;
+    if (!fr::write_csv(out, c->nDims, c->nS, c->nFp, c->E, U.data(), Uf.data(), c->geo.pos_spts.data(),
+                       c->geo.pos_fpts.data(), c->in.gamma, e)) {
+      c->err = e;
+      return FR_ERR_ARG;
+    }
+    return FR_OK;
+  }
+  auto &k = c->cp;
+  if (!k.pending) {
+    const int st = fr_checkpoint(c);
+    if (st != FR_OK) return st;
+  }
+  if (cudaEventSynchronize(k.done) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "checkpoint copy failed";
+    return FR_ERR_CUDA;
+  }
+  k.pending = false;
+  if (k.pos.empty() &&
+      !fr::positions_at(c->mesh, fr::loc_ppts(c->nDims, c->in.order, c->in.sptsTypeQuad), k.pos, e)) {
+    c->err = e;
+    return FR_ERR_ARG;
+  }
+  std::snprintf(name, sizeof name, "_%.09lld.vtu", k.iter);
+  const std::string out = path ? std::string(path) : c->in.dataFileName + name;
+  const double time = k.host[(size_t)k.nP * c->E * c->nF];
+  if (!fr::write_paraview(out, c->nDims, c->in.order, c->E, time, k.iter, k.host, k.pos.data(), e)) {
+    c->err = e;
+    return FR_ERR_ARG;
+  }
+  return FR_OK;
+}
+
+int fr_read_restart(fr_case *c, const char *path) {
+  if (!c) return FR_ERR_ARG;
+  if (c->hostOnly) {
+    c->err = "host-only case: no device state";
+    return FR_ERR_STATE;
+  }
+  char name[64];
+  std::snprintf(name, sizeof name, "_%.09d.vtu", c->in.restartIter);
+  const std::string in = path ? std::string(path) : c->in.dataFileName + name;
+  std::vector<double> U;
+  double time = 0.0;
+  long long iter = 0;
+  bool hasTime = false, hasIter = false;
+  std::string e;
+  if (!fr::read_restart_vtu(in, c->in, c->in.order, c->E, U, time, hasTime, iter, hasIter, e)) {
+    c->err = e;
+    return FR_ERR_ARG;
+  }
+  int st = fr_set_state(c, U.data(), U.size());
+  if (st != FR_OK) return st;
+  // src/solver.cpp:1829-1836: the simulation time from the file's comment;
+  // the iteration count is the deck's restartIter (src/input.cpp:463-467)
+  if (hasTime && cudaMemcpy(c->timeAcc, &time, sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    c->err = "cudaMemcpy H2D failed";
+    return FR_ERR_CUDA;
+  }
+  if (!path) c->iter = c->in.restartIter;
+  else if (hasIter) c->iter = iter;
+  return FR_OK;
 }
 
 int fr_synchronize(fr_case *c) {

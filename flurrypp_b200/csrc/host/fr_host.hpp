@@ -87,7 +87,10 @@ struct Input {
   int sptsTypeQuad = PTS_LEGENDRE;
   int vcjhSchemeQuad = 0;
   int PMG = 0, lowOrder = 0, smoothSteps = 1;
-  int restart = 0;
+  int restart = 0, restartIter = 0;
+  // output (reference: src/input.cpp:428-433)
+  std::string dataFileName = "simData";
+  int plotType = 1, plotFreq = 100;
   // derived
   int nRKSteps = 4;
   std::vector<double> RKa, RKb;
@@ -201,6 +204,28 @@ struct Geometry {
 bool build_geometry(const Mesh &m, int order, int ptsType, Geometry &g, std::string &err);
 // True when nNodes names a quad (nDims 2) or hex (nDims 3) shape above.
 bool shape_supported(int nDims, int nNodes);
+// Physical positions of reference-space points `loc` in every element,
+// [point][element][nDims] (reference: src/solver.cpp:1248-1313, shape_ppts).
+bool positions_at(const Mesh &m, const std::vector<Pt> &loc, std::vector<double> &pos, std::string &err);
+
+// --- solution files (output.cpp) ---------------------------------------------
+// Plot points: the (P+3)^d grid of -1, the solution points' 1-D set, +1
+// (reference: src/points.cpp:164-196), and the interpolation from the
+// solution points, [nPpts][nSpts] (src/operators.cpp:145-165).
+std::vector<Pt> loc_ppts(int nDims, int order, int ptsType);
+std::vector<double> spts_to_ppts(int nDims, int order, int ptsType);
+// The reference's ParaView file from primitive variables at the plot points
+// Vp [nPpts][E][nDims+2] and their positions [nPpts][E][nDims].
+bool write_paraview(const std::string &path, int nDims, int order, int E, double time, long long iter,
+                    const double *Vp, const double *pos, std::string &err);
+// The reference's CSV file: primitives at the solution then flux points.
+bool write_csv(const std::string &path, int nDims, int nS, int nFp, int E, const double *U, const double *Ufpts,
+               const double *posS, const double *posF, double gamma, std::string &err);
+// State [nS][E][nF] of a case of order `order` from a ParaView restart file
+// of any order (interpolated when the orders differ), with its TIME and
+// ITER comments when present.
+bool read_restart_vtu(const std::string &path, const Input &in, int order, int E, std::vector<double> &U,
+                      double &time, bool &hasTime, long long &iter, bool &hasIter, std::string &err);
 
 // Initial conditions.  kinds: 0 = reference icType of the deck
 // (src/ele.cpp:733-832), 1 = vortex (eps, xc, yc, Mach), 2 = Taylor-Green

@@ -142,6 +142,10 @@ bool read_deck(const std::string &path, Input &in, std::string &err) {
     d.get("nzWall", in.nzWall);
   }
   d.get("restart", in.restart);
+  if (in.restart) d.get("restartIter", in.restartIter);
+  d.get("dataFileName", in.dataFileName);
+  d.get("plotType", in.plotType);
+  d.get("plotFreq", in.plotFreq);
   d.get("meshType", in.meshType);
   if (in.meshType == 1) {
     d.get("nx", in.nx);

@@ -554,6 +554,25 @@ bool shape_supported(int nDims, int nNodes) {
   return (nDims == 2 || nDims == 3) && nNodes >= 4 && nNodes <= 216 && sf.init(nDims, nNodes, err);
 }
 
+bool positions_at(const Mesh &m, const std::vector<Pt> &loc, std::vector<double> &pos, std::string &err) {
+  ShapeFn sf;
+  if (!sf.init(m.nDims, m.nNodes, err)) return false;
+  const int nd = m.nDims, nN = m.nNodes, E = m.nEles, nP = (int)loc.size();
+  std::vector<double> N((size_t)nP * nN);
+  for (int q = 0; q < nP; q++) sf.eval(loc[q], &N[(size_t)q * nN]);
+  pos.assign((size_t)nP * E * nd, 0.0);
+  for (int e = 0; e < E; e++) {
+    const int *cv = &m.c2v[(size_t)e * nN];
+    for (int q = 0; q < nP; q++)
+      for (int d = 0; d < nd; d++) {
+        double x = 0.0;
+        for (int k = 0; k < nN; k++) x += N[(size_t)q * nN + k] * m.xv[(size_t)cv[k] * nd + d];
+        pos[((size_t)q * E + e) * nd + d] = x;
+      }
+  }
+  return true;
+}
+
 bool build_faces(const Mesh &m, int order, int ptsType, std::vector<Face> &faces, std::string &err) {
   const int nd = m.nDims;
   const int nLocF = nd == 2 ? 4 : 6;

@@ -242,6 +242,9 @@ void launch_check_state(int nS, int E, int nF, const R *U, unsigned int *bad, cu
 //   join    : (U32, comp) -> U64 = U32 + comp
 //   narrow  : FP64 -> FP32 (metrics, normals, face areas)
 //   widen   : FP32 -> FP64 (residuals, traces read back by tools)
+// Primitive variables at the plot points from the FP64 state (output only).
+void launch_plot_primitives(int nDims, const double *U, const double *opp, double *Vp, int nS, int nP, int E,
+                            double gamma, cudaStream_t st);
 void launch_split(long long n, const double *U64, float *U32, float *comp, cudaStream_t st);
 void launch_join(long long n, const float *U32, const float *comp, double *U64, cudaStream_t st);
 void launch_narrow(long long n, const double *in, float *out, cudaStream_t st);

@@ -1,8 +1,11 @@
 // Minimal FlurryPP-style driver on the B200 path (reference: src/flurry.cpp:71-188):
-// read a deck, set up, apply the deck's initial condition, take N steps of
-// update(), printing the residual norm every `freq` steps and at the end.
+// read a deck, set up, apply the deck's initial condition (or its restart
+// file), take N steps of update(), printing the residual norm every `freq`
+// steps and at the end.  With WRITE = 1 it also writes the deck's solution
+// files like the reference's loop: at the start, every plotFreq iterations
+// (taken as checkpoints, written while the next steps run) and at the end.
 //
-//   flurry_b200 DECK NSTEPS [FREQ]
+//   flurry_b200 DECK NSTEPS [FREQ [WRITE [PLOTFREQ]]]
 #include <cstdio>
 #include <cstdlib>
 
@@ -15,6 +18,8 @@ int main(int argc, char **argv) {
   }
   const int nsteps = std::atoi(argv[2]);
   const int freq = argc > 3 ? std::atoi(argv[3]) : 10;
+  const bool write = argc > 4 && std::atoi(argv[4]) != 0;
+  const int plotFreq = argc > 5 ? std::atoi(argv[5]) : 100;
   try {
     fr::b200::Solver S;
     S.setup(argv[1]);
@@ -22,8 +27,19 @@ int main(int argc, char **argv) {
     const fr_info &inf = S.info();
     std::printf("case: nDims %d order %d nEles %d nSpts %d nFields %d\n", inf.nDims, inf.order, inf.nEles,
                 inf.nSpts, inf.nFields);
+    if (write) S.writeData();
+    const long long iter0 = S.info().iter;
+    bool pending = false;
     for (int iter = 1; iter <= nsteps; iter++) {
       S.update();
+      if (write && pending) {  // the previous checkpoint's copy overlapped this step
+        S.writeData();
+        pending = false;
+      }
+      if (write && ((iter0 + iter) % plotFreq == 0 || iter == nsteps)) {
+        S.checkpoint();
+        pending = true;
+      }
       if (iter % freq == 0 || iter == nsteps) {
         auto r = S.residualNorm(2);
         std::printf("iter %6d  time %.10e  res", iter, S.info().time);
@@ -31,6 +47,7 @@ int main(int argc, char **argv) {
         std::printf("\n");
       }
     }
+    if (pending) S.writeData();
   } catch (const fr::b200::Error &e) {
     std::fprintf(stderr, "fr_b200 error %d: %s\n", e.code, e.what());
     return 1;

@@ -169,6 +169,28 @@ int fr_check_state(fr_case *c);
  * "face_fptR" (ints).  *count on input: capacity in elements; on output: size. */
 int fr_get_array(fr_case *c, const char *name, void *host, size_t *count);
 
+/* ---- Solution files --------------------------------------------------------
+ * fr_checkpoint takes a snapshot of the current state for output: one kernel
+ * on the case's stream forms the primitive variables at the plot points, and
+ * their copy to pinned host memory runs on a side stream, so the caller can
+ * keep stepping while it is in flight.  A later checkpoint replaces one that
+ * was not written yet.
+ * fr_write_data writes the latest checkpoint (taking one first if none is
+ * pending) as the reference's writeData does (src/output.cpp:43-58): with
+ * the deck's plotType 1 a ParaView file <dataFileName>_<iter, 9 digits>.vtu
+ * in the reference's layout (src/output.cpp:137-512); with plotType 0 the CSV
+ * <dataFileName>.csv.<iter> of primitives at the solution and flux points
+ * (output.cpp:60-135, synchronous).  `path` NULL: that name, else `path`.
+ * fr_read_restart sets the state and time from a ParaView file as
+ * solver::readRestartFile does (src/solver.cpp:1789-1890, ele.cpp:1497-1921),
+ * interpolating when the file's order differs from the case's; `path` NULL:
+ * <dataFileName>_<restartIter>.vtu of the deck, and the iteration count
+ * becomes restartIter.  fr_init_solution with kind 0 on a deck with
+ * "restart 1" reads that file instead of the initial condition. */
+int fr_checkpoint(fr_case *c);
+int fr_write_data(fr_case *c, const char *path);
+int fr_read_restart(fr_case *c, const char *path);
+
 /* Device pointer of a state array ("U_spts", "U_fpts", "divF_0", ...) for
  * callers that keep data resident (no copy).  Valid until fr_destroy. */
 int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes);

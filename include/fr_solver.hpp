@@ -75,6 +75,13 @@ class Solver {
     return r;
   }
 
+  // writeData (src/output.cpp:43-58): ParaView or CSV per the deck's
+  // plotType; checkpoint() snapshots the state so the file can be written
+  // later while stepping goes on; readRestartFile (src/solver.cpp:1789-1890)
+  void checkpoint() { check(fr_checkpoint(c_)); }
+  void writeData(const char *path = nullptr) { check(fr_write_data(c_, path)); }
+  void readRestartFile(const char *path = nullptr) { check(fr_read_restart(c_, path)); }
+
   const fr_info &info() {
     check(fr_get_info(c_, &info_));
     return info_;

@@ -24,6 +24,9 @@
  *   --steps N                     time steps after the residual dump
  *   --time K,W                    W untimed then K timed steps, print JSON
  *   --threads T                   OpenMP threads (omp build)
+ *   --write-vtu PREFIX            after the steps, writeData with dataFileName
+ *                                 PREFIX (the deck's plotType: 1 ParaView
+ *                                 PREFIX_<iter>.vtu, 0 CSV PREFIX.csv.<iter>)
  */
 #define private public
 #define protected public
@@ -34,6 +37,7 @@
 #include "intFace.hpp"
 #include "boundFace.hpp"
 #include "ele.hpp"
+#include "output.hpp"
 #undef private
 #undef protected
 
@@ -98,6 +102,7 @@ struct Opts {
   int steps = 0;
   int timeK = 0, timeW = 0;
   int threads = 0;
+  std::string vtu;
 };
 
 /* Uniform double in [0,1) from the top 53 bits of a 64-bit Mersenne twister
@@ -284,6 +289,7 @@ int main(int argc, char **argv) {
     else if (a == "--time") {
       if (sscanf(next(), "%d,%d", &o.timeK, &o.timeW) != 2) exit(2);
     } else if (a == "--threads") o.threads = atoi(next());
+    else if (a == "--write-vtu") o.vtu = next();
     else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
   }
   fr_refshim_blas_threads(1);
@@ -357,6 +363,11 @@ int main(int argc, char **argv) {
       for (auto &e : S.eles) edt.push_back(e->dt);
       dumpd("ele_dt", edt, {S.nEles});
     }
+  }
+
+  if (!o.vtu.empty()) {
+    params.dataFileName = o.vtu;
+    writeData(&S, &params);  /* plotType 1: ParaView, 0: CSV */
   }
 
   if (o.timeK > 0) {

@@ -114,6 +114,61 @@ REF_MESHES = {
 }
 
 
+# cases whose fixture also keeps the reference's own solution files written
+# after the N steps (gzip-compressed text): the ParaView file, and for the
+# first one also the CSV (deck plotType 0)
+OUTPUT_CASES = ["vortex2d_p3_8", "tgv3d_p2_4", "curved2d_q2_p3"]
+CSV_CASES = ["vortex2d_p3_8", "tgv3d_p2_4"]
+
+
+def gz_bytes(path: str) -> np.ndarray:
+    with open(path, "rb") as f:
+        return np.frombuffer(gzip.compress(f.read(), 9, mtime=0), dtype=np.uint8)
+
+
+def solution_files(name: str, deck_path: str, args: list[str], steps: int, wd: str) -> dict:
+    """The reference's writeData output of the case after its steps."""
+    out = {}
+    with tempfile.TemporaryDirectory() as od:
+        cmd = [HARNESS, deck_path, "-"] + args + ["--steps", str(steps), "--write-vtu", os.path.join(od, "ref")]
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        out["ref_vtu_gz"] = gz_bytes(os.path.join(od, f"ref_{steps:09d}.vtu"))
+        if name in CSV_CASES:
+            csv_deck = os.path.join(wd, "csv.deck")
+            with open(csv_deck, "w") as f:
+                f.write("plotType 0\n" + open(deck_path).read())
+            cmd[1] = csv_deck
+            subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=wd)
+            out["ref_csv_gz"] = gz_bytes(os.path.join(od, f"ref.csv.{steps:09d}"))
+    return out
+
+
+def restart_across_orders() -> None:
+    """restart_p2_to_p3: the reference writes the 8x8 vortex at P2 after 5
+    steps, then a P3 case of the same mesh restarts from that file
+    (interpolating, src/ele.cpp:1554-1596); keeps the P2 file and the P3
+    state the reference read."""
+    base = open(os.path.join(DECKS, "vortex2d_p3_8.deck")).read()
+    with tempfile.TemporaryDirectory() as wd, tempfile.TemporaryDirectory() as td:
+        d2 = os.path.join(wd, "p2.deck")
+        with open(d2, "w") as f:
+            f.write("order 2\n" + base)
+        subprocess.run([HARNESS, d2, "-", "--ic", "vortex", "--vortex", "5,0,0,0.5", "--cfl-dt", "0.5",
+                        "--steps", "5", "--write-vtu", os.path.join(wd, "p2")],
+                       check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        d3 = os.path.join(wd, "p3.deck")
+        with open(d3, "w") as f:
+            f.write(f"restart 1\nrestartIter 5\ndataFileName {os.path.join(wd, 'p2')}\n" + base)
+        subprocess.run([HARNESS, d3, td], check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        arrays, meta = read_dump(td)
+        out = {"ref_vtu_gz": gz_bytes(os.path.join(wd, "p2_000000005.vtu")), "ref_U_restart": arrays["U_init"]}
+    meta.update({"case": "restart_p2_to_p3", "deck": "vortex2d_p3_8", "harness_args": [], "steps": 0,
+                 "restart_iter": 5})
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "restart_p2_to_p3.npz"), **out)
+    print(f"restart_p2_to_p3: {len(out) - 1} arrays")
+
+
 def write_meshes() -> None:
     sys.path.insert(0, ROOT)
     from flurrypp_b200.meshgen import curved_box, write_gmsh_ho
@@ -193,6 +248,9 @@ def run_case(name: str) -> None:
     else:
         names = SETUP + RESID + FINAL if keep == "all" else keep
         out = {k: arrays[k] for k in names if k in arrays}
+    if name in OUTPUT_CASES:
+        with tempfile.TemporaryDirectory() as wd:
+            out.update(solution_files(name, stage_deck(deck, wd), args, steps, wd))
     meta.update({"case": name, "deck": deck, "harness_args": args, "steps": steps})
     out["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
@@ -203,8 +261,11 @@ def main(argv: list[str]) -> None:
     if not os.path.exists(HARNESS):
         sys.exit(f"{HARNESS} missing: run `make -C oracle` first")
     write_meshes()
-    for name in argv or list(CASES):
-        run_case(name)
+    for name in argv or list(CASES) + ["restart_p2_to_p3"]:
+        if name == "restart_p2_to_p3":
+            restart_across_orders()
+        else:
+            run_case(name)
 
 
 if __name__ == "__main__":
