@@ -10,7 +10,9 @@ L2 (the state alone is 84 MB, one stage touches ~1.2 GB), so no flush is needed.
 
 One JSON line (rank 0).  value = DOF * RK stages / s over all ranks with the
 state resident in HBM; e2e = the same metric through the C ABI with the state
-in pinned host memory, copied in and out every step.  N > 1 runs independent
+in pinned host memory, copied in and out every step (three independent cases
+in flight on their own streams, so copies and steps of different cases
+overlap).  N > 1 runs independent
 replicas (one case per GPU, no collective on the data path).
 
 At N = 1 the line also carries "forms", the other workloads of the path,
@@ -51,6 +53,7 @@ DECK_GPU = os.path.join(ROOT, "flurrypp_b200", "decks", "tgv3d_p3_32.deck")
 DECK_CPU = os.path.join(ROOT, "flurrypp_b200", "decks", "tgv3d_p3_16.deck")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "fr_ref_harness_omp")
 METRIC = "DOF·RK-stage/s"
+E2E_CASES = 3  # cases in flight in the end-to-end measurement
 WORKLOAD = "3D Euler Taylor-Green vortex, 32^3 hexes, P=3, RK4, Rusanov, FP64 plain form"
 
 
@@ -518,7 +521,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=12)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="precision_tgv32,precision_ns_tgv40,batch256,serve",
@@ -604,23 +607,48 @@ def main():
         torch.cuda.synchronize()
         kt[k] = a.elapsed_time(b) / reps
 
-    # end to end through the C ABI with host buffers (pinned), every step:
-    # state H2D, one update, state D2H
-    U_host = torch.empty(s.shape, dtype=torch.float64, pin_memory=True).numpy()
-    s.get_state(out=U_host)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.set_state(U_host)
-    s.update()
-    s.get_state(out=U_host)
+    # end to end through the C ABI with host buffers (pinned): every step
+    # copies its case's state in from pinned host memory, advances it one RK
+    # step and copies the result back out, and the next step of that case
+    # starts from the copy that came back.  E2E_CASES independent cases, each
+    # on its own stream, are in flight together, so one case's copy in, another
+    # case's step and a third case's copy out overlap (the two PCIe directions
+    # and the SMs are separate engines).
+    flight = [(s, stream)]
+    for _ in range(E2E_CASES - 1):
+        sx, stx = fb.Solver(DECK_GPU, device=local), torch.cuda.Stream()
+        sx.set_stream(stx.cuda_stream)
+        sx.initialize_solution(fb.IC_TGV, (0.1,))
+        sx.set_dt(dt)
+        sx.run(2)  # first (eager) step and the graph capture
+        flight.append((sx, stx))
+    bufs = [torch.empty(s.shape, dtype=torch.float64, pin_memory=True).numpy() for _ in flight]
+    for (sx, _), b in zip(flight, bufs):
+        sx.get_state(out=b)
+
+    def e2e_round(nsteps):
+        for i in range(nsteps):
+            k = i % len(flight)
+            sx = flight[k][0]
+            sx.set_state(bufs[k])         # pinned host -> device
+            sx.run(1)                     # one RK step (graph replay)
+            sx.get_state_async(bufs[k])   # device -> pinned host
+
+    e2e_round(len(flight))
     torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
-        s.set_state(U_host)   # pinned host -> device
-        s.update()
-        s.get_state(out=U_host)  # device -> pinned host
+    for _, stx in flight[1:]:
+        stx.wait_event(e0)
+    e2e_round(args.e2e_steps)
+    for _, stx in flight[1:]:
+        ev = torch.cuda.Event()
+        ev.record(stx)
+        stream.wait_event(ev)
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
+    del flight[1:]
 
     ms, ms_e2e = max_over_ranks([ms, ms_e2e], "cuda")
 
@@ -647,7 +675,8 @@ def main():
             "config": {"workload": WORKLOAD, "nEles": E, "order": s.order, "dof": dof, "rk_stages": nrk,
                        "dt": dt, "l2_flush": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8},
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8,
+                    "cases_in_flight": E2E_CASES, "steps": args.e2e_steps},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": profiled_traffic("traffic_bytes_per_launch"),

@@ -123,6 +123,7 @@ def _load() -> ctypes.CDLL:
         "fr_init_solution": (i, [P, i, dp, i]),
         "fr_set_state": (i, [P, dp, sz]),
         "fr_get_state": (i, [P, dp, sz]),
+        "fr_get_state_async": (i, [P, dp, sz]),
         "fr_calc_residual": (i, [P, i]),
         "fr_get_residual": (i, [P, i, dp, sz]),
         "fr_update": (i, [P, i]),
@@ -233,6 +234,14 @@ class Solver:
         elif out.dtype != np.float64 or out.size != self.nSpts * self.nEles * self.nFields or not out.flags.c_contiguous:
             raise ValueError("out must be a C-contiguous float64 array of the state's size")
         self._check(lib.fr_get_state(self._c, _dptr(out), out.size))
+        return out
+
+    def get_state_async(self, out: np.ndarray) -> np.ndarray:
+        """Queue the copy of U_spts into `out` (pinned, C-contiguous float64)
+        on the case's stream; valid once that stream has reached it."""
+        if out.dtype != np.float64 or out.size != self.nSpts * self.nEles * self.nFields or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of the state's size")
+        self._check(lib.fr_get_state_async(self._c, _dptr(out), out.size))
         return out
 
     def calc_residual(self, step: int = 0):

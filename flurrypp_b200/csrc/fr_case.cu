@@ -1556,6 +1556,27 @@ int fr_get_state(fr_case *c, double *U, size_t count) {
   return copy_dev(c, c->U, n, U, &count);
 }
 
+int fr_get_state_async(fr_case *c, double *U, size_t count) {
+  PdlScope pdlScope(c);
+  if (!c || !U) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = c->hostOnly ? "host-only case: no device state" : "no state set";
+    return FR_ERR_STATE;
+  }
+  const size_t n = (size_t)c->nS * c->E * c->nF;
+  if (count != n) {
+    c->err = "state size mismatch";
+    return FR_ERR_ARG;
+  }
+  if (c->mixed) c->join_state();
+  if (cudaMemcpyAsync(U, c->U, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "cudaMemcpy D2H failed";
+    return FR_ERR_CUDA;
+  }
+  return FR_OK;
+}
+
 int fr_calc_residual(fr_case *c, int step) {
   PdlScope pdlScope(c);
   if (!c) return FR_ERR_ARG;

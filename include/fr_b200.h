@@ -126,6 +126,11 @@ int fr_init_solution(fr_case *c, int kind, const double *prm, int nprm);
  * include/solver.hpp:94). */
 int fr_set_state(fr_case *c, const double *U, size_t count);
 int fr_get_state(fr_case *c, double *U, size_t count);
+/* fr_get_state without the wait: the copy is queued on the case's stream
+ * behind the work already queued there, and U holds the state once that
+ * stream (fr_synchronize, or an event the caller records) has reached it.
+ * Overlaps with other work only when U is page-locked host memory. */
+int fr_get_state_async(fr_case *c, double *U, size_t count);
 
 /* One residual evaluation into divF_spts[step] (solver::calcResidual,
  * include/solver.hpp:175, src/solver.cpp:366-445). */

@@ -238,3 +238,19 @@ def test_programmatic_launch_overlap_changes_nothing(case, precision):
             outs.append(s.get_state())
     for o in outs[1:]:
         assert np.array_equal(o, outs[0])
+
+
+@pytest.mark.parametrize("precision", [fb.FR_PREC_FP64, fb.FR_PREC_MIXED])
+def test_async_state_copy(precision):
+    """fr_get_state_async into pinned memory, read after the stream is
+    reached, equals fr_get_state."""
+    import torch
+
+    a, meta = load_golden("tgv3d_p3_4")
+    s = gpu_case(meta, precision=precision)
+    s.set_state(a["U_init"])
+    s.run(3)
+    pinned = torch.empty(s.shape, dtype=torch.float64, pin_memory=True).numpy()
+    s.get_state_async(pinned)
+    s.synchronize()
+    assert np.array_equal(pinned, s.get_state())
