@@ -92,6 +92,16 @@ CASES = {
     "curved3d_s20_p2": ("curved3d_s20_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 4, "all"),
     "curved3d_q3_p3": ("curved3d_q3_p3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 3, "all"),
     "cyl2d_p2": ("cyl2d_p2", [], 10, "all"),
+    "lobatto_hu3d_p3": ("lobatto_hu3d_p3", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "13,0.05"], 5, "all"),
+    "cplus_rk2_3d_p2": ("cplus_rk2_3d_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "17,0.05"], 6, "all"),
+    "sd_euler3d_p4": ("sd_euler3d_p4", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "19,0.05"], 6, "all"),
+    "p5_3d": ("p5_3d", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "23,0.04"], 3, "all"),
+    "p0_3d": ("p0_3d", ["--ic", "tgv", "--tgv-mach", "0.2"], 6, "all"),
+    # vortex centre off the face-point columns: on a column through the centre
+    # the normal velocity at the far-field faces is zero up to round-off, and
+    # the characteristic condition's inflow/outflow branch follows its sign
+    "supsub3d_p2": ("supsub3d_p2", ["--ic", "vortex", "--vortex", "2,0.13,-0.21,0.5", "--cfl-dt", "0.4"], 6, "all"),
+    "ns_walls3d_p2": ("ns_walls3d_p2", ["--ic", "uniform"], 6, "all"),
     "naca_p4": ("naca_p4", [], 0, "summary"),
     "cyl3d_p2": ("cyl3d_p2", [], 0, "summary"),
 }
