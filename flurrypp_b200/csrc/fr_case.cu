@@ -108,12 +108,23 @@ struct fr_case {
     std::vector<float> tuneMs;  // element-stage time per tile variant (autotuner)
   } f32;
 
+  // moving mesh (deck "motion" 1..5): the vertex law, the metrics rebuilt at
+  // every RK stage and the chain-rule residual (kernels/motion.cu)
+  struct MotionState {
+    bool on = false;
+    frk::MotionArgs a;
+    double *F = nullptr, *disFn = nullptr;  // physical flux at spts; Fn - extrapolated normal flux
+    unsigned int *err = nullptr;
+  } mo;
+
   // solution output: primitive variables at the plot points, copied to a
   // pinned host buffer on a side stream so that stepping goes on meanwhile
   struct Checkpoint {
     double *opp = nullptr;   // [nPpts][nSpts] spts -> plot points
     double *Vp = nullptr;    // [nPpts][E][nF], then the time
     double *host = nullptr;  // pinned copy of Vp
+    double *xv = nullptr, *xvHost = nullptr;  // moving mesh: vertex positions, then velocities, at the snapshot
+    std::vector<double> gridVel;              // moving mesh: grid velocity at the plot points
     cudaStream_t copy = nullptr;
     cudaEvent_t ready = nullptr, done = nullptr;
     bool pending = false;
@@ -125,6 +136,7 @@ struct fr_case {
   ~fr_case() {
     if (cp.copy) cudaStreamSynchronize(cp.copy);
     if (cp.host) cudaFreeHost(cp.host);
+    if (cp.xvHost) cudaFreeHost(cp.xvHost);
     if (cp.ready) cudaEventDestroy(cp.ready);
     if (cp.done) cudaEventDestroy(cp.done);
     if (cp.copy) cudaStreamDestroy(cp.copy);
@@ -136,8 +148,10 @@ struct fr_case {
   }
   cudaStream_t ownedStream = nullptr;
 
-  bool fail(int, const std::string &m) {
+  int errCode = 0;  // the FR_ERR_* of the last fail()
+  bool fail(int code, const std::string &m) {
     err = m;
+    errCode = code;
     return false;
   }
   template <typename T>
@@ -147,6 +161,7 @@ struct fr_case {
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) {
       err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      errCode = FR_ERR_CUDA;
       return false;
     }
     cudaMemsetAsync(q, 0, bytes, stream);
@@ -161,6 +176,7 @@ struct fr_case {
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) {
       err = std::string("cudaMemcpy: ") + cudaGetErrorString(e);
+      errCode = FR_ERR_CUDA;
       return false;
     }
     return true;
@@ -355,6 +371,7 @@ struct fr_case {
       }
     }
     if (!alloc(devErr, 1)) return false;
+    if (in.motion && !setup_motion()) return false;
     usePdl = !opts.no_pdl && (long long)nS * E <= 148LL * 1024;
     if (!mixed) {
       useTma = useTp && !opts.no_tma && build_tma(0);
@@ -500,6 +517,148 @@ struct fr_case {
     E = mesh.nEles;
     nPF = nDims == 2 ? in.order + 1 : (in.order + 1) * (in.order + 1);
     return true;
+  }
+
+  bool setup_motion() {
+    if (mixed) return fail(FR_ERR_UNSUPPORTED, "moving meshes run in the plain form, not the precision form");
+    auto &a = mo.a;
+    const int nd = nDims;
+    a.type = in.motion;
+    a.nDims = nd;
+    a.nVerts = mesh.nVerts;
+    a.E = E;
+    a.nS = nS;
+    a.nFp = nFp;
+    a.nNodes = mesh.nNodes;
+    a.time = timeAcc;
+    a.dt = dt;
+    // motion 1 scales by the periodic lengths (src/geo.cpp:2737-2738)
+    a.DX = mesh.period[0];
+    a.DY = mesh.period[1];
+    a.Ax = in.moveAx;
+    a.Ay = in.moveAy;
+    a.Fx = in.moveFx;
+    a.Fy = in.moveFy;
+    a.Ar = in.moveAr;
+    a.Fr = in.moveFr;
+    std::vector<double> xv0(mesh.xv.begin(), mesh.xv.begin() + (size_t)mesh.nVerts * nd);
+    double *dxv0, *dxv, *dgv;
+    if (!upload(dxv0, xv0) || !alloc(dxv, xv0.size()) || !alloc(dgv, xv0.size())) return false;
+    a.xv0 = dxv0;
+    a.xv = dxv;
+    a.gv = dgv;
+    if (in.motion == 5) {  // spherical coordinates of the initial vertices (src/geo.cpp:208-216)
+      std::vector<double> rv((size_t)mesh.nVerts * 3);
+      for (int i = 0; i < mesh.nVerts; i++) {
+        const double x = xv0[(size_t)i * 3], y = xv0[(size_t)i * 3 + 1], z = xv0[(size_t)i * 3 + 2];
+        rv[(size_t)i * 3] = std::sqrt(x * x + y * y + z * z);
+        rv[(size_t)i * 3 + 1] = std::atan2(y, x);
+        rv[(size_t)i * 3 + 2] = std::acos(z / rv[(size_t)i * 3]);
+      }
+      double *drv;
+      if (!upload(drv, rv)) return false;
+      a.rv0 = drv;
+    }
+    int *dc2v;
+    if (!upload(dc2v, mesh.c2v)) return false;
+    a.c2v = dc2v;
+    auto loc = fr::loc_spts(nd, in.order, in.sptsTypeQuad);
+    auto lf = fr::loc_fpts(nd, in.order, in.sptsTypeQuad);
+    loc.insert(loc.end(), lf.begin(), lf.end());
+    std::vector<double> N, dN;
+    std::string e;
+    if (!fr::shape_tables(nd, mesh.nNodes, loc, N, dN, e)) return fail(FR_ERR_SETUP, e);
+    double *dNs, *ddN, *dtn, *dJ, *dgs, *dgf;
+    if (!upload(dNs, N) || !upload(ddN, dN) || !upload(dtn, op.tNorm) || !alloc(dJ, (size_t)nd * nS * E * nd) ||
+        !alloc(dgs, (size_t)nS * E * nd) || !alloc(dgf, (size_t)nFp * E * nd))
+      return false;
+    a.shape = dNs;
+    a.dshape = ddN;
+    a.tNorm = dtn;
+    a.Jac = dJ;
+    a.gVs = dgs;
+    a.gVf = dgf;
+    a.JGinv = JGinv;
+    a.detJ = detJ;
+    a.norm = norm;
+    a.dA = dA;
+    std::vector<double> G;
+    for (int d = 0; d < nd; d++) G.insert(G.end(), op.grad[d].begin(), op.grad[d].end());
+    double *dG, *dX, *dC;
+    if (!upload(dG, G) || !upload(dX, op.ext) || !upload(dC, op.corr)) return false;
+    a.opGrad = dG;
+    a.opExt = dX;
+    a.opCorr = dC;
+    if (!alloc(mo.err, 1) || !alloc(mo.F, (size_t)nd * nS * E * nF) || !alloc(mo.disFn, (size_t)nFp * E * nF))
+      return false;
+    a.err = mo.err;
+    mo.on = true;
+    // solver::initializeSolution places the mesh at the current time before
+    // the initial condition (src/solver.cpp:1902-1904); the metrics are those
+    // of the mesh as set up, which a rigid translation (motion 4) keeps
+    frk::launch_move_vertices(mo.a, 0.0, stream);
+    frk::launch_motion_geometry(mo.a, true, stream);
+    frk::launch_face_refresh(ft, nDims, norm, dA, stream);
+    return cuda_ok("motion setup");
+  }
+
+  // solver::moveMesh (src/solver.cpp:1168-1246, non-overset branch): the
+  // vertices at time + dt * rkVal, then grid velocities and (except for a
+  // rigid translation, motion 4) the metrics and the face table's copies.
+  void move_mesh(double rkVal) {
+    frk::launch_move_vertices(mo.a, rkVal, stream);
+    frk::launch_motion_geometry(mo.a, in.motion != 4, stream);
+    launches += 2;
+    if (in.motion != 4) {
+      frk::launch_face_refresh(ft, nDims, norm, dA, stream);
+      launches++;
+    }
+  }
+
+  // calcResidual on the moving mesh (src/solver.cpp:366-445 with motion):
+  // extrapolation, common flux with grid velocity, chain-rule divergence,
+  // correction; divF into divF[step].
+  void residual_motion(int step) {
+    extrapolate();
+    frk::launch_faces_motion(nDims, ft, Ufpts, Fn, waveSp, mo.a.gVf, ph, stream);
+    frk::launch_motion_residual(mo.a, U, Fn, in.gamma, mo.F, mo.disFn, divF[step], stream);
+    launches += 5;
+    fptsFresh = false;
+  }
+
+  // solver::update with motion (src/solver.cpp:319-363): the metrics move
+  // with every stage, and a standard RK step combines its stored stage
+  // residuals at the end with the last stage's metrics.
+  bool update_motion() {
+    const double *eDt = in.dtType == 2 ? eleDt : nullptr;
+    const long long nSE = (long long)nS * E;
+    const bool jameson = in.timeType >= 5;
+    for (int step = 0; step < nRK - 1; step++) {
+      if (step == 0 && in.dtType != 0) calc_dt_dev();
+      move_mesh(in.RKa[step]);
+      if (step == 0) cudaMemcpyAsync(U0, U, (size_t)nSE * nF * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+      residual_motion(step);
+      frk::launch_motion_step_a(nSE, nF, E, U0, divF[step], detJ, dt, eDt, in.RKa[step + 1], U, stream);
+      launches++;
+    }
+    move_mesh(in.RKa[nRK - 1]);
+    residual_motion(nRK - 1);
+    if (!jameson) {
+      if (nRK == 1 && in.dtType != 0) calc_dt_dev();
+      frk::MotionStages stg;
+      stg.n = nRK;
+      for (int s2 = 0; s2 < nRK; s2++) {
+        stg.divF[s2] = divF[s2];
+        stg.rkb[s2] = in.RKb[s2];
+      }
+      frk::launch_motion_step_b(nSE, nF, E, nRK > 1 ? U0 : U, stg, detJ, dt, eDt, U, stream);
+    } else {
+      frk::launch_motion_step_a(nSE, nF, E, U0, divF[nRK - 1], detJ, dt, eDt, in.RKa[nRK], U, stream);
+    }
+    frk::launch_add_time(dt, timeAcc, stream);
+    launches += 2;
+    fptsFresh = false;
+    return cuda_ok("update (moving mesh)");
   }
 
   // Tensor-product tables of the dense operators, used only if every dense
@@ -1047,7 +1206,9 @@ struct fr_case {
   // Everything of a stage before the element kernel: the common flux Fn (and,
   // viscous, the LDG jumps and the corrected gradients it needs).
   void wavesp_init() {
-    if (mixed)
+    if (mo.on)
+      frk::launch_wavesp_motion(nDims, nFp, E, Ufpts, norm, mo.a.gVf, in.gamma, waveSp, stream);
+    else if (mixed)
       frk::launch_wavesp_init<float>(nDims, nFp, E, f32.Ufpts, norm, in.gamma, waveSp, stream);
     else
       frk::launch_wavesp_init<double>(nDims, nFp, E, Ufpts, norm, in.gamma, waveSp, stream);
@@ -1170,6 +1331,14 @@ struct fr_case {
 
   bool calc_residual(int step) {
     if (step < 0 || step >= nRK) return fail(FR_ERR_ARG, "step out of range");
+    if (mo.on) {
+      residual_motion(step);
+      if (Fdbg)
+        cudaMemcpyAsync(Fdbg, mo.F, (size_t)nDims * nS * E * nF * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+      if (disFnDbg)
+        cudaMemcpyAsync(disFnDbg, mo.disFn, (size_t)nFp * E * nF * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+      return cuda_ok("calc_residual");
+    }
     // the last element stage extrapolated the state it wrote; otherwise
     // (a new or restricted/prolonged state) extrapolate here
     if (!fptsFresh) extrapolate();
@@ -1194,6 +1363,7 @@ struct fr_case {
 
   // solver::update (solver.cpp:319-363)
   bool update_once(bool pmgSource) {
+    if (mo.on) return update_motion();
     if (!fptsFresh) extrapolate();
     const bool jameson = in.timeType >= 5;
     for (int step = 0; step < nRK - 1; step++) {
@@ -1276,6 +1446,12 @@ struct fr_case {
         timedOut = true;
         return fail(FR_ERR_TIMEOUT, "a bounded device wait ran out (TMA tile load)");
       }
+    }
+    if (mo.err) {
+      unsigned int w = 0;
+      if (cudaMemcpy(&w, mo.err, sizeof(w), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(FR_ERR_CUDA, "status read failed");
+      if (w) return fail(FR_ERR_SETUP, "Negative Jacobian at solution points.");  // src/solver.cpp:1638
     }
     return true;
   }
@@ -1387,9 +1563,9 @@ int create_common(const char *deck, const fr_mesh *mesh, const fr_setup_opts *op
   bool ok = c->setup(o);
   int st = FR_OK;
   if (!ok) {
-    st = c->err.find("mixed") != std::string::npos || c->err.find("viscous") != std::string::npos ||
-                 c->err.find("tensor-product") != std::string::npos
-             ? FR_ERR_UNSUPPORTED
+    st = c->errCode == FR_ERR_UNSUPPORTED || c->errCode == FR_ERR_CUDA || c->errCode == FR_ERR_SETUP ||
+                 c->errCode == FR_ERR_ARG
+             ? c->errCode
              : (c->err.find("cuda") != std::string::npos ? FR_ERR_CUDA : FR_ERR_SETUP);
   }
   *out = c.release();
@@ -1906,9 +2082,9 @@ int fr_batch_create(fr_case *const *cases, int n, fr_batch **out) {
   for (int i = 0; i < n; i++) {
     fr_case *c = cases[i];
     if (!c || c->hostOnly || !c->stateSet) return FR_ERR_STATE;
-    if (c->in.viscous || c->in.PMG || c->in.dtType != 0 || c->in.nDims != cases[0]->in.nDims ||
+    if (c->in.viscous || c->in.PMG || c->in.motion || c->in.dtType != 0 || c->in.nDims != cases[0]->in.nDims ||
         c->in.timeType != cases[0]->in.timeType || c->opts.precision != cases[0]->opts.precision) {
-      return FR_ERR_UNSUPPORTED;  // batches hold inviscid, fixed-dt cases of one RK scheme and precision
+      return FR_ERR_UNSUPPORTED;  // batches hold inviscid, static-mesh, fixed-dt cases of one RK scheme and precision
     }
     b->members.push_back(c);
   }
@@ -2043,6 +2219,12 @@ int fr_checkpoint(fr_case *c) {
     k.nP = c->nDims == 2 ? n3 * n3 : n3 * n3 * n3;
     if (!c->upload(k.opp, fr::spts_to_ppts(c->nDims, c->in.order, c->in.sptsTypeQuad)) || !c->alloc(k.Vp, nV))
       return FR_ERR_CUDA;
+    const size_t nX = c->mo.on ? 2 * (size_t)c->mesh.nVerts * c->nDims : 0;
+    if (nX && (!c->alloc(k.xv, nX) || cudaMallocHost(&k.xvHost, nX * sizeof(double)) != cudaSuccess)) {
+      cudaGetLastError();
+      c->err = "cannot allocate the checkpoint buffers";
+      return FR_ERR_CUDA;
+    }
     if (cudaMallocHost(&k.host, nV * sizeof(double)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&k.copy, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&k.ready, cudaEventDisableTiming) != cudaSuccess ||
@@ -2058,9 +2240,15 @@ int fr_checkpoint(fr_case *c) {
   frk::launch_plot_primitives(c->nDims, c->U, k.opp, k.Vp, c->nS, k.nP, c->E, c->in.gamma, c->stream);
   c->launches++;
   cudaMemcpyAsync(k.Vp + nV - 1, c->timeAcc, sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  const size_t nX = c->mo.on ? (size_t)c->mesh.nVerts * c->nDims : 0;
+  if (nX) {
+    cudaMemcpyAsync(k.xv, c->mo.a.xv, nX * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(k.xv + nX, c->mo.a.gv, nX * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  }
   cudaEventRecord(k.ready, c->stream);
   cudaStreamWaitEvent(k.copy, k.ready, 0);
   cudaMemcpyAsync(k.host, k.Vp, nV * sizeof(double), cudaMemcpyDeviceToHost, k.copy);
+  if (nX) cudaMemcpyAsync(k.xvHost, k.xv, 2 * nX * sizeof(double), cudaMemcpyDeviceToHost, k.copy);
   cudaEventRecord(k.done, k.copy);
   k.pending = true;
   k.iter = c->iter;
@@ -2105,15 +2293,29 @@ int fr_write_data(fr_case *c, const char *path) {
     return FR_ERR_CUDA;
   }
   k.pending = false;
-  if (k.pos.empty() &&
-      !fr::positions_at(c->mesh, fr::loc_ppts(c->nDims, c->in.order, c->in.sptsTypeQuad), k.pos, e)) {
+  if (c->mo.on) {  // the vertices (and their velocities) where the snapshot was taken
+    const size_t nX = (size_t)c->mesh.nVerts * c->nDims;
+    const auto loc = fr::loc_ppts(c->nDims, c->in.order, c->in.sptsTypeQuad);
+    fr::Mesh moved = c->mesh;
+    std::copy(k.xvHost, k.xvHost + nX, moved.xv.begin());
+    k.pos.clear();
+    bool ok = fr::positions_at(moved, loc, k.pos, e);
+    std::copy(k.xvHost + nX, k.xvHost + 2 * nX, moved.xv.begin());  // velocities interpolate the same way
+    ok = ok && fr::positions_at(moved, loc, k.gridVel, e);
+    if (!ok) {
+      c->err = e;
+      return FR_ERR_ARG;
+    }
+  } else if (k.pos.empty() &&
+             !fr::positions_at(c->mesh, fr::loc_ppts(c->nDims, c->in.order, c->in.sptsTypeQuad), k.pos, e)) {
     c->err = e;
     return FR_ERR_ARG;
   }
   std::snprintf(name, sizeof name, "_%.09lld.vtu", k.iter);
   const std::string out = path ? std::string(path) : c->in.dataFileName + name;
   const double time = k.host[(size_t)k.nP * c->E * c->nF];
-  if (!fr::write_paraview(out, c->nDims, c->in.order, c->E, time, k.iter, k.host, k.pos.data(), e)) {
+  if (!fr::write_paraview(out, c->nDims, c->in.order, c->E, time, k.iter, k.host, k.pos.data(),
+                          c->mo.on ? k.gridVel.data() : nullptr, e)) {
     c->err = e;
     return FR_ERR_ARG;
   }
@@ -2148,6 +2350,11 @@ int fr_read_restart(fr_case *c, const char *path) {
   }
   if (!path) c->iter = c->in.restartIter;
   else if (hasIter) c->iter = iter;
+  if (c->mo.on) {  // the mesh at the restart time (src/solver.cpp:1855-1857)
+    PdlScope pdlScope(c);
+    c->move_mesh(0.0);
+    if (!c->cuda_ok("restart")) return FR_ERR_CUDA;
+  }
   return FR_OK;
 }
 

@@ -59,6 +59,7 @@ struct Input {
   double dt = 0.0;
   int viscous = 0;
   int motion = 0;
+  double moveAx = 0, moveAy = 0, moveFx = 0, moveFy = 0, moveAr = 0, moveFr = 0;
   int order = 3;
   int riemannType = 0;
   int testCase = 0;
@@ -204,6 +205,10 @@ struct Geometry {
 bool build_geometry(const Mesh &m, int order, int ptsType, Geometry &g, std::string &err);
 // True when nNodes names a quad (nDims 2) or hex (nDims 3) shape above.
 bool shape_supported(int nDims, int nNodes);
+// Shape functions N [nPts][nNodes] and their reference-space derivatives
+// dN [nPts][nNodes][nDims] at the points `loc`.
+bool shape_tables(int nDims, int nNodes, const std::vector<Pt> &loc, std::vector<double> &N,
+                  std::vector<double> &dN, std::string &err);
 // Physical positions of reference-space points `loc` in every element,
 // [point][element][nDims] (reference: src/solver.cpp:1248-1313, shape_ppts).
 bool positions_at(const Mesh &m, const std::vector<Pt> &loc, std::vector<double> &pos, std::string &err);
@@ -215,9 +220,10 @@ bool positions_at(const Mesh &m, const std::vector<Pt> &loc, std::vector<double>
 std::vector<Pt> loc_ppts(int nDims, int order, int ptsType);
 std::vector<double> spts_to_ppts(int nDims, int order, int ptsType);
 // The reference's ParaView file from primitive variables at the plot points
-// Vp [nPpts][E][nDims+2] and their positions [nPpts][E][nDims].
+// Vp [nPpts][E][nDims+2], their positions [nPpts][E][nDims] and, on a moving
+// mesh, the grid velocity there (same layout; null on a static mesh).
 bool write_paraview(const std::string &path, int nDims, int order, int E, double time, long long iter,
-                    const double *Vp, const double *pos, std::string &err);
+                    const double *Vp, const double *pos, const double *gridVel, std::string &err);
 // The reference's CSV file: primitives at the solution then flux points.
 bool write_csv(const std::string &path, int nDims, int nS, int nFp, int E, const double *U, const double *Ufpts,
                const double *posS, const double *posF, double gamma, std::string &err);

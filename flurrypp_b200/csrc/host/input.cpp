@@ -108,6 +108,15 @@ bool read_deck(const std::string &path, Input &in, std::string &err) {
   }
   d.get("viscous", in.viscous);
   d.get("motion", in.motion);
+  if (in.motion == 4) {  // reference: src/input.cpp:324-332
+    d.get("moveAx", in.moveAx);
+    d.get("moveAy", in.moveAy);
+    d.get("moveFx", in.moveFx);
+    d.get("moveFy", in.moveFy);
+  } else if (in.motion == 5) {
+    d.get("moveAr", in.moveAr);
+    d.get("moveFr", in.moveFr);
+  }
   d.get("order", in.order);
   d.get("riemannType", in.riemannType);
   d.get("testCase", in.testCase);
@@ -213,8 +222,20 @@ bool finalize_input(Input &in, std::string &err) {
     err = "order must be in 0..5";
     return false;
   }
-  if (in.motion != 0) {
-    err = "moving meshes (motion != 0) are not on the B200 path";
+  if (in.motion < 0 || in.motion > 5) {
+    err = "motion must be 0 (static) or one of the reference's laws 1..5";
+    return false;
+  }
+  if (in.motion != 0 && (in.viscous || in.riemannType != 0 || in.PMG)) {
+    err = "moving meshes run the inviscid Rusanov path without P-multigrid";
+    return false;
+  }
+  if (in.motion == 5 && in.nDims != 3) {
+    err = "motion 5 (radial expansion) is 3-D only";  // reference: src/geo.cpp:208-216
+    return false;
+  }
+  if (in.motion == 3 && in.nDims != 2) {
+    err = "motion 3 is 2-D only";  // reference: src/geo.cpp:2775-2789
     return false;
   }
   if (in.riemannType == 1 && in.nDims == 3) {

@@ -554,6 +554,19 @@ bool shape_supported(int nDims, int nNodes) {
   return (nDims == 2 || nDims == 3) && nNodes >= 4 && nNodes <= 216 && sf.init(nDims, nNodes, err);
 }
 
+bool shape_tables(int nDims, int nNodes, const std::vector<Pt> &loc, std::vector<double> &N,
+                  std::vector<double> &dN, std::string &err) {
+  ShapeFn sf;
+  if (!sf.init(nDims, nNodes, err)) return false;
+  N.assign(loc.size() * nNodes, 0.0);
+  dN.assign(loc.size() * nNodes * nDims, 0.0);
+  for (size_t q = 0; q < loc.size(); q++) {
+    sf.eval(loc[q], &N[q * nNodes]);
+    sf.deval(loc[q], &dN[q * nNodes * nDims]);
+  }
+  return true;
+}
+
 bool positions_at(const Mesh &m, const std::vector<Pt> &loc, std::vector<double> &pos, std::string &err) {
   ShapeFn sf;
   if (!sf.init(m.nDims, m.nNodes, err)) return false;

@@ -88,7 +88,7 @@ struct TextOut {
 }  // namespace
 
 bool write_paraview(const std::string &path, int nDims, int order, int E, double time, long long iter,
-                    const double *Vp, const double *pos, std::string &err) {
+                    const double *Vp, const double *pos, const double *gridVel, std::string &err) {
   std::FILE *f = std::fopen(path.c_str(), "wb");
   if (!f) {
     err = "cannot open " + path + " for writing";
@@ -123,6 +123,14 @@ bool write_paraview(const std::string &path, int nDims, int order, int E, double
     o.str("\t\t\t\t<DataArray type=\"Float32\" Name=\"Pressure\" format=\"ascii\">\n");
     for (int q = 0; q < nP; q++) o.num(V(q, nDims + 1));
     o.str("\n\t\t\t\t</DataArray>\n");
+    if (gridVel) {  // moving mesh (src/output.cpp:383-399)
+      o.str("\t\t\t\t<DataArray type=\"Float32\" NumberOfComponents=\"3\" Name=\"GridVelocity\" format=\"ascii\">\n");
+      for (int q = 0; q < nP; q++) {
+        for (int d = 0; d < nDims; d++) o.num(gridVel[((size_t)q * E + e) * nDims + d]);
+        if (nDims == 2) o.num(0.0);
+      }
+      o.str("\n\t\t\t\t</DataArray>\n");
+    }
     o.str("\t\t\t</PointData>\n");
     o.str("\t\t\t<Points>\n");
     o.str("\t\t\t\t<DataArray type=\"Float32\" NumberOfComponents=\"3\" format=\"ascii\">\n");

@@ -93,7 +93,7 @@ struct Prim {
 // Rusanov common flux on the left normal; returns the wave speed stored for
 // the dt estimate (reference: src/face.cpp:314-374).
 template <int ND, typename R>
-__device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R gam, R *Fn) {
+__device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R gam, R *Fn, R vgn = R(0)) {
   constexpr int NF = ND + 2;
   const Prim<ND, R> L(UL, gam), Rt(UR, gam);
   R vnL = R(0), vnR = R(0);
@@ -119,7 +119,9 @@ __device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R gam
   R eig = fmax(eigL, eigR);
 #pragma unroll
   for (int i = 0; i < NF; i++) Fn[i] = R(0.5) * (tL[i] + tR[i] - eig * (UR[i] - UL[i]));
-  return fmax(eigL, eigR);
+  // the wave speed kept for the time step is relative to the grid velocity
+  // on a moving mesh (face.cpp:366-371; vgn is zero on a static one)
+  return fmax(fabs(vnL - vgn) + sqrt(csqL), fabs(vnR - vgn) + sqrt(csqR));
 }
 
 // Roe flux with entropy fix, 2-D (reference: src/face.cpp:376-495).
@@ -179,11 +181,12 @@ __device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R ga
   for (int i = 0; i < 4; i++) Fn[i] *= R(0.5);
 }
 
-// Ghost (right) state of a boundary face (reference: src/boundFace.cpp:65-314,
-// static mesh: grid velocity zero).
+// Ghost (right) state of a boundary face (reference: src/boundFace.cpp:65-314).
+// vG: the grid velocity at the point on a moving mesh (slip walls reflect the
+// velocity relative to it, no-slip walls move with it); null on a static one.
 template <int ND, typename R>
 __device__ __forceinline__ void boundary_state(int bc, const R *UL, const R *n, const Phys &ph,
-                                               R *UR) {
+                                               R *UR, const R *vG = nullptr) {
   const R gamma = R(ph.gamma);
   const R gmo = gamma - R(1.);
   R rhoR = R(0), pR = R(0), ER = R(0);
@@ -225,16 +228,16 @@ __device__ __forceinline__ void boundary_state(int bc, const R *UL, const R *n, 
   } else if (bc == BC_SLIP_WALL || bc == BC_SYMMETRY) {
     rhoR = rhoL;
     R vnL = R(0.);
-    for (int i = 0; i < ND; i++) vnL += (vL[i] - R(0)) * n[i];
+    for (int i = 0; i < ND; i++) vnL += (vL[i] - (vG ? vG[i] : R(0))) * n[i];
     for (int i = 0; i < ND; i++) vR[i] = vL[i] - (R(2.0)) * vnL * n[i];
     ER = eL;
   } else if (bc == BC_ISO_NOSLIP_MOVING) {
     pR = pL;
     R TR = R(ph.TWall);
     rhoR = pR / (R(ph.RGas) * TR);
-    vR[0] = R(ph.uWall);
-    vR[1] = R(ph.vWall);
-    if (ND == 3) vR[2] = R(ph.wWall);
+    vR[0] = (vG ? vG[0] : R(0)) + R(ph.uWall);
+    vR[1] = (vG ? vG[1] : R(0)) + R(ph.vWall);
+    if (ND == 3) vR[2] = (vG ? vG[2] : R(0)) + R(ph.wWall);
     vSq = R(0.);
     for (int i = 0; i < ND; i++) vSq += (vR[i] * vR[i]);
     ER = (pR / (gamma - R(1.0))) + R(0.5) * rhoR * vSq;
@@ -242,14 +245,14 @@ __device__ __forceinline__ void boundary_state(int bc, const R *UL, const R *n, 
     pR = pL;
     R TR = R(ph.TWall);
     rhoR = pR / (R(ph.RGas) * TR);
-    for (int i = 0; i < ND; i++) vR[i] = R(0);
+    for (int i = 0; i < ND; i++) vR[i] = vG ? vG[i] : R(0);
     vSq = R(0.);
     for (int i = 0; i < ND; i++) vSq += (vR[i] * vR[i]);
     ER = (pR / (gamma - R(1.0))) + R(0.5) * rhoR * vSq;
   } else if (bc == BC_ADI_NOSLIP) {
     rhoR = rhoL;
     pR = pL;
-    for (int i = 0; i < ND; i++) vR[i] = R(0);
+    for (int i = 0; i < ND; i++) vR[i] = vG ? vG[i] : R(0);
     vSq = R(0.);
     for (int i = 0; i < ND; i++) vSq += (vR[i] * vR[i]);
     ER = (pR / (gamma - R(1.0))) + R(0.5) * rhoR * vSq;

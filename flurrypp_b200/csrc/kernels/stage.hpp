@@ -242,6 +242,44 @@ void launch_check_state(int nS, int E, int nF, const R *U, unsigned int *bad, cu
 //   join    : (U32, comp) -> U64 = U32 + comp
 //   narrow  : FP64 -> FP32 (metrics, normals, face areas)
 //   widen   : FP32 -> FP64 (residuals, traces read back by tools)
+// ---- moving meshes (motion.cu), FP64 ------------------------------------
+struct MotionArgs {
+  int type = 0, nDims = 2, nVerts = 0, E = 0, nS = 0, nFp = 0, nNodes = 0;
+  const double *time = nullptr, *dt = nullptr;  // device scalars
+  double DX = 0, DY = 0, Ax = 0, Ay = 0, Fx = 0, Fy = 0, Ar = 0, Fr = 0;
+  const double *xv0 = nullptr, *rv0 = nullptr;  // initial vertices [nVerts][nDims], (r, theta, psi)
+  double *xv = nullptr, *gv = nullptr;          // moved vertices and their velocities
+  const int *c2v = nullptr;                     // [E][nNodes]
+  const double *shape = nullptr, *dshape = nullptr;  // [nS + nFp][nNodes] and [..][nNodes][nDims]
+  const double *tNorm = nullptr;                // [nFp][nDims]
+  double *Jac = nullptr;                        // [nDims][nS][E][nDims], d x_comp / d xi_dim
+  double *JGinv = nullptr, *detJ = nullptr, *norm = nullptr, *dA = nullptr;
+  double *gVs = nullptr, *gVf = nullptr;        // grid velocity [nS|nFp][E][nDims]
+  const double *opGrad = nullptr;               // [nDims][nS][nS] dense
+  const double *opExt = nullptr;                // [nFp][nS]
+  const double *opCorr = nullptr;               // [nS][nFp]
+  unsigned int *err = nullptr;                  // bit 2: negative Jacobian
+};
+struct MotionStages {
+  const double *divF[8];
+  double rkb[8];
+  int n = 0;
+};
+void launch_move_vertices(const MotionArgs &m, double rkVal, cudaStream_t st);
+void launch_motion_geometry(const MotionArgs &m, bool transforms, cudaStream_t st);
+void launch_face_refresh(const FaceTableT<double> &ft, int nDims, const double *norm, const double *dA,
+                         cudaStream_t st);
+void launch_faces_motion(int nDims, const FaceTableT<double> &ft, const double *Uf, double *Fn, double *waveSp,
+                         const double *gVf, const Phys &ph, cudaStream_t st);
+void launch_wavesp_motion(int nDims, int nFp, int E, const double *Uf, const double *norm, const double *gVf,
+                          double gamma, double *waveSp, cudaStream_t st);
+void launch_motion_residual(const MotionArgs &m, const double *U, const double *Fn, double gamma, double *F,
+                            double *disFn, double *divF, cudaStream_t st);
+void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const double *divF, const double *detJ,
+                          const double *dt, const double *eleDt, double rk, double *U, cudaStream_t st);
+void launch_motion_step_b(long long nSE, int nF, int E, const double *base, const MotionStages &stages,
+                          const double *detJ, const double *dt, const double *eleDt, double *U, cudaStream_t st);
+
 // Primitive variables at the plot points from the FP64 state (output only).
 void launch_plot_primitives(int nDims, const double *U, const double *opp, double *Vp, int nS, int nP, int E,
                             double gamma, cudaStream_t st);

@@ -51,6 +51,10 @@ def has_pmg(meta):
     return int(float(deck_option(meta, "PMG", 0))) == 1
 
 
+def has_motion(meta):
+    return int(float(deck_option(meta, "motion", 0))) != 0
+
+
 def harness_ic(meta):
     """(kind, params) of the product's fr_init_solution matching the fixture."""
     a = meta["harness_args"]

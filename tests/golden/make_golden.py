@@ -102,6 +102,14 @@ CASES = {
     # the characteristic condition's inflow/outflow branch follows its sign
     "supsub3d_p2": ("supsub3d_p2", ["--ic", "vortex", "--vortex", "2,0.13,-0.21,0.5", "--cfl-dt", "0.4"], 6, "all"),
     "ns_walls3d_p2": ("ns_walls3d_p2", ["--ic", "uniform"], 6, "all"),
+    "motion1_2d_p3": ("motion1_2d_p3", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5", "--cfl-dt", "0.5"], 10, "all"),
+    "motion2_2d_p2_cfl": ("motion2_2d_p2_cfl", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 10, "all"),
+    "motion2_2d_p3_jameson": ("motion2_2d_p3_jameson", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 8, "all"),
+    "motion1_2d_p2_euler": ("motion1_2d_p2_euler", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 8, "all"),
+    "motion4_2d_p2_walls": ("motion4_2d_p2_walls", ["--ic", "vortex", "--vortex", "3,0.13,-0.21,0.4", "--cfl-dt", "0.5"],
+                            10, "all"),
+    "motion2_3d_p2": ("motion2_3d_p2", ["--ic", "vortex", "--vortex", "3,0.13,-0.21,0.5", "--cfl-dt", "0.5"], 4, "all"),
+    "motion5_3d_p1": ("motion5_3d_p1", ["--ic", "vortex", "--vortex", "1,1.5,1.5,0.5"], 6, "all"),
     "naca_p4": ("naca_p4", [], 0, "summary"),
     "cyl3d_p2": ("cyl3d_p2", [], 0, "summary"),
 }
@@ -127,7 +135,7 @@ REF_MESHES = {
 # cases whose fixture also keeps the reference's own solution files written
 # after the N steps (gzip-compressed text): the ParaView file, and for the
 # first one also the CSV (deck plotType 0)
-OUTPUT_CASES = ["vortex2d_p3_8", "tgv3d_p2_4", "curved2d_q2_p3"]
+OUTPUT_CASES = ["vortex2d_p3_8", "tgv3d_p2_4", "curved2d_q2_p3", "motion2_2d_p2_cfl"]
 CSV_CASES = ["vortex2d_p3_8", "tgv3d_p2_4"]
 
 

@@ -23,7 +23,7 @@ from solution_files import read_csv, read_vtu
 
 pytestmark = pytest.mark.gpu
 
-OUTPUT_CASES = ["vortex2d_p3_8", "tgv3d_p2_4", "curved2d_q2_p3"]
+OUTPUT_CASES = ["vortex2d_p3_8", "tgv3d_p2_4", "curved2d_q2_p3", "motion2_2d_p2_cfl"]
 TEXT_TOL = 5e-15   # 16 printed digits, then primitive -> conservative rounding
 FILE_TOL = 1e-13   # plot-point extrapolation: summation order differs from the reference's BLAS
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "fr_ref_harness")

@@ -72,7 +72,8 @@ def test_steps_match_reference(case):
 
 
 @pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "localdt_jameson2d_p3",
-                                  "channel2d_p2", "euler_fwd2d_p1", "pmg_vortex2d_p3_8", "ns_walls2d_p2"])
+                                  "channel2d_p2", "euler_fwd2d_p1", "pmg_vortex2d_p3_8", "ns_walls2d_p2",
+                                  "motion2_2d_p3_jameson", "motion5_3d_p1"])
 def test_graph_run_equals_update_loop(case):
     """fr_run (CUDA-graph steady state) gives the same bits as fr_update."""
     a, meta = load_golden(case)
@@ -254,3 +255,19 @@ def test_async_state_copy(precision):
     s.get_state_async(pinned)
     s.synchronize()
     assert np.array_equal(pinned, s.get_state())
+
+
+def test_moving_mesh_cases_are_not_batched():
+    a, meta = load_golden("motion1_2d_p3")
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    with pytest.raises(fb.FrError) as ei:
+        fb.Batch([s])
+    assert ei.value.code == fb.FR_ERR_UNSUPPORTED
+
+
+def test_moving_mesh_precision_form_refused():
+    a, meta = load_golden("motion1_2d_p3")
+    with pytest.raises(fb.FrError) as ei:
+        gpu_case(meta, precision=fb.FR_PREC_MIXED)
+    assert ei.value.code == fb.FR_ERR_UNSUPPORTED
