@@ -137,6 +137,7 @@ def _load() -> ctypes.CDLL:
         "fr_device_ptr": (i, [P, ctypes.c_char_p, ctypes.POINTER(P), ctypes.POINTER(sz)]),
         "fr_synchronize": (i, [P]),
         "fr_checkpoint": (i, [P]),
+        "fr_integrate_error": (i, [P, i, dp, i]),
         "fr_write_data": (i, [P, ctypes.c_char_p]),
         "fr_read_restart": (i, [P, ctypes.c_char_p]),
         "fr_bench_kernel": (i, [P, ctypes.c_char_p, i]),
@@ -261,6 +262,12 @@ class Solver:
 
     def pmg_cycle(self):
         self._check(lib.fr_pmg_cycle(self._c))
+
+    def integrate_error(self, error_norm: int = -1) -> np.ndarray:
+        """integrateError of the deck's test case (errorNorm 0, 1, 2; -1: deck's)."""
+        out = np.zeros(self.nFields)
+        self._check(lib.fr_integrate_error(self._c, int(error_norm), _dptr(out), self.nFields))
+        return out
 
     def checkpoint(self):
         """Snapshot for output; the copy to the host overlaps later steps."""

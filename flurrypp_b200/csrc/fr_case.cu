@@ -117,6 +117,15 @@ struct fr_case {
     unsigned int *err = nullptr;
   } mo;
 
+  // error integrals (testCase 1): evaluation tables for the solution-point
+  // (errorNorm 0) and Gauss-Legendre (1, 2) quadratures, built on first use
+  struct ErrorTables {
+    int nQ = 0;
+    double *opQ = nullptr, *wQ = nullptr, *shapeQ = nullptr;
+  } errT[2];
+  double *errXv = nullptr, *errElem = nullptr, *errOut = nullptr;
+  int *errC2v = nullptr;
+
   // solution output: primitive variables at the plot points, copied to a
   // pinned host buffer on a side stream so that stepping goes on meanwhile
   struct Checkpoint {
@@ -2356,6 +2365,108 @@ int fr_read_restart(fr_case *c, const char *path) {
     if (!c->cuda_ok("restart")) return FR_ERR_CUDA;
   }
   return FR_OK;
+}
+
+int fr_integrate_error(fr_case *c, int errorNorm, double *out, int nFields) {
+  PdlScope pdlScope(c);
+  if (!c || !out) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = c->hostOnly ? "host-only case: no device state" : "no state set";
+    return FR_ERR_STATE;
+  }
+  if (nFields != c->nF) {
+    c->err = "nFields mismatch";
+    return FR_ERR_ARG;
+  }
+  const int norm = errorNorm < 0 ? c->in.errorNorm : errorNorm;
+  if (norm < 0 || norm > 2) {
+    c->err = "errorNorm must be 0, 1 or 2";
+    return FR_ERR_ARG;
+  }
+  const int nd = c->nDims, nN = c->mesh.nNodes;
+  // tables: errorNorm 0 on the solution points, 1 and 2 on quadOrder points
+  auto &T = c->errT[norm == 0 ? 0 : 1];
+  if (!T.opQ) {
+    std::vector<fr::Pt> loc;
+    std::vector<double> op, w;
+    const int n = c->in.order + 1;
+    if (norm == 0) {
+      loc = fr::loc_spts(nd, c->in.order, c->in.sptsTypeQuad);
+      op.assign((size_t)c->nS * c->nS, 0.0);
+      for (int s2 = 0; s2 < c->nS; s2++) op[(size_t)s2 * c->nS + s2] = 1.0;
+      w = fr::spt_weights(nd, c->in.order);
+    } else {
+      if (c->in.quadOrder < 0 || c->in.quadOrder > 10) {
+        c->err = "quadOrder must be in 0..10";  // the reference's weight tables (src/points.cpp:435-520)
+        return FR_ERR_ARG;
+      }
+      loc = fr::loc_spts(nd, c->in.quadOrder, fr::PTS_LEGENDRE);
+      w = fr::spt_weights(nd, c->in.quadOrder);
+      const std::vector<double> s1 = fr::pts1d(c->in.sptsTypeQuad, c->in.order);
+      op.assign(loc.size() * c->nS, 0.0);
+      for (size_t q = 0; q < loc.size(); q++)  // src/operators.cpp:241-280
+        for (int s2 = 0; s2 < c->nS; s2++) {
+          double v = fr::lagrange(s1, loc[q].x, s2 % n) * fr::lagrange(s1, loc[q].y, (s2 / n) % n);
+          if (nd == 3) v *= fr::lagrange(s1, loc[q].z, s2 / (n * n));
+          op[q * c->nS + s2] = v;
+        }
+    }
+    std::vector<double> N, dN;
+    std::string e;
+    if (!fr::shape_tables(nd, nN, loc, N, dN, e)) {
+      c->err = e;
+      return FR_ERR_ARG;
+    }
+    if (!c->upload(T.opQ, op) || !c->upload(T.wQ, w) || !c->upload(T.shapeQ, N)) return FR_ERR_CUDA;
+    T.nQ = (int)loc.size();
+  }
+  if (!c->errElem) {
+    if (!c->alloc(c->errElem, 2 * (size_t)c->E * c->nF) || !c->alloc(c->errOut, c->nF)) return FR_ERR_CUDA;
+    if (!c->mo.on) {
+      std::vector<double> xv(c->mesh.xv.begin(), c->mesh.xv.begin() + (size_t)c->mesh.nVerts * nd);
+      if (!c->upload(c->errXv, xv) || !c->upload(c->errC2v, c->mesh.c2v)) return FR_ERR_CUDA;
+    }
+  }
+  frk::ErrorArgs a;
+  a.nDims = nd;
+  a.nS = c->nS;
+  a.nQ = T.nQ;
+  a.E = c->E;
+  a.nF = c->nF;
+  a.nNodes = nN;
+  a.icType = c->in.icType;
+  a.testCase = c->in.testCase;
+  a.errorNorm = norm;
+  a.gamma = c->in.gamma;
+  a.pIC = c->in.pIC;
+  a.rhoIC = c->in.rhoIC;
+  a.vortexAngle = c->in.vortexAngle;
+  a.pi = 4.0 * std::atan(1.0);  // the reference's pi (include/global.hpp:72)
+  // periodic box of the exact vortex (src/funcs.cpp:1349-1358, 1391-1400)
+  if (c->in.meshType == 1) {
+    a.xmin = c->in.xmin, a.xmax = c->in.xmax, a.ymin = c->in.ymin, a.ymax = c->in.ymax;
+  } else if (c->in.icType == 2) {
+    a.xmin = c->in.vortexXmin, a.xmax = c->in.vortexXmax, a.ymin = c->in.vortexYmin, a.ymax = c->in.vortexYmax;
+  }
+  a.time = c->timeAcc;
+  if (c->mixed) c->join_state();
+  a.U = c->U;
+  a.detJ = c->detJ;
+  a.opQ = T.opQ;
+  a.wQ = T.wQ;
+  a.shapeQ = T.shapeQ;
+  a.xv = c->mo.on ? c->mo.a.xv : c->errXv;
+  a.c2v = c->mo.on ? c->mo.a.c2v : c->errC2v;
+  a.elemErr = c->errElem;
+  a.elemU = c->errElem + (size_t)c->E * c->nF;
+  frk::launch_error_integral(a, c->errOut, c->stream);
+  c->launches += 2;
+  if (cudaMemcpyAsync(out, c->errOut, c->nF * sizeof(double), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "cudaMemcpy D2H failed";
+    return FR_ERR_CUDA;
+  }
+  return c->sync() ? FR_OK : FR_ERR_CUDA;
 }
 
 int fr_synchronize(fr_case *c) {

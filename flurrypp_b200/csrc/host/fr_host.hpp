@@ -51,6 +51,8 @@ struct Input {
          pBound = 0.7142857143;
   double rhoIC = 1.0, vxIC = 0.2, vyIC = 0.0, vzIC = 0.0, pIC = 0.7142857143;
   double vortexAngle = 0.4636476090008061;  // atan(0.5)
+  double vortexXmin = -5, vortexXmax = 5, vortexYmin = -5, vortexYmax = 5;
+  int errorNorm = 1, quadOrder = 10;  // error integrals against an exact solution (testCase 1)
   int timeType = 4;
   int dtType = 0;
   int iterMax = 0;

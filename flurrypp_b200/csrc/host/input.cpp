@@ -94,6 +94,10 @@ bool read_deck(const std::string &path, Input &in, std::string &err) {
     d.get("pIC", in.pIC);
   } else if (in.icType == 2) {
     d.get("vortexAngle", in.vortexAngle);
+    d.get("vortexXmin", in.vortexXmin);
+    d.get("vortexXmax", in.vortexXmax);
+    d.get("vortexYmin", in.vortexYmin);
+    d.get("vortexYmax", in.vortexYmax);
   }
   d.get("timeType", in.timeType);
   d.get("dtType", in.dtType);
@@ -190,6 +194,8 @@ bool read_deck(const std::string &path, Input &in, std::string &err) {
   d.get("periodicDZ", in.periodicDZ);
   d.get("periodicTol", in.periodicTol);
   d.get("resType", in.resType);
+  d.get("errorNorm", in.errorNorm);  // reference: src/input.cpp:424-425
+  d.get("quadOrder", in.quadOrder);
   std::string spts = "Legendre";
   d.get("spts_type_quad", spts);
   if (spts == "Legendre")

@@ -280,6 +280,22 @@ void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const 
 void launch_motion_step_b(long long nSE, int nF, int E, const double *base, const MotionStages &stages,
                           const double *detJ, const double *dt, const double *eleDt, double *U, cudaStream_t st);
 
+// ---- error integrals against the exact solution (error.cu) ---------------
+struct ErrorArgs {
+  int nDims = 2, nS = 0, nQ = 0, E = 0, nF = 0, nNodes = 0;
+  int icType = 0, testCase = 0, errorNorm = 0;
+  double gamma = 1.4, pIC = 1, rhoIC = 1, vortexAngle = 0, pi = 0;
+  double xmin = -5, xmax = 5, ymin = -5, ymax = 5;  // periodic box of the exact vortex
+  const double *time = nullptr;                     // device scalar
+  const double *U = nullptr, *detJ = nullptr;       // [nS][E][nF], [nS][E]
+  const double *opQ = nullptr, *wQ = nullptr;       // [nQ][nS] spts -> evaluation points, weights
+  const double *shapeQ = nullptr;                   // [nQ][nNodes]
+  const double *xv = nullptr;                       // vertex positions [nVerts][nDims]
+  const int *c2v = nullptr;                         // [E][nNodes]
+  double *elemErr = nullptr, *elemU = nullptr;      // per-element integrals [E][nF]
+};
+void launch_error_integral(const ErrorArgs &a, double *out, cudaStream_t st);
+
 // Primitive variables at the plot points from the FP64 state (output only).
 void launch_plot_primitives(int nDims, const double *U, const double *opp, double *Vp, int nS, int nP, int E,
                             double gamma, cudaStream_t st);

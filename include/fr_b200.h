@@ -192,6 +192,15 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count);
  * <dataFileName>_<restartIter>.vtu of the deck, and the iteration count
  * becomes restartIter.  fr_init_solution with kind 0 on a deck with
  * "restart 1" reads that file instead of the initial condition. */
+/* solver::integrateError (src/solver.cpp:1945-2028) as writeError reports
+ * it for testCase 1: per field, errorNorm 0 the integral of the exact
+ * solution (|int(U - exact) - int U|, solution-point quadrature), 1 the
+ * integral of |U - exact| and 2 the square root of the integral of
+ * (U - exact)^2 on (quadOrder+1)^d Gauss points; exact = the deck's icType
+ * field at the current time (src/funcs.cpp:1318-1476).  errorNorm < 0: the
+ * deck's.  No reference counterpart for other testCase values. */
+int fr_integrate_error(fr_case *c, int errorNorm, double *out, int nFields);
+
 int fr_checkpoint(fr_case *c);
 int fr_write_data(fr_case *c, const char *path);
 int fr_read_restart(fr_case *c, const char *path);

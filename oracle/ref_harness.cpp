@@ -24,6 +24,8 @@
  *   --steps N                     time steps after the residual dump
  *   --time K,W                    W untimed then K timed steps, print JSON
  *   --threads T                   OpenMP threads (omp build)
+ *   --error                       after the steps, dump solver::integrateError
+ *                                 for errorNorm 0, 1, 2 (err_integrals [3][nF])
  *   --write-vtu PREFIX            after the steps, writeData with dataFileName
  *                                 PREFIX (the deck's plotType: 1 ParaView
  *                                 PREFIX_<iter>.vtu, 0 CSV PREFIX.csv.<iter>)
@@ -103,6 +105,7 @@ struct Opts {
   int timeK = 0, timeW = 0;
   int threads = 0;
   std::string vtu;
+  bool error = false;
 };
 
 /* Uniform double in [0,1) from the top 53 bits of a 64-bit Mersenne twister
@@ -290,6 +293,7 @@ int main(int argc, char **argv) {
       if (sscanf(next(), "%d,%d", &o.timeK, &o.timeW) != 2) exit(2);
     } else if (a == "--threads") o.threads = atoi(next());
     else if (a == "--write-vtu") o.vtu = next();
+    else if (a == "--error") o.error = true;
     else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
   }
   fr_refshim_blas_threads(1);
@@ -363,6 +367,16 @@ int main(int argc, char **argv) {
       for (auto &e : S.eles) edt.push_back(e->dt);
       dumpd("ele_dt", edt, {S.nEles});
     }
+  }
+
+  if (o.error && g_manifest) {
+    std::vector<double> errs;
+    for (int nrm = 0; nrm < 3; nrm++) {
+      params.errorNorm = nrm;
+      std::vector<double> e = S.integrateError();
+      errs.insert(errs.end(), e.begin(), e.end());
+    }
+    dumpd("err_integrals", errs, {3, (size_t)S.nFields});
   }
 
   if (!o.vtu.empty()) {

@@ -47,7 +47,7 @@ SETUP = ["opp_spts_to_fpts", "opp_grad_spts_0", "opp_grad_spts_1", "opp_grad_spt
          "face_bc", "face_fptR"]
 RESID = ["U_init", "U_fpts", "F_spts", "Fn_fpts", "disFn_fpts", "divF_0", "waveSp_fpts",
          "dU_spts", "dU_fpts", "dUc_fpts"]
-FINAL = ["U_final", "time_dt", "ele_dt"]
+FINAL = ["U_final", "time_dt", "ele_dt", "err_integrals"]
 
 # name -> (deck, harness args, steps, keep)
 CASES = {
@@ -110,6 +110,15 @@ CASES = {
                             10, "all"),
     "motion2_3d_p2": ("motion2_3d_p2", ["--ic", "vortex", "--vortex", "3,0.13,-0.21,0.5", "--cfl-dt", "0.5"], 4, "all"),
     "motion5_3d_p1": ("motion5_3d_p1", ["--ic", "vortex", "--vortex", "1,1.5,1.5,0.5"], 6, "all"),
+    "err_ic1_2d_p3": ("err_ic1_2d_p3", ["--cfl-dt", "0.5", "--error"], 10, "all"),
+    "err_ic2_2d_p3": ("err_ic2_2d_p3", ["--cfl-dt", "0.5", "--error"], 10, "all"),
+    # the reference's own run of its icType 1 vortex at 32x32 P3, the deck's dt:
+    # error integrals only (the test starts from the deck's initial condition)
+    "err_ic1_2d_p3_32": ("err_ic1_2d_p3_32", ["--error"], 20, ["err_integrals", "time_dt"]),
+    "err_entropy3d_p2": ("err_entropy3d_p2", ["--ic", "tgv", "--tgv-mach", "0.3", "--cfl-dt", "0.5", "--error"], 4,
+                         "all"),
+    "err_curved2d_p3": ("err_curved2d_p3", ["--cfl-dt", "0.5", "--error"], 6, "all"),
+    "err_motion2d_p3": ("err_motion2d_p3", ["--cfl-dt", "0.5", "--error"], 6, "all"),
     "naca_p4": ("naca_p4", [], 0, "summary"),
     "cyl3d_p2": ("cyl3d_p2", [], 0, "summary"),
 }

@@ -271,3 +271,34 @@ def test_moving_mesh_precision_form_refused():
     with pytest.raises(fb.FrError) as ei:
         gpu_case(meta, precision=fb.FR_PREC_MIXED)
     assert ei.value.code == fb.FR_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("case", golden_cases(require=("err_integrals", "U_init")))
+def test_error_integrals_match_reference(case):
+    """solver::integrateError (errorNorm 0, 1, 2) after the fixture's steps:
+    the exact-solution error integrals of testCase 1 as the reference reports
+    them, on straight, curved and moving meshes."""
+    a, meta = load_golden(case)
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    for _ in range(meta["steps"]):
+        s.update()
+    want = a["err_integrals"]
+    for norm in range(3):
+        got = s.integrate_error(norm)
+        scale = float(np.max(np.abs(want[norm])))
+        assert np.max(np.abs(got - want[norm])) <= 1e-9 * scale, (norm, got, want[norm])
+
+
+def test_error_integrals_of_the_reference_vortex_run():
+    """The reference's icType 1 vortex, 32x32 P3, 20 steps of the deck's dt,
+    started from the deck's own initial condition: L1, L2 and conservation
+    error integrals as the reference reports them."""
+    a, meta = load_golden("err_ic1_2d_p3_32")
+    s = fb.Solver(deck_path(meta))
+    s.initialize_solution()
+    s.run(meta["steps"])
+    assert s.info().time == pytest.approx(a["time_dt"][0], rel=1e-14)
+    for norm in range(3):
+        got, want = s.integrate_error(norm), a["err_integrals"][norm]
+        assert np.max(np.abs(got - want)) <= 1e-9 * np.max(np.abs(want)), (norm, got, want)
