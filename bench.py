@@ -394,14 +394,21 @@ def form_serve(args, fb, torch):
         msh = os.path.join(tmp, f"bump{i}.msh")
         write_gmsh(msh, channel_bump(nx, nx // 3, h))
         dof = nx * (nx // 3) * (P + 1) ** 2 * 4
-        reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), dof))
+        # residual evaluations per driver step on every P-multigrid level
+        # (lowOrder 0, 2 smoothing steps, RK4): the fine update's 4 stages and
+        # the cycle's fine residual; per coarse level p its source-term
+        # residual, 2 x 2 smoothing updates of 4 stages and, above level 0,
+        # the residual restricted downwards
+        all_dof = dof * 5 + sum(nx * (nx // 3) * (p + 1) ** 2 * 4 * (1 + 2 * 2 * 4 + (1 if p > 0 else 0))
+                                for p in range(P))
+        reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), dof, all_dof))
 
     def serve(subset, max_inflight, rate):
         srv = fb.Server(budget_bytes=args.serve_budget_gb << 30, max_inflight=max_inflight, check_every=10)
         gaps = np.random.default_rng(args.serve_seed + 1).exponential(1.0 / rate, len(subset)) if rate else None
         t0 = time.perf_counter()
         ids = []
-        for k, (deck, dof) in enumerate(subset):
+        for k, (deck, dof, _) in enumerate(subset):
             if rate:
                 time.sleep(float(gaps[k]))
             ids.append(srv.submit(deck, tol=1e-8, max_steps=args.serve_max_steps))
@@ -416,13 +423,14 @@ def form_serve(args, fb, torch):
         srv.close()
         lat = [p["latency_s"] for p in polls]
         done = [p for p in polls if p["status"] == 2]
-        stages = sum(4 * p["steps"] * dof for p, (_, dof) in zip(polls, subset))
+        stages = sum(4 * p["steps"] * dof for p, (_, dof, _) in zip(polls, subset))
+        all_stages = sum(p["steps"] * all_dof for p, (_, _, all_dof) in zip(polls, subset))
         return {"solves_per_s": len(done) / sec, "seconds": sec, "completed": len(done),
                 "converged_1e-8": sum(1 for p in done if p["res_ratio"] <= 1e-8),
                 "median_residual_drop": float(np.median([p["res_ratio"] for p in done])) if done else None,
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                 "steps_mean": float(np.mean([p["steps"] for p in polls])),
-                "fine_dof_stage_per_s": stages / sec}
+                "fine_dof_stage_per_s": stages / sec, "all_level_dof_stage_per_s": all_stages / sec}
 
     sweep = {}
     for rate in args.serve_rates:
