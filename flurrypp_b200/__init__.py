@@ -138,6 +138,8 @@ def _load() -> ctypes.CDLL:
         "fr_synchronize": (i, [P]),
         "fr_checkpoint": (i, [P]),
         "fr_integrate_error": (i, [P, i, dp, i]),
+        "fr_wall_force": (i, [P, dp]),
+        "fr_mass_flux": (i, [P, i, dp, i]),
         "fr_write_data": (i, [P, ctypes.c_char_p]),
         "fr_read_restart": (i, [P, ctypes.c_char_p]),
         "fr_bench_kernel": (i, [P, ctypes.c_char_p, i]),
@@ -267,6 +269,18 @@ class Solver:
         """integrateError of the deck's test case (errorNorm 0, 1, 2; -1: deck's)."""
         out = np.zeros(self.nFields)
         self._check(lib.fr_integrate_error(self._c, int(error_norm), _dptr(out), self.nFields))
+        return out
+
+    def wall_force(self) -> np.ndarray:
+        """writeResidual's force coefficients: pressure (x, y, z), viscous (x, y, z)."""
+        out = np.zeros(6)
+        self._check(lib.fr_wall_force(self._c, _dptr(out)))
+        return out
+
+    def mass_flux(self, error_norm: int = -1) -> np.ndarray:
+        """computeMassFlux (testCase 2 monitor) per field."""
+        out = np.zeros(self.nFields)
+        self._check(lib.fr_mass_flux(self._c, int(error_norm), _dptr(out), self.nFields))
         return out
 
     def checkpoint(self):

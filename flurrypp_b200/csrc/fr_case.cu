@@ -124,6 +124,33 @@ struct fr_case {
     double *opQ = nullptr, *wQ = nullptr, *shapeQ = nullptr;
   } errT[2];
   double *errXv = nullptr, *errElem = nullptr, *errOut = nullptr;
+  double *monPart = nullptr, *monOut = nullptr;  // boundary monitors: per-point parts, totals
+
+  // wall forces and mass flux from the face data of the last residual
+  // evaluation (boundFace::computeWallForce / computeMassFlux)
+  bool boundary_monitors(int errorNorm, double *host11) {
+    const int nB = ft.n - ft.nInterior;
+    if (!monOut && (!alloc(monPart, (size_t)std::max(nB, 1) * 11) || !alloc(monOut, 11))) return false;
+    if (!mixed) {
+      frk::MonitorArgsT<double> a;
+      a.E = E, a.nPF = nPF, a.nI = ft.nInterior, a.n = ft.n;
+      a.slotL = ft.slotL, a.slotR = ft.slotR, a.nrm = ft.nrm, a.dAL = ft.dAL;
+      a.Uf = Ufpts, a.Fn = Fn, a.dUf = in.viscous ? dUf : nullptr, a.fStride = (long long)nFp * E * nF;
+      a.wSurf = wSurf, a.ph = ph, a.errorNorm = errorNorm, a.part = monPart;
+      frk::launch_boundary_monitors<double>(nDims, a, monOut, stream);
+    } else {
+      frk::MonitorArgsT<float> a;
+      a.E = E, a.nPF = nPF, a.nI = f32.ft.nInterior, a.n = f32.ft.n;
+      a.slotL = f32.ft.slotL, a.slotR = f32.ft.slotR, a.nrm = f32.ft.nrm, a.dAL = f32.ft.dAL;
+      a.Uf = f32.Ufpts, a.Fn = f32.Fn, a.dUf = in.viscous ? f32.dUf : nullptr, a.fStride = (long long)nFp * E * nF;
+      a.wSurf = wSurf, a.ph = ph, a.errorNorm = errorNorm, a.part = monPart;
+      frk::launch_boundary_monitors<float>(nDims, a, monOut, stream);
+    }
+    launches += 2;
+    if (cudaMemcpyAsync(host11, monOut, 11 * sizeof(double), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+      return fail(FR_ERR_CUDA, "cudaMemcpy D2H failed");
+    return sync();
+  }
   int *errC2v = nullptr;
 
   // solution output: primitive variables at the plot points, copied to a
@@ -2467,6 +2494,50 @@ int fr_integrate_error(fr_case *c, int errorNorm, double *out, int nFields) {
     return FR_ERR_CUDA;
   }
   return c->sync() ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_wall_force(fr_case *c, double *out) {
+  PdlScope pdlScope(c);
+  if (!c || !out) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = c->hostOnly ? "host-only case: no device state" : "no state set";
+    return FR_ERR_STATE;
+  }
+  double v[11];
+  if (!c->boundary_monitors(0, v)) return FR_ERR_CUDA;
+  // writeResidual (src/output.cpp:1048-1066): coefficients on 0.5 rho U^2 of
+  // the boundary state, turned to the free-stream direction
+  const auto &in = c->in;
+  const double wB = c->nDims == 2 ? 0.0 : in.wBound;
+  const double Uinf = std::sqrt(in.uBound * in.uBound + in.vBound * in.vBound + wB * wB);
+  double f[6];
+  for (int k = 0; k < 6; k++) f[k] = v[k] / (0.5 * in.rhoBound * Uinf * Uinf);
+  const double alpha = std::atan2(in.vBound, in.uBound);
+  out[0] = f[0] * std::cos(alpha) + f[1] * std::sin(alpha);
+  out[1] = f[1] * std::cos(alpha) - f[0] * std::sin(alpha);
+  out[2] = f[2];
+  out[3] = in.viscous ? f[3] * std::cos(alpha) + f[4] * std::sin(alpha) : f[3];
+  out[4] = in.viscous ? f[4] * std::cos(alpha) - f[3] * std::sin(alpha) : f[4];
+  out[5] = f[5];
+  return FR_OK;
+}
+
+int fr_mass_flux(fr_case *c, int errorNorm, double *out, int nFields) {
+  PdlScope pdlScope(c);
+  if (!c || !out) return FR_ERR_ARG;
+  if (c->hostOnly || !c->stateSet) {
+    c->err = c->hostOnly ? "host-only case: no device state" : "no state set";
+    return FR_ERR_STATE;
+  }
+  const int norm = errorNorm < 0 ? c->in.errorNorm : errorNorm;
+  if (nFields != c->nF || norm < 0 || norm > 2) {
+    c->err = "nFields mismatch or errorNorm outside 0..2";
+    return FR_ERR_ARG;
+  }
+  double v[11];
+  if (!c->boundary_monitors(norm, v)) return FR_ERR_CUDA;
+  for (int k = 0; k < c->nF; k++) out[k] = v[6 + k];
+  return FR_OK;
 }
 
 int fr_synchronize(fr_case *c) {

@@ -280,6 +280,24 @@ void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const 
 void launch_motion_step_b(long long nSE, int nF, int E, const double *base, const MotionStages &stages,
                           const double *detJ, const double *dt, const double *eleDt, double *U, cudaStream_t st);
 
+// ---- boundary monitors: wall forces and mass flux (monitor.cu) -----------
+template <typename R>
+struct MonitorArgsT {
+  int E = 0, nPF = 0, nI = 0, n = 0;       // face-point table: boundary points are [nI, n)
+  const int *slotL = nullptr, *slotR = nullptr;
+  const R *nrm = nullptr, *dAL = nullptr;
+  const R *Uf = nullptr, *Fn = nullptr;    // U_fpts, Fn_fpts (= common flux * dA)
+  const R *dUf = nullptr;                  // viscous: gradient at the flux points, else null
+  long long fStride = 0;                   // dUf stride between dimensions
+  const double *wSurf = nullptr;           // [nPF] Gauss weights within a face
+  Phys ph{};
+  int errorNorm = 0;
+  double *part = nullptr;                  // [n - nI][11] scratch
+};
+// out[0..5]: pressure and viscous force (x, y, z each); out[6..]: mass flux per field.
+template <typename R>
+void launch_boundary_monitors(int nDims, const MonitorArgsT<R> &a, double *out, cudaStream_t st);
+
 // ---- error integrals against the exact solution (error.cu) ---------------
 struct ErrorArgs {
   int nDims = 2, nS = 0, nQ = 0, E = 0, nF = 0, nNodes = 0;

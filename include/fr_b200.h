@@ -201,6 +201,20 @@ int fr_get_array(fr_case *c, const char *name, void *host, size_t *count);
  * deck's.  No reference counterpart for other testCase values. */
 int fr_integrate_error(fr_case *c, int errorNorm, double *out, int nFields);
 
+/* Boundary monitors on the face data of the last residual evaluation (call
+ * fr_calc_residual first to evaluate them on the current state).
+ * fr_wall_force: the force coefficients writeResidual prints
+ * (src/output.cpp:1048-1066, boundFace::computeWallForce,
+ * src/boundFace.cpp:412-458): out[0..2] pressure force, out[3..5] viscous
+ * force, summed over slip, adiabatic and isothermal walls, divided by
+ * 0.5 rhoBound Uinf^2 and turned to the free-stream direction (x, y).
+ * fr_mass_flux: boundFace::computeMassFlux (src/boundFace.cpp:460-496), the
+ * testCase 2 monitor: per field, the common flux through characteristic and
+ * sub/supersonic boundaries, integrated (errorNorm 0), |.| n_x (1) or
+ * (.)^2 n_x (2); errorNorm < 0: the deck's. */
+int fr_wall_force(fr_case *c, double *out);
+int fr_mass_flux(fr_case *c, int errorNorm, double *out, int nFields);
+
 int fr_checkpoint(fr_case *c);
 int fr_write_data(fr_case *c, const char *path);
 int fr_read_restart(fr_case *c, const char *path);

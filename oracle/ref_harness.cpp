@@ -24,6 +24,10 @@
  *   --steps N                     time steps after the residual dump
  *   --time K,W                    W untimed then K timed steps, print JSON
  *   --threads T                   OpenMP threads (omp build)
+ *   --monitors                    after the steps, calcResidual(0) and dump the
+ *                                 wall-force coefficients writeResidual prints
+ *                                 (wall_force [6]) and computeMassFlux for
+ *                                 errorNorm 0, 1, 2 (mass_flux [3][nF])
  *   --error                       after the steps, dump solver::integrateError
  *                                 for errorNorm 0, 1, 2 (err_integrals [3][nF])
  *   --write-vtu PREFIX            after the steps, writeData with dataFileName
@@ -106,6 +110,7 @@ struct Opts {
   int threads = 0;
   std::string vtu;
   bool error = false;
+  bool monitors = false;
 };
 
 /* Uniform double in [0,1) from the top 53 bits of a 64-bit Mersenne twister
@@ -294,6 +299,7 @@ int main(int argc, char **argv) {
     } else if (a == "--threads") o.threads = atoi(next());
     else if (a == "--write-vtu") o.vtu = next();
     else if (a == "--error") o.error = true;
+    else if (a == "--monitors") o.monitors = true;
     else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
   }
   fr_refshim_blas_threads(1);
@@ -377,6 +383,29 @@ int main(int argc, char **argv) {
       errs.insert(errs.end(), e.begin(), e.end());
     }
     dumpd("err_integrals", errs, {3, (size_t)S.nFields});
+  }
+
+  if (o.monitors && g_manifest) {
+    S.calcResidual(0);
+    /* src/output.cpp:1048-1066 */
+    std::vector<double> force = S.computeWallForce();
+    for (auto &f : force) f /= (0.5 * params.rhoBound * params.Uinf * params.Uinf);
+    double alpha = std::atan2(params.vBound, params.uBound);
+    std::vector<double> fTmp = force;
+    force[0] = fTmp[0] * cos(alpha) + fTmp[1] * sin(alpha);
+    force[1] = fTmp[1] * cos(alpha) - fTmp[0] * sin(alpha);
+    if (params.viscous) {
+      force[3] = fTmp[3] * cos(alpha) + fTmp[4] * sin(alpha);
+      force[4] = fTmp[4] * cos(alpha) - fTmp[3] * sin(alpha);
+    }
+    dumpd("wall_force", force, {6});
+    std::vector<double> flux;
+    for (int nrm = 0; nrm < 3; nrm++) {
+      params.errorNorm = nrm;
+      std::vector<double> m = S.computeMassFlux();
+      flux.insert(flux.end(), m.begin(), m.end());
+    }
+    dumpd("mass_flux", flux, {3, (size_t)S.nFields});
   }
 
   if (!o.vtu.empty()) {

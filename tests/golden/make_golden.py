@@ -47,7 +47,7 @@ SETUP = ["opp_spts_to_fpts", "opp_grad_spts_0", "opp_grad_spts_1", "opp_grad_spt
          "face_bc", "face_fptR"]
 RESID = ["U_init", "U_fpts", "F_spts", "Fn_fpts", "disFn_fpts", "divF_0", "waveSp_fpts",
          "dU_spts", "dU_fpts", "dUc_fpts"]
-FINAL = ["U_final", "time_dt", "ele_dt", "err_integrals"]
+FINAL = ["U_final", "time_dt", "ele_dt", "err_integrals", "wall_force", "mass_flux"]
 
 # name -> (deck, harness args, steps, keep)
 CASES = {
@@ -79,19 +79,19 @@ CASES = {
                                                   "--cfl-dt", "0.3"], 4, "all"),
     "ns_tgv3d_p3_3": ("ns_tgv3d_p3_3", ["--ic", "tgv", "--tgv-mach", "0.1", "--cfl-dt", "0.3"], 3, "all"),
     "ns_vortex2d_p3_6": ("ns_vortex2d_p3_6", ["--ic", "vortex", "--vortex", "3,0,0,0.5", "--cfl-dt", "0.3"], 10, "all"),
-    "ns_walls2d_p2": ("ns_walls2d_p2", ["--ic", "uniform", "--cfl-dt", "0.2"], 10, "all"),
+    "ns_walls2d_p2": ("ns_walls2d_p2", ["--ic", "uniform", "--cfl-dt", "0.2", "--monitors"], 10, "all"),
     "ns_sutherland2d_p3": ("ns_sutherland2d_p3", ["--ic", "vortex", "--vortex", "2,0,0,0.3"], 10, "all"),
     "pmg_vortex2d_p3_8": ("pmg_vortex2d_p3_8", ["--ic", "vortex", "--vortex", "5,0,0,0.5"], 5, "all"),
     "pmg_tgv3d_p3_3": ("pmg_tgv3d_p3_3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.4"], 3, "all"),
     "chbump_p2_pmg": ("chbump_p2_pmg", [], 5, "all"),
-    "chbump_p3": ("chbump_p3", [], 10, "all"),
-    "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5"], 5, "all"),
+    "chbump_p3": ("chbump_p3", ["--monitors"], 10, "all"),
+    "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5", "--monitors"], 5, "all"),
     "curved2d_q2_p3": ("curved2d_q2_p3", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),
     "curved2d_q4_p2": ("curved2d_q4_p2", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),
     "curved3d_q2_p2": ("curved3d_q2_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 4, "all"),
     "curved3d_s20_p2": ("curved3d_s20_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 4, "all"),
     "curved3d_q3_p3": ("curved3d_q3_p3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.5"], 3, "all"),
-    "cyl2d_p2": ("cyl2d_p2", [], 10, "all"),
+    "cyl2d_p2": ("cyl2d_p2", ["--monitors"], 10, "all"),
     "lobatto_hu3d_p3": ("lobatto_hu3d_p3", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "13,0.05"], 5, "all"),
     "cplus_rk2_3d_p2": ("cplus_rk2_3d_p2", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "17,0.05"], 6, "all"),
     "sd_euler3d_p4": ("sd_euler3d_p4", ["--ic", "tgv", "--tgv-mach", "0.2", "--perturb", "19,0.05"], 6, "all"),
@@ -100,8 +100,8 @@ CASES = {
     # vortex centre off the face-point columns: on a column through the centre
     # the normal velocity at the far-field faces is zero up to round-off, and
     # the characteristic condition's inflow/outflow branch follows its sign
-    "supsub3d_p2": ("supsub3d_p2", ["--ic", "vortex", "--vortex", "2,0.13,-0.21,0.5", "--cfl-dt", "0.4"], 6, "all"),
-    "ns_walls3d_p2": ("ns_walls3d_p2", ["--ic", "uniform"], 6, "all"),
+    "supsub3d_p2": ("supsub3d_p2", ["--ic", "vortex", "--vortex", "2,0.13,-0.21,0.5", "--cfl-dt", "0.4", "--monitors"], 6, "all"),
+    "ns_walls3d_p2": ("ns_walls3d_p2", ["--ic", "uniform", "--monitors"], 6, "all"),
     "motion1_2d_p3": ("motion1_2d_p3", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5", "--cfl-dt", "0.5"], 10, "all"),
     "motion2_2d_p2_cfl": ("motion2_2d_p2_cfl", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 10, "all"),
     "motion2_2d_p3_jameson": ("motion2_2d_p3_jameson", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 8, "all"),

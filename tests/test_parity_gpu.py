@@ -302,3 +302,26 @@ def test_error_integrals_of_the_reference_vortex_run():
     for norm in range(3):
         got, want = s.integrate_error(norm), a["err_integrals"][norm]
         assert np.max(np.abs(got - want)) <= 1e-9 * np.max(np.abs(want)), (norm, got, want)
+
+
+@pytest.mark.parametrize("case", golden_cases(require=("wall_force", "U_init")))
+def test_boundary_monitors_match_reference(case):
+    """Wall-force coefficients as writeResidual prints them and the testCase 2
+    mass flux (errorNorm 0, 1, 2), on the face data of a residual evaluated
+    after the fixture's steps (2-D/3-D, slip and viscous walls, far field,
+    sub/supersonic boundaries, the reference's cylinder mesh)."""
+    a, meta = load_golden(case)
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    for _ in range(meta["steps"]):
+        s.update()
+    s.calc_residual(0)
+    f, want = s.wall_force(), a["wall_force"]
+    assert np.max(np.abs(f - want)) <= 1e-9 * max(np.max(np.abs(want)), 1e-3), (f, want)
+    # inflow and outflow cancel in every norm (n_x carries its sign), so the
+    # sums are measured against the unit scale of the non-dimensional fluxes
+    flux = a["mass_flux"]
+    for norm in range(3):
+        got = s.mass_flux(norm)
+        assert np.max(np.abs(got - flux[norm])) <= 1e-10 * max(1.0, np.max(np.abs(flux[norm]))), \
+            (norm, got, flux[norm])
