@@ -5,7 +5,10 @@
 // files like the reference's loop: at the start, every plotFreq iterations
 // (taken as checkpoints, written while the next steps run) and at the end.
 //
-//   flurry_b200 DECK NSTEPS [FREQ [WRITE [PLOTFREQ]]]
+// With ERR = 1 it ends with the error integrals of a testCase 1 deck.
+//
+//   flurry_b200 DECK NSTEPS [FREQ [WRITE [PLOTFREQ [ERR]]]]
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 
@@ -20,6 +23,7 @@ int main(int argc, char **argv) {
   const int freq = argc > 3 ? std::atoi(argv[3]) : 10;
   const bool write = argc > 4 && std::atoi(argv[4]) != 0;
   const int plotFreq = argc > 5 ? std::atoi(argv[5]) : 100;
+  const bool err = argc > 6 && std::atoi(argv[6]) != 0;
   try {
     fr::b200::Solver S;
     S.setup(argv[1]);
@@ -48,6 +52,15 @@ int main(int argc, char **argv) {
       }
     }
     if (pending) S.writeData();
+    if (err) {  // writeAllError for testCase 1 (src/output.cpp:1212-1227)
+      const char *what[3] = {"Integrated conservation error", "Integral L1 error", "Integral L2 error"};
+      for (int n = 0; n < 3; n++) {
+        auto e = S.integrateError(n);
+        std::printf("%s:\n%-8lld Err ", what[n], S.info().iter);
+        for (double v : e) std::printf(" %.6e", std::fabs(v));
+        std::printf("\n");
+      }
+    }
   } catch (const fr::b200::Error &e) {
     std::fprintf(stderr, "fr_b200 error %d: %s\n", e.code, e.what());
     return 1;

@@ -82,6 +82,24 @@ class Solver {
   void writeData(const char *path = nullptr) { check(fr_write_data(c_, path)); }
   void readRestartFile(const char *path = nullptr) { check(fr_read_restart(c_, path)); }
 
+  // integrateError (src/solver.cpp:1945-2028), writeResidual's force
+  // coefficients, computeMassFlux (testCase 2)
+  std::vector<double> integrateError(int errorNorm = -1) {
+    std::vector<double> e(info_.nFields);
+    check(fr_integrate_error(c_, errorNorm, e.data(), info_.nFields));
+    return e;
+  }
+  std::vector<double> wallForce() {
+    std::vector<double> f(6);
+    check(fr_wall_force(c_, f.data()));
+    return f;
+  }
+  std::vector<double> massFlux(int errorNorm = -1) {
+    std::vector<double> m(info_.nFields);
+    check(fr_mass_flux(c_, errorNorm, m.data(), info_.nFields));
+    return m;
+  }
+
   const fr_info &info() {
     check(fr_get_info(c_, &info_));
     return info_;
