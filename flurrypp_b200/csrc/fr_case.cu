@@ -84,6 +84,7 @@ struct fr_case {
   // own fixed dt held per element
   bool perElementDt = false;
   double *sol = nullptr, *corrPmg = nullptr;
+  float *src32 = nullptr;  // precision form: the P-multigrid source in FP32
   frk::Csr restrictOp, prolongOp;
   // precision form (FR_PREC_MIXED): the stage arrays in FP32; U (FP64) is
   // the boundary copy, and detJ, norm, dA, waveSp, the time step and the
@@ -265,7 +266,6 @@ struct fr_case {
       return fail(FR_ERR_UNSUPPORTED, "unknown precision");
     mixed = o.precision == FR_PREC_MIXED;
     if (!setup_host()) return false;
-    if (mixed && in.PMG) return fail(FR_ERR_UNSUPPORTED, "P-multigrid runs in the plain form, not the precision form");
     return setup_device();
   }
 
@@ -428,6 +428,7 @@ struct fr_case {
       return fail(FR_ERR_CUDA, "dt upload");
     if (in.PMG) {
       if (!alloc(src, nU) || !alloc(sol, nU) || !alloc(corrPmg, nU)) return false;
+      if (mixed && !alloc(src32, nU)) return false;
       if (in.order > 0 && !make_csr(op.restrict_, op.nSptsRes, nS, restrictOp)) return false;
       if (!make_csr(op.prolong, op.nSptsPro, nS, prolongOp)) return false;
       if (!pmgCoarse && !build_levels()) return false;
@@ -484,6 +485,17 @@ struct fr_case {
     C.fptsFresh = false;
     launches += 2;
   }
+  // precision form: the state restricted in FP64 from the joined state and
+  // split again on the coarse level; the FP32 residual restricted in FP32
+  void restrict_to32(fr_case &C) {
+    const long long N = (long long)C.E * C.nF;
+    join_state();
+    frk::launch_apply_op(restrictOp, U, C.U, N, 1.0, 0.0, stream);
+    C.split_state();
+    frk::launch_apply_op_t<float>(restrictOp, f32.divF[0], C.f32.divF[0], N, stream);
+    C.fptsFresh = false;
+    launches += 4;
+  }
   // prolong_err (multigrid.cpp:347-364): finer U += prolong(corr)
   void prolong_to(fr_case &F) {
     frk::launch_apply_op(prolongOp, corrPmg, F.U, (long long)E * nF, 1.0, 1.0, stream);
@@ -492,8 +504,54 @@ struct fr_case {
   }
 
   // multiGrid::cycle (multigrid.cpp:169-313) for this (finest) level
+  // multiGrid::cycle in the precision form: the smoothing stages run in FP32
+  // with the source term in FP32; the restriction of the state, the source
+  // term, the saved coarse solution, the correction and its prolongation run
+  // in FP64 on the joined state (join/split around each transfer)
+  bool pmg_cycle32() {
+    if (!calc_residual(0)) return false;
+    restrict_to32(*levels[in.order - 1]);
+    for (int P = in.order - 1; P >= in.lowOrder; P--) {
+      fr_case &L = *levels[P];
+      const long long n = (long long)L.nS * L.E * L.nF;
+      // compute_source_term (multigrid.cpp:366-384): restricted residual
+      // minus the coarse level's own
+      frk::launch_widen(n, L.f32.divF[0], L.src, stream);
+      if (!L.calc_residual(0)) return fail(FR_ERR_CUDA, L.err);
+      frk::launch_widen(n, L.f32.divF[0], L.corrPmg, stream);
+      frk::launch_add(n, L.src, L.src, L.corrPmg, -1.0, stream);
+      frk::launch_narrow(n, L.src, L.src32, stream);
+      L.join_state();
+      cudaMemcpyAsync(L.sol, L.U, n * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+      L.launches += 5;
+      for (int st = 0; st < in.smoothSteps; st++)
+        if (!L.update(true)) return fail(FR_ERR_CUDA, L.err);
+      if (P - 1 >= in.lowOrder) {
+        if (!L.calc_residual(0)) return fail(FR_ERR_CUDA, L.err);
+        frk::launch_add32(n, L.f32.divF[0], L.f32.divF[0], L.src32, 1.0, stream);
+        L.launches++;
+        L.restrict_to32(*levels[P - 1]);
+      }
+    }
+    for (int P = in.lowOrder; P <= in.order - 1; P++) {
+      fr_case &L = *levels[P];
+      const long long n = (long long)L.nS * L.E * L.nF;
+      for (int st = 0; st < in.smoothSteps; st++)
+        if (!L.update(true)) return fail(FR_ERR_CUDA, L.err);
+      L.join_state();
+      frk::launch_add(n, L.corrPmg, L.U, L.sol, -1.0, stream);
+      fr_case &F = P < in.order - 1 ? *levels[P + 1] : *this;
+      F.join_state();
+      L.prolong_to(F);
+      F.split_state();
+      L.launches += 4;
+    }
+    return cuda_ok("pmg_cycle");
+  }
+
   bool pmg_cycle() {
     if (!in.PMG || levels.empty()) return fail(FR_ERR_STATE, "no P-multigrid levels (PMG 0)");
+    if (mixed) return pmg_cycle32();
     const long long nU = (long long)nS * E * nF;
     if (!calc_residual(0)) return false;
     restrict_to(*levels[in.order - 1]);
@@ -1360,6 +1418,7 @@ struct fr_case {
       a.rka_next = rka;
       a.rkb = rkb;
       a.divF_out = keepDivF ? f32.divF[0] : nullptr;
+      a.src = pmgSource ? src32 : nullptr;
       a.Ufpts_out = f32.Ufpts;
       element32(a);
     }

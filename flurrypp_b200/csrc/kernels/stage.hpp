@@ -226,6 +226,7 @@ void launch_add_time(const double *dt, double *time_acc, cudaStream_t st);
 // out[i] = x[i] + sgn * y[i] (sgn = +1 or -1), the elementwise updates of the
 // P-multigrid cycle (reference: multigrid.cpp:199-205, 282-290, 366-384).
 void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st);
+void launch_add32(long long n, float *out, const float *x, const float *y, double sgn, cudaStream_t st);
 
 // Per-element residual norm contributions (reference: ele.cpp:1922-1944),
 // accumulated in FP64 whatever the type of divF.

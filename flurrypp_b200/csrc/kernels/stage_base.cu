@@ -417,8 +417,8 @@ __global__ void k_residual_norm(int nS, int E, int nF, const R *__restrict__ div
   }
 }
 
-__global__ void k_add(long long n, double *__restrict__ out, const double *__restrict__ x,
-                      const double *__restrict__ y, double sgn) {
+template <typename R>
+__global__ void k_add(long long n, R *__restrict__ out, const R *__restrict__ x, const R *__restrict__ y, double sgn) {
   pdl_wait();
   pdl_trigger();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -602,7 +602,12 @@ void launch_residual_norm(int nS, int E, int nF, const R *divF, const double *de
 
 void launch_add(long long n, double *out, const double *x, const double *y, double sgn, cudaStream_t st) {
   if (n <= 0) return;
-  launch_k(k_add, (unsigned)((n + 255) / 256), 256, 0, st, n, out, x, y, sgn);
+  launch_k(k_add<double>, (unsigned)((n + 255) / 256), 256, 0, st, n, out, x, y, sgn);
+}
+
+void launch_add32(long long n, float *out, const float *x, const float *y, double sgn, cudaStream_t st) {
+  if (n <= 0) return;
+  launch_k(k_add<float>, (unsigned)((n + 255) / 256), 256, 0, st, n, out, x, y, sgn);
 }
 
 template <typename R>

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 import flurrypp_b200 as fb
-from conftest import deck_path, golden_cases, has_motion, has_pmg, load_golden, perturb_opts, rel_err
+from conftest import deck_path, golden_cases, has_motion, load_golden, perturb_opts, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -35,9 +35,8 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-# P-multigrid and moving meshes run in the plain form only
-MIXED_CASES = [c for c in golden_cases(("U_init", "U_final"))
-               if not has_pmg(load_golden(c)[1]) and not has_motion(load_golden(c)[1])]
+# moving meshes run in the plain form only
+MIXED_CASES = [c for c in golden_cases(("U_init", "U_final")) if not has_motion(load_golden(c)[1])]
 
 
 @pytest.mark.parametrize("case", MIXED_CASES)
@@ -200,3 +199,19 @@ def test_tensor_core_variant_near_cuda_core_variant():
         s.run(20)
         out.append(s.get_state())
     assert rel_l2(out[1], out[0]) < 1e-7
+
+
+@pytest.mark.parametrize("case", ["pmg_vortex2d_p3_8", "chbump_p2_pmg"])
+def test_mixed_pmg_graph_equals_cycle_loop(case):
+    """Precision-form P-multigrid: the graph-replayed step (update + V-cycle)
+    equals update() followed by pmg_cycle() bit for bit."""
+    a, meta = load_golden(case)
+    s1 = mixed_case(meta)
+    s1.set_state(a["U_init"])
+    s1.run(4)
+    s2 = mixed_case(meta)
+    s2.set_state(a["U_init"])
+    for _ in range(4):
+        s2.update()
+        s2.pmg_cycle()
+    assert np.array_equal(s1.get_state(), s2.get_state())
