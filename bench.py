@@ -403,8 +403,9 @@ def form_serve(args, fb, torch):
                                 for p in range(P))
         reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), dof, all_dof))
 
-    def serve(subset, max_inflight, rate):
-        srv = fb.Server(budget_bytes=args.serve_budget_gb << 30, max_inflight=max_inflight, check_every=10)
+    def serve(subset, max_inflight, rate, precision=fb.FR_PREC_FP64):
+        srv = fb.Server(budget_bytes=args.serve_budget_gb << 30, max_inflight=max_inflight, check_every=10,
+                        precision=precision)
         gaps = np.random.default_rng(args.serve_seed + 1).exponential(1.0 / rate, len(subset)) if rate else None
         t0 = time.perf_counter()
         ids = []
@@ -435,6 +436,9 @@ def form_serve(args, fb, torch):
     sweep = {}
     for rate in args.serve_rates:
         sweep[f"rate_{rate:g}_per_s"] = dict(max_inflight=args.serve_inflight, **serve(reqs, args.serve_inflight, rate))
+    top = max(args.serve_rates)
+    precision = dict(max_inflight=args.serve_inflight, rate_per_s=top,
+                     **serve(reqs, args.serve_inflight, top, fb.FR_PREC_MIXED))
     k = min(args.serve_alone, len(reqs))
     alone = serve(reqs[:k], 1, 0.0)
     alone["sample"] = f"the first {k} requests, submitted together, one in flight"
@@ -445,6 +449,7 @@ def form_serve(args, fb, torch):
                      "P-multigrid (lowOrder 0, 2 smoothing steps), run to a residual drop of 1e-8 "
                      f"(at most {args.serve_max_steps} steps), FP64, programmatic dependent launch"),
         "sweep": sweep,
+        "precision_served": precision,
         "one_at_a_time": alone,
         "speedup_solves_per_s": best / max(alone["solves_per_s"], 1e-30),
     }

@@ -159,6 +159,7 @@ def _load() -> ctypes.CDLL:
         "fr_server_cancel": (i, [P, ctypes.c_longlong]),
         "fr_server_stats": (i, [P, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(sz)]),
         "fr_server_destroy": (None, [P]),
+        "fr_server_set_precision": (i, [P, i]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -383,11 +384,15 @@ class Batch:
 class Server:
     """Continuous-batching solve server (fr_server_*)."""
 
-    def __init__(self, budget_bytes: int, max_inflight: int = 8, check_every: int = 10, device: int = 0):
+    def __init__(self, budget_bytes: int, max_inflight: int = 8, check_every: int = 10, device: int = 0,
+                 precision: int = FR_PREC_FP64):
         self._s = ctypes.c_void_p()
         st = lib.fr_server_create(int(budget_bytes), max_inflight, check_every, device, ctypes.byref(self._s))
         if st != FR_OK:
             raise FrError(st, "server create failed")
+        st = lib.fr_server_set_precision(self._s, int(precision))
+        if st != FR_OK:
+            raise FrError(st, "server precision")
         self._keep = {}
 
     def close(self):

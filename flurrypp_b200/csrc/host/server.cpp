@@ -64,6 +64,7 @@ struct fr_server {
   bool stop = false;
   size_t budget = 0, inflightBytes = 0;
   int maxInflight = 8, checkEvery = 10, device = 0;
+  int precision = FR_PREC_FP64;  // form of the cases admitted from now on
   long long nextId = 1;
   std::deque<long long> queue;
   std::map<long long, std::unique_ptr<Request>> reqs;
@@ -88,6 +89,7 @@ struct fr_server {
     fr_setup_opts o;
     fr_setup_opts_default(&o);
     o.device = device;
+    o.precision = precision;
     fr_case *c = nullptr;
     int st = r.hasMesh ? fr_create_with_mesh(r.deck.c_str(), &r.mesh, &o, &c)
                        : fr_create_from_deck(r.deck.c_str(), &o, &c);
@@ -224,6 +226,13 @@ int fr_server_create(size_t budget_bytes, int max_inflight, int check_every, int
   s->device = device;
   s->worker = std::thread([s] { s->loop(); });
   *out = s;
+  return FR_OK;
+}
+
+int fr_server_set_precision(fr_server *s, int precision) {
+  if (!s || (precision != FR_PREC_FP64 && precision != FR_PREC_MIXED)) return FR_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->precision = precision;
   return FR_OK;
 }
 

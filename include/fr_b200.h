@@ -257,6 +257,9 @@ void fr_batch_destroy(fr_batch *b);
  * waiting requests take its place.  No reference counterpart. */
 typedef struct fr_server fr_server;
 int fr_server_create(size_t budget_bytes, int max_inflight, int check_every, int device, fr_server **out);
+/* Form (FR_PREC_FP64 or FR_PREC_MIXED) of the requests the server admits
+ * from now on (default FP64).  No reference counterpart. */
+int fr_server_set_precision(fr_server *s, int precision);
 int fr_server_submit(fr_server *s, const char *deck, const fr_mesh *mesh, int ic_kind, const double *ic_prm,
                      int n_prm, double tol, int max_steps, long long *id);
 /* status: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled; latency from submission. */

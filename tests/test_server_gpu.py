@@ -88,3 +88,34 @@ def test_over_budget_request_fails_cleanly(tmp_path):
         srv.wait(r, 60)
     assert ei.value.code == fb.FR_ERR_BUDGET
     srv.close()
+
+
+def test_precision_form_served(tmp_path):
+    """The precision form (FP32 stages, P-multigrid included) through the
+    server: the same alone and in the mix, equal to the same number of
+    driver steps of a precision-form case, and within the precision form's
+    L2 bound of the FP64 served result."""
+    decks = [make_case(tmp_path, i, *sp) for i, sp in enumerate(SPECS)]
+    tol, max_steps = 1e-3, 80
+    alone = fb.Server(budget_bytes=8 << 30, max_inflight=1, check_every=10, precision=fb.FR_PREC_MIXED)
+    rid = alone.submit(decks[1], tol=tol, max_steps=max_steps)
+    alone.wait(rid, 300)
+    ua, pa = alone.result(rid, shape_of(decks[1])), alone.poll(rid)
+    alone.close()
+    mix = fb.Server(budget_bytes=8 << 30, max_inflight=4, check_every=10, precision=fb.FR_PREC_MIXED)
+    ids = [mix.submit(d, tol=tol, max_steps=max_steps) for d in decks]
+    for r in ids:
+        mix.wait(r, 300)
+    um, pm = mix.result(ids[1], shape_of(decks[1])), mix.poll(ids[1])
+    mix.close()
+    assert pa["steps"] == pm["steps"]
+    assert np.array_equal(ua, um)
+    s = fb.Solver(decks[1], precision=fb.FR_PREC_MIXED)
+    s.initialize_solution(fb.IC_DECK)
+    s.run(pa["steps"])
+    assert np.array_equal(s.get_state(), ua)
+    d = fb.Solver(decks[1])
+    d.initialize_solution(fb.IC_DECK)
+    d.run(pa["steps"])
+    ud = d.get_state()
+    assert np.linalg.norm(ua - ud) / np.linalg.norm(ud) < 1e-6
