@@ -42,10 +42,19 @@ struct Tm {
   // in elements of R; every tile starts on 128 bytes
   static constexpr int AL = 128 / (int)sizeof(R);
   static constexpr int al(int n) { return (n + AL - 1) / AL * AL; }
+  // FP64 3-D P3: the flux tile is padded by PADR values after each row of N
+  // points and PADP after each plane of N*N points.  Unpadded, the plane
+  // stride (16 points of EB*NF doubles) is a multiple of 128 bytes, so the
+  // lines that end on one face of a hex land 8 deep on the same two banks,
+  // and x-lines two deep; padded, every line pattern of the kernel is within
+  // one wavefront of conflict-free.  (FP32 tiles, measured, gain nothing.)
+  static constexpr bool PADDED = ND == 3 && P == 3 && !F32;
+  static constexpr int PADR = PADDED ? 4 : 0, PADP = PADDED ? 2 : 0;
+  static constexpr int padF() { return ND == 3 ? N * N * PADR + N * PADP : 0; }
   static constexpr size_t smem_for(int eb) {
     // U, U0, acc, comp tiles; Fn; J; det; F; tables; indices; barriers
     return sizeof(R) * (size_t)(4 * al(NS * eb * NF) + al(NFP * eb * NF) + al(ND * NS * eb * ND) + al(NS * eb) +
-                                al(ND * NS * eb * NF) + al(N * N + 4 * N) + al(NS * 2 * ND) +
+                                al(ND * (NS * eb * NF + padF())) + al(N * N + 4 * N) + al(NS * 2 * ND) +
                                 al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1) + AL) +
            128;
   }
@@ -68,6 +77,7 @@ struct Tm {
   static constexpr int EB = F32 ? shrink(eb32_want()) : shrink64(eb64());
   static constexpr int NT = NS * EB;
   static constexpr int ROW = EB * NF;
+  static constexpr int SLAB = NS * ROW + padF();  // one dimension's flux tile
   static constexpr int O_U = 0;
   static constexpr int O_U0 = O_U + al(NS * ROW);
   static constexpr int O_ACC = O_U0 + al(NS * ROW);
@@ -76,7 +86,7 @@ struct Tm {
   static constexpr int O_J = O_FN + al(NFP * ROW);
   static constexpr int O_DET = O_J + al(ND * NS * EB * ND);
   static constexpr int O_F = O_DET + al(NS * EB);
-  static constexpr int O_TAB = O_F + al(ND * NS * ROW);
+  static constexpr int O_TAB = O_F + al(ND * SLAB);
   static constexpr int O_CV = O_TAB + al(N * N + 4 * N);     // corrVal [NS][2ND]
   static constexpr int O_IDX = O_CV + al(NS * 2 * ND);        // ints: fpt line [NFP], corrFpt [NS][2ND]
   static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1);
@@ -132,6 +142,18 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
   using T = Tm<ND, P, R, V>;
   constexpr bool F32 = T::F32;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  // viscous stages load the gradient into the flux tile as one dense box, so
+  // they keep the flux tile unpadded; otherwise the new state is copied into
+  // the padded flux tile for the extrapolation (E)
+  constexpr bool PADDED = !VISC && T::PADDED;
+  constexpr int SL = VISC ? NS * ROW : T::SLAB;
+  // offset of point p of dimension d's flux tile
+  const auto fidx = [](int d, int p) {
+    if constexpr (PADDED)
+      return d * SL + p * ROW + (p / N) * T::PADR + (p / (N * N)) * T::PADP;
+    else
+      return (d * NS + p) * ROW;
+  };
   extern __shared__ __align__(128) unsigned char smem_bytes[];
   // tiles start on 128-byte boundaries relative to an aligned base
   R *smem = reinterpret_cast<R *>((reinterpret_cast<uintptr_t>(smem_bytes) + 127) & ~uintptr_t(127));
@@ -142,7 +164,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
   R *sFn = smem + T::O_FN;    // Fn -> Fn - extrapolated flux -> new U_fpts
   R *sJ = smem + T::O_J;      // [ND][NS][EB*ND]
   R *sDet = smem + T::O_DET;  // [NS][EB]
-  R *sF = smem + T::O_F;      // [ND][NS][ROW]
+  R *sF = smem + T::O_F;      // [ND][SL]: points at fo(p)
   R *sD = smem + T::O_TAB;
   R *sE = sD + N * N;
   R *sEF = sE + 2 * N;
@@ -260,7 +282,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
         fk[k] = f;
         if (a.F_dbg && valid) a.F_dbg[(((long long)d1 * NS + s) * E + e) * NF + k] = f;
       }
-      stp<NF, R>(&sF[(d1 * NS + s) * ROW + el * NF], fk);
+      stp<NF, R>(&sF[fidx(d1, s) + el * NF], fk);
     }
   }
   __syncthreads();
@@ -283,7 +305,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     for (int m = 0; m < N; m++) {
       const R dv = Dr[m];
       R x[NF];
-      ldp<NF, R>(&sF[(d * NS + base + m * stride) * ROW + el * NF], x);
+      ldp<NF, R>(&sF[fidx(d, base + m * stride) + el * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += dv * x[k];
     }
@@ -311,7 +333,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     for (int m = 0; m < N; m++) {
       const R ev = sEF[side * N + m];
       R x[NF];
-      ldp<NF, R>(&sF[(dn * NS + base + m * stride) * ROW + fe * NF], x);
+      ldp<NF, R>(&sF[fidx(dn, base + m * stride) + fe * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
     }
@@ -397,6 +419,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     }
     if (a.mode != MODE_RESIDUAL) {
       stp<NF, R>(&sU[l0], vU);
+      if (PADDED) stp<NF, R>(&sF[fidx(0, s) + el * NF], vU);  // the flux tile is dead after C2
       if (a.mode == MODE_RK_STAGE) stp<NF, R>(&sAcc[l0], vAcc);
       if (needCmp) stp<NF, R>(&sCmp[l0], vCmp);
     }
@@ -428,7 +451,10 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V>::NT) k_elem_tma(ElemArgsT<R> a
     for (int m = 0; m < N; m++) {
       const R ev = sE[side * N + m];
       R x[NF];
-      ldp<NF, R>(&sU[(base + m * stride) * ROW + fe * NF], x);
+      if (PADDED)
+        ldp<NF, R>(&sF[fidx(0, base + m * stride) + fe * NF], x);
+      else
+        ldp<NF, R>(&sU[(base + m * stride) * ROW + fe * NF], x);
 #pragma unroll
       for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
     }
