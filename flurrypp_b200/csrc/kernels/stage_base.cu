@@ -112,6 +112,62 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
   face_interior<ND, R>(i, slotL, slotR, nrm, dAL, dAR, Uf, Fn, waveSp, gam, roe);
 }
 
+// PPT face points per thread (points i and i + grid size), all gathers
+// issued before any flux is formed: the gather is latency-bound, and two
+// points per thread at 128 threads per CTA keep a third more loads in flight
+// per SM than one point per thread at the register-limited occupancy
+// (measured: 3-D FP64 faces 0.090 -> 0.083 ms, FP32 0.054 -> 0.050 ms).
+constexpr int kFacePpt = 2, kFaceNt = 128;
+
+template <int ND, typename R, int PPT>
+__global__ void __launch_bounds__(kFaceNt) k_faces_interior_ilp(int n, const int *__restrict__ slotL,
+                                                           const int *__restrict__ slotR, const R *__restrict__ nrm,
+                                                           const R *__restrict__ dAL, const R *__restrict__ dAR,
+                                                           const R *__restrict__ Uf, R *__restrict__ Fn,
+                                                           double *__restrict__ waveSp, R gam, int roe) {
+  pdl_wait();
+  pdl_trigger();
+  constexpr int NF = ND + 2;
+  const int stride = gridDim.x * blockDim.x;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  int ii[PPT], sL[PPT], sR[PPT];
+#pragma unroll
+  for (int q = 0; q < PPT; q++) {
+    ii[q] = min(i0 + q * stride, n - 1);
+    sL[q] = slotL[ii[q]];
+    sR[q] = slotR[ii[q]];
+  }
+  R UL[PPT][NF], UR[PPT][NF], nv[PPT][ND], aL[PPT], aR[PPT];
+#pragma unroll
+  for (int q = 0; q < PPT; q++) {
+#pragma unroll
+#pragma unroll
+    for (int k = 0; k < NF; k++) UL[q][k] = Uf[(long long)sL[q] * NF + k];
+#pragma unroll
+    for (int k = 0; k < NF; k++) UR[q][k] = Uf[(long long)sR[q] * NF + k];
+#pragma unroll
+    for (int d = 0; d < ND; d++) nv[q][d] = nrm[(long long)ii[q] * ND + d];
+    aL[q] = dAL[ii[q]];
+    aR[q] = dAR[ii[q]];
+  }
+#pragma unroll
+  for (int q = 0; q < PPT; q++) {
+    if (i0 + q * stride >= n) break;
+    R F[NF];
+    if (ND == 2 && roe) {
+      roe2d<R>(UL[q], UR[q], nv[q], gam, F);
+    } else {
+      const R ws = rusanov<ND, R>(UL[q], UR[q], nv[q], gam, F);
+      if (waveSp) waveSp[sL[q]] = ws;
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      Fn[(long long)sL[q] * NF + k] = F[k] * aL[q];
+      Fn[(long long)sR[q] * NF + k] = -F[k] * aR[q];
+    }
+  }
+}
+
 template <int ND, typename R>
 __global__ void k_faces_boundary(int n0, int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
                                  const R *__restrict__ nrm, const R *__restrict__ dAL, const R *__restrict__ Uf,
@@ -517,7 +573,17 @@ void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R
                waveSp, ph);
     return;
   }
-  if (nI > 0) {
+  // two points per thread except 2-D FP32, where one measured faster
+  if (nI > 0 && (nDims == 3 || sizeof(R) == 8)) {
+    const int per = kFaceNt * kFacePpt;
+    const int g = (nI + per - 1) / per;
+    if (nDims == 2)
+      launch_k(k_faces_interior_ilp<2, R, kFacePpt>, g, kFaceNt, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL,
+               ft.dAR, Ufpts, Fn, waveSp, R(ph.gamma), ph.riemannType == 1);
+    else
+      launch_k(k_faces_interior_ilp<3, R, kFacePpt>, g, kFaceNt, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL,
+               ft.dAR, Ufpts, Fn, waveSp, R(ph.gamma), 0);
+  } else if (nI > 0) {
     const int g = (nI + b - 1) / b;
     if (nDims == 2)
       launch_k(k_faces_interior<2, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
