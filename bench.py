@@ -663,11 +663,44 @@ def main():
     ms_e2e = e0.elapsed_time(e1)
     del flight[1:]
 
-    ms, ms_e2e = max_over_ranks([ms, ms_e2e], "cuda")
+    # the same copies alone (a state in on one stream, a state out on
+    # another, as in the end-to-end loop): the end-to-end rate if the RK
+    # step itself took no time, i.e. the PCIe bound of that number
+    hin = torch.empty(s.shape, dtype=torch.float64, pin_memory=True)
+    hout = torch.empty(s.shape, dtype=torch.float64, pin_memory=True)
+    din = torch.empty(s.shape, dtype=torch.float64, device=f"cuda:{local}")
+    dout = torch.empty_like(din)
+    cin, cout = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def copies(n):
+        for _ in range(n):
+            with torch.cuda.stream(cin):
+                din.copy_(hin, non_blocking=True)
+            with torch.cuda.stream(cout):
+                hout.copy_(dout, non_blocking=True)
+
+    copies(2)
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    cin.wait_event(c0)
+    cout.wait_event(c0)
+    copies(args.e2e_steps)
+    for cs in (cin, cout):
+        ev = torch.cuda.Event()
+        ev.record(cs)
+        stream.wait_event(ev)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    ms_copy = c0.elapsed_time(c1)
+    del hin, hout, din, dout
+
+    ms, ms_e2e, ms_copy = max_over_ranks([ms, ms_e2e, ms_copy], "cuda")
 
     if rank == 0:
         value = whole_job_rate(world, dof, nrk, args.steps, ms)
         e2e = whole_job_rate(world, dof, nrk, args.e2e_steps, ms_e2e)
+        e2e_copy_bound = whole_job_rate(world, dof, nrk, args.e2e_steps, ms_copy)
         peak, peak_kind = measured_peak_hbm()
         # algorithmic bytes per launch of the element kernel (intermediate RK
         # stage, FP64): per element read U, U0, acc, Fn (nFpts*nF), JGinv
@@ -689,7 +722,8 @@ def main():
                        "dt": dt, "l2_flush": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8,
-                    "cases_in_flight": E2E_CASES, "steps": args.e2e_steps},
+                    "cases_in_flight": E2E_CASES, "steps": args.e2e_steps,
+                    "copy_bound": e2e_copy_bound, "frac_of_copy_bound": e2e / e2e_copy_bound},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": profiled_traffic("traffic_bytes_per_launch"),
