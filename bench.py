@@ -41,6 +41,10 @@ from __future__ import annotations
 import argparse
 import json
 import os
+
+# 32 hardware work queues (CUDA's default is 8) before any CUDA context, for
+# the many-stream serving and end-to-end forms; the package sets the same
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 import statistics
 import subprocess
 import sys

@@ -15,6 +15,13 @@ from __future__ import annotations
 import ctypes
 import os
 
+# Hardware work queues per process: CUDA's default of 8 makes streams beyond
+# the eighth share queues, which serialises the per-request streams of the
+# server (measured: 16 channel solves in flight, 0.63 -> 0.69 solves/s FP64,
+# 0.66 -> 0.93 in the precision form).  Takes effect only if set before the
+# process creates its CUDA context; a value the caller set is kept.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
