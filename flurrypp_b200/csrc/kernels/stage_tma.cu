@@ -94,9 +94,13 @@ struct Tm {
   static constexpr int O_J = O_DET + al(NS * EB);
   static constexpr int O_F = LEAN ? O_J : O_J + al(ND * NS * EB * ND);
   static constexpr int O_TAB = O_F + (al(ND * SLAB) > al(ND * NS * EB * ND) ? al(ND * SLAB) : al(ND * NS * EB * ND));
-  static constexpr int O_CV = O_TAB + al(N * N + 4 * N);     // corrVal [NS][2ND]
-  static constexpr int O_IDX = O_CV + al(NS * 2 * ND);        // ints: fpt line [NFP], corrFpt [NS][2ND]
-  static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1);
+  // correction tables (corrVal [NS][2ND], corrFpt [NS][2ND]) in shared
+  // memory, except in the lean tile set, which reads them through L1 from
+  // global memory (4.6 KB per CTA at 3-D P3, one more CTA per SM)
+  static constexpr int NCT = LEAN ? 0 : NS * 2 * ND;
+  static constexpr int O_CV = O_TAB + al(N * N + 4 * N);
+  static constexpr int O_IDX = O_CV + al(NCT);                // ints: fpt line [NFP], corrFpt
+  static constexpr int O_BAR = O_IDX + al((int)((NFP + NCT) * 4 / sizeof(R)) + 1);
   static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
   static_assert(SMEM <= kMaxSmem, "TMA tile set does not fit in shared memory");
   static_assert(NT <= 1024, "too many threads");
@@ -234,10 +238,11 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     sEF[i] = t.EFn1[i];
   }
   for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
-  for (int i = tid; i < NS * 2 * ND; i += NT) {
-    sCF[i] = t.corrFpt[i];
-    sCV[i] = t.corrVal[i];
-  }
+  if constexpr (!LEAN)
+    for (int i = tid; i < NS * 2 * ND; i += NT) {
+      sCF[i] = t.corrFpt[i];
+      sCV[i] = t.corrVal[i];
+    }
   if (!mbar_wait_bounded(&bar[0], 0, 1u << 22)) {
     // give up: flag it, let the copies in flight land (bounded), leave
     if (a.err) atomicOr(a.err, 1);
@@ -394,8 +399,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     for (int k = 0; k < NF; k++) cq[k] = R(0);
 #pragma unroll
     for (int fc = 0; fc < 2 * ND; fc++) {
-      const int fp = sCF[s * 2 * ND + fc];
-      const R cv = sCV[s * 2 * ND + fc];
+      const int fp = LEAN ? __ldg(&t.corrFpt[s * 2 * ND + fc]) : sCF[s * 2 * ND + fc];
+      const R cv = LEAN ? __ldg(&t.corrVal[s * 2 * ND + fc]) : sCV[s * 2 * ND + fc];
       R x[NF];
       ldp<NF, R>(&sFn[fp * ROW + el * NF], x);
 #pragma unroll
