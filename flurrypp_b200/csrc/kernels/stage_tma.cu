@@ -94,10 +94,11 @@ struct Tm {
   static constexpr int O_J = O_DET + al(NS * EB);
   static constexpr int O_F = LEAN ? O_J : O_J + al(ND * NS * EB * ND);
   static constexpr int O_TAB = O_F + (al(ND * SLAB) > al(ND * NS * EB * ND) ? al(ND * SLAB) : al(ND * NS * EB * ND));
-  // correction tables (corrVal [NS][2ND], corrFpt [NS][2ND]) in shared
-  // memory, except in the lean tile set, which reads them through L1 from
-  // global memory (4.6 KB per CTA at 3-D P3, one more CTA per SM)
-  static constexpr int NCT = LEAN ? 0 : NS * 2 * ND;
+  // correction tables (corrVal [NS][2ND], corrFpt [NS][2ND]): inviscid
+  // stages read them through L1 from global memory instead of staging them
+  // (4.6 KB per FP64 CTA at 3-D P3, one more CTA per SM)
+  static constexpr bool GTAB = !VS;
+  static constexpr int NCT = GTAB ? 0 : NS * 2 * ND;
   static constexpr int O_CV = O_TAB + al(N * N + 4 * N);
   static constexpr int O_IDX = O_CV + al(NCT);                // ints: fpt line [NFP], corrFpt
   static constexpr int O_BAR = O_IDX + al((int)((NFP + NCT) * 4 / sizeof(R)) + 1);
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     sEF[i] = t.EFn1[i];
   }
   for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
-  if constexpr (!LEAN)
+  if constexpr (!T::GTAB)
     for (int i = tid; i < NS * 2 * ND; i += NT) {
       sCF[i] = t.corrFpt[i];
       sCV[i] = t.corrVal[i];
@@ -399,8 +400,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     for (int k = 0; k < NF; k++) cq[k] = R(0);
 #pragma unroll
     for (int fc = 0; fc < 2 * ND; fc++) {
-      const int fp = LEAN ? __ldg(&t.corrFpt[s * 2 * ND + fc]) : sCF[s * 2 * ND + fc];
-      const R cv = LEAN ? __ldg(&t.corrVal[s * 2 * ND + fc]) : sCV[s * 2 * ND + fc];
+      const int fp = T::GTAB ? __ldg(&t.corrFpt[s * 2 * ND + fc]) : sCF[s * 2 * ND + fc];
+      const R cv = T::GTAB ? __ldg(&t.corrVal[s * 2 * ND + fc]) : sCV[s * 2 * ND + fc];
       R x[NF];
       ldp<NF, R>(&sFn[fp * ROW + el * NF], x);
 #pragma unroll
