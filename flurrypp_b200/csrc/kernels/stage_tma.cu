@@ -528,6 +528,14 @@ void launch_tma(const ElemArgsT<R> &a, const TpTablesT<R> &t, const TmaMaps &m, 
   launch_k(k_elem_tma<ND, P, R, V, VISC>, g, T::NT, T::SMEM, st, a, t, m);
 }
 
+// The CTAs per SM the tile layouts are built for at 3-D P3 (228 KB of shared
+// memory per SM, 1 KB of it reserved per CTA): the lean FP64 set, six
+// 2-element or three 4-element CTAs; FP32 4-element tiles, four.
+constexpr bool ctas_fit(size_t smem, int ctas) { return (smem + 1024) * ctas <= 228 * 1024; }
+static_assert(ctas_fit(Tm<3, 3, double, 0>::SMEM, 6) && Tm<3, 3, double, 0>::EB == 2, "FP64 P3 2-element tiles");
+static_assert(ctas_fit(Tm<3, 3, double, 1>::SMEM, 3) && Tm<3, 3, double, 1>::EB == 4, "FP64 P3 4-element tiles");
+static_assert(ctas_fit(Tm<3, 3, float, 0>::SMEM, 4) && Tm<3, 3, float, 0>::EB == 4, "FP32 P3 4-element tiles");
+
 // (nDims, order) -> compile-time case; variants only for the precision form
 #define FR_TM_ORDERS(X) X(2, 0) X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 5) X(3, 0) X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 5)
 
