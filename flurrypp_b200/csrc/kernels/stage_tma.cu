@@ -38,8 +38,10 @@ struct Tm {
   // from global memory at each thread's own point (it is read once, so a
   // tile buys nothing) and the flux tile is laid over the metric tile, which
   // every thread copies to registers first.  At 3-D P3 this takes a 2-element
-  // CTA from 54.8 to 40.8 KB, five CTAs per SM instead of four.  Viscous
-  // stages load the gradient into the flux tile together with the metrics.
+  // CTA from 54.8 to 40.8 KB (36.3 KB with the correction tables below: six
+  // CTAs per SM instead of four).  Viscous stages load the gradient into the
+  // flux tile together with the metrics.  (smem_for, which only sizes EB,
+  // counts the full set.)
   static constexpr bool LEAN = !F32 && !VS;
   static constexpr int N = P + 1;
   static constexpr int NF = ND + 2;
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
   R *sFn = smem + T::O_FN;    // Fn -> Fn - extrapolated flux -> new U_fpts
   R *sJ = smem + T::O_J;      // [ND][NS][EB*ND]
   R *sDet = smem + T::O_DET;  // [NS][EB]
-  R *sF = smem + T::O_F;      // [ND][SL]: points at fo(p)
+  R *sF = smem + T::O_F;      // [ND][SL]: point p of dimension d at fidx(d, p)
   R *sD = smem + T::O_TAB;
   R *sE = sD + N * N;
   R *sEF = sE + 2 * N;
