@@ -222,8 +222,6 @@ def test_programmatic_launch_overlap_changes_nothing(case, precision):
     steps with plain stream order give bit-identical states, in the
     graph-replayed and the step-by-step loop."""
     a, meta = load_golden(case)
-    if precision == fb.FR_PREC_MIXED and has_pmg(meta):
-        pytest.skip("P-multigrid runs in the plain form only")
     outs = []
     for no_pdl in (0, 1):
         for graph in (True, False):
