@@ -733,6 +733,7 @@ def main():
                          "traffic": profiled_traffic("traffic_bytes_per_launch"),
                          "traffic_source": "profiles/fp64_stage_tgv32_p3.md (ncu, one launch)",
                          "kernel": "k_elem_tma<3, 3>" if inf.tensor_kernels == 2 else "k_elem_tp<3, 3>",
+                         "tile_variant": inf.tile_variant, "elems_per_block": inf.elems_per_block,
                          "kernel_ms": kt["element_stage"], "algorithmic_bytes": elem_bytes,
                          "peak_source": peak_kind},
             "kernels_ms": {"element_stage": kt["element_stage"], "faces": kt["faces"],
