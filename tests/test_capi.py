@@ -45,3 +45,22 @@ def test_server_reports_setup_failure_without_gpu_work(tmp_path):
     assert ei.value.code == fb.FR_ERR_ARG
     assert srv.poll(r)["status"] == 3
     srv.close()
+
+
+def test_hardware_work_queues_default_and_caller_value_kept():
+    """Importing the package asks for 32 CUDA hardware work queues unless the
+    caller chose a value (checked in fresh interpreters, before any CUDA
+    context)."""
+    import subprocess
+    import sys
+
+    code = "import os, flurrypp_b200; print(os.environ['CUDA_DEVICE_MAX_CONNECTIONS'])"
+    env = {k: v for k, v in os.environ.items() if k != "CUDA_DEVICE_MAX_CONNECTIONS"}
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "32"
+    env["CUDA_DEVICE_MAX_CONNECTIONS"] = "4"
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.stdout.strip() == "4"
