@@ -147,6 +147,8 @@ def _load() -> ctypes.CDLL:
         "fr_integrate_error": (i, [P, i, dp, i]),
         "fr_wall_force": (i, [P, dp]),
         "fr_mass_flux": (i, [P, i, dp, i]),
+        "fr_shard_plan": (i, [P, i, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong),
+                              ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong]),
         "fr_write_data": (i, [P, ctypes.c_char_p]),
         "fr_read_restart": (i, [P, ctypes.c_char_p]),
         "fr_bench_kernel": (i, [P, ctypes.c_char_p, i]),
@@ -290,6 +292,24 @@ class Solver:
         out = np.zeros(self.nFields)
         self._check(lib.fr_mass_flux(self._c, int(error_norm), _dptr(out), self.nFields))
         return out
+
+    def shard_plan(self, nparts: int, rank: int):
+        """Sharding plan for part `rank` of `nparts` (host only; see
+        fr_shard_plan): (part of every element, owned element count, halo
+        peers, halo slots), the halo in the order both sides of a cut share."""
+        part = np.zeros(self.nEles, dtype=np.int32)
+        n_owned, n_halo = ctypes.c_int(0), ctypes.c_longlong(0)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lp = ctypes.POINTER(ctypes.c_longlong)
+        self._check(lib.fr_shard_plan(self._c, int(nparts), int(rank), part.ctypes.data_as(ip),
+                                      ctypes.byref(n_owned), ctypes.byref(n_halo), None, None, 0))
+        peer = np.zeros(n_halo.value, dtype=np.int32)
+        slot = np.zeros(n_halo.value, dtype=np.int64)
+        if n_halo.value:
+            self._check(lib.fr_shard_plan(self._c, int(nparts), int(rank), None, ctypes.byref(n_owned),
+                                          ctypes.byref(n_halo), peer.ctypes.data_as(ip), slot.ctypes.data_as(lp),
+                                          n_halo.value))
+        return part, n_owned.value, peer, slot
 
     def checkpoint(self):
         """Snapshot for output; the copy to the host overlaps later steps."""

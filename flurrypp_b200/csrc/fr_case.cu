@@ -2599,6 +2599,33 @@ int fr_mass_flux(fr_case *c, int errorNorm, double *out, int nFields) {
   return FR_OK;
 }
 
+int fr_shard_plan(fr_case *c, int nparts, int rank, int *part, int *n_owned, long long *n_halo, int *halo_peer,
+                  long long *halo_slot, long long cap) {
+  if (!c || !n_owned || !n_halo || nparts < 1 || rank < 0 || rank >= nparts || cap < 0) return FR_ERR_ARG;
+  if (cap > 0 && (!halo_peer || !halo_slot)) return FR_ERR_ARG;
+  if (c->in.motion != 0) {
+    c->err = "sharding plan: moving meshes are not partitioned";
+    return FR_ERR_UNSUPPORTED;
+  }
+  std::vector<int> pt, owned, peer;
+  std::vector<long long> slot;
+  if (!fr::partition_elements(c->mesh, nparts, pt, c->err) ||
+      !fr::halo_plan(c->mesh, c->faces, c->nPF, pt, rank, owned, peer, slot, c->err))
+    return FR_ERR_ARG;
+  if (part) std::copy(pt.begin(), pt.end(), part);
+  *n_owned = (int)owned.size();
+  *n_halo = (long long)slot.size();
+  if (cap > 0) {
+    if (cap < (long long)slot.size()) {
+      c->err = "sharding plan: halo buffers smaller than the halo";
+      return FR_ERR_ARG;
+    }
+    std::copy(peer.begin(), peer.end(), halo_peer);
+    std::copy(slot.begin(), slot.end(), halo_slot);
+  }
+  return FR_OK;
+}
+
 int fr_synchronize(fr_case *c) {
   if (!c) return FR_ERR_ARG;
   if (c->hostOnly) {

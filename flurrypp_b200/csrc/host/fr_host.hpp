@@ -205,6 +205,16 @@ struct Geometry {
   std::vector<double> detJac_fpts;  // [nFpts][nEles]
 };
 bool build_geometry(const Mesh &m, int order, int ptsType, Geometry &g, std::string &err);
+
+// Partition of the elements into nparts by recursive coordinate bisection
+// of their centroids (the reference uses METIS, src/geo.cpp:2380-2470), and
+// the halo of one part: its elements (ascending global ids; local id = index
+// here) and every point of a face cut by the partition as (peer part, slot
+// fpt*nOwned + local element), ordered by face and point so that both sides
+// of a cut list the same points in the same order (src/mpiFace.cpp:122-175).
+bool partition_elements(const Mesh &m, int nparts, std::vector<int> &part, std::string &err);
+bool halo_plan(const Mesh &m, const std::vector<Face> &faces, int nPF, const std::vector<int> &part, int rank,
+               std::vector<int> &owned, std::vector<int> &peer, std::vector<long long> &slot, std::string &err);
 // True when nNodes names a quad (nDims 2) or hex (nDims 3) shape above.
 bool shape_supported(int nDims, int nNodes);
 // Shape functions N [nPts][nNodes] and their reference-space derivatives

@@ -215,6 +215,22 @@ int fr_integrate_error(fr_case *c, int errorNorm, double *out, int nFields);
 int fr_wall_force(fr_case *c, double *out);
 int fr_mass_flux(fr_case *c, int errorNorm, double *out, int nFields);
 
+/* Sharding plan for running the case on nparts GPUs (host only; works on a
+ * case created without a device).  The elements are split by recursive
+ * coordinate bisection of their centroids, where the reference uses METIS
+ * (geo::partitionMesh, src/geo.cpp:2380-2470).  For part `rank`: part[nEles]
+ * (may be NULL) receives every element's part, *n_owned its element count
+ * (local element ids follow ascending global ids), and *n_halo the number of
+ * points on faces cut by the partition that it shares with other parts; with
+ * cap >= *n_halo, halo_peer[k] and halo_slot[k] receive each point's peer
+ * part and its slot fpt * n_owned + local element.  Both sides of a cut list
+ * their shared points in the same order (by face, then by point in the
+ * face's left order), so traces packed in list order are what the peer
+ * expects, as mpiFace::communicate / getRightState exchange them
+ * (src/mpiFace.cpp:122-175). */
+int fr_shard_plan(fr_case *c, int nparts, int rank, int *part, int *n_owned, long long *n_halo, int *halo_peer,
+                  long long *halo_slot, long long cap);
+
 int fr_checkpoint(fr_case *c);
 int fr_write_data(fr_case *c, const char *path);
 int fr_read_restart(fr_case *c, const char *path);
