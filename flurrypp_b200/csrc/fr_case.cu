@@ -11,9 +11,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -28,9 +31,32 @@ namespace {
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
+  bool fp32 = false;
 };
 
+// FP32 device arrays of the live cases, begin -> end address: the
+// no-allocation norm takes raw FP64 pointers and refuses these
+std::mutex g_fp32Mu;
+std::map<uintptr_t, uintptr_t> g_fp32Arrays;
+
+void note_fp32(void *p, size_t bytes, bool add) {
+  std::lock_guard<std::mutex> lk(g_fp32Mu);
+  if (add)
+    g_fp32Arrays[(uintptr_t)p] = (uintptr_t)p + bytes;
+  else
+    g_fp32Arrays.erase((uintptr_t)p);
+}
+
 }  // namespace
+
+bool fr_internal_is_fp32(const void *p) {
+  const uintptr_t a = (uintptr_t)p;
+  std::lock_guard<std::mutex> lk(g_fp32Mu);
+  auto it = g_fp32Arrays.upper_bound(a);
+  if (it == g_fp32Arrays.begin()) return false;
+  --it;
+  return a >= it->first && a < it->second;
+}
 
 // cases with fewer solution points than this do not time tile variants
 constexpr long long kTuneMinPoints = 1LL << 18;
@@ -180,7 +206,10 @@ struct fr_case {
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
     levels.clear();  // coarse levels use this case's stream: release them first
-    for (auto &b : allocs) cudaFree(b.p);
+    for (auto &b : allocs) {
+      if (b.fp32) note_fp32(b.p, b.bytes, false);
+      cudaFree(b.p);
+    }
     if (ownStream && ownedStream) cudaStreamDestroy(ownedStream);
   }
   cudaStream_t ownedStream = nullptr;
@@ -202,7 +231,9 @@ struct fr_case {
       return false;
     }
     cudaMemsetAsync(q, 0, bytes, stream);
-    allocs.push_back({q, bytes});
+    const bool fp32 = std::is_same<T, float>::value;
+    if (fp32) note_fp32(q, bytes, true);
+    allocs.push_back({q, bytes, fp32});
     p = (T *)q;
     return true;
   }

@@ -139,7 +139,7 @@ __device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R ga
   R hR = (UR[nDims + 1] + pR) / UR[0];
   R sq_rho = sqrt(UR[0] / UL[0]);
   R rrho = R(1.) / (sq_rho + R(1.));
-  R usq = R(0.), unm = R(0.), vgn = R(0.);
+  R usq = R(0.), unm = R(0.);
   for (int i = 0; i < nDims; i++) {
     um[i] = rrho * (vL[i] + sq_rho * vR[i]);
     usq += R(0.5) * um[i] * um[i];
@@ -158,9 +158,9 @@ __device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R ga
   Fn[2] = rhoUnL * vL[1] + rhoUnR * vR[1] + (pL + pR) * n[1];
   Fn[3] = rhoUnL * hL + rhoUnR * hR;
   for (int i = 0; i < 4; i++) du[i] = UR[i] - UL[i];
-  R lambda0 = fabs(unm - vgn);
-  R lambdaP = fabs(unm - vgn + am);
-  R lambdaM = fabs(unm - vgn - am);
+  R lambda0 = fabs(unm);
+  R lambdaP = fabs(unm + am);
+  R lambdaM = fabs(unm - am);
   R eps = R(0.5) * (fabs(rhoUnL / UL[0] - rhoUnR / UR[0]) +
                     fabs(sqrt(gamma * pL / UL[0]) - sqrt(gamma * pR / UR[0])));
   if (lambda0 < R(2.) * eps) lambda0 = R(0.25) * lambda0 * lambda0 / eps + eps;
@@ -214,9 +214,7 @@ __device__ __forceinline__ void boundary_state(int bc, const R *UL, const R *n, 
     ER = (pR / (gamma - R(1.0))) + R(0.5) * rhoR * vSq;
   } else if (bc == BC_SUP_IN) {
     rhoR = R(ph.rhoBound);
-    vR[0] = R(ph.uBound);
-    vR[1] = R(ph.vBound);
-    vR[2] = R(ph.wBound);
+    for (int i = 0; i < ND; i++) vR[i] = vBound[i];
     pR = R(ph.pBound);
     vSq = R(0.);
     for (int i = 0; i < ND; i++) vSq += (vR[i] * vR[i]);

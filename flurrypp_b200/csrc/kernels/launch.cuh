@@ -21,6 +21,10 @@ namespace frk {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Maximum that keeps a NaN of either operand (fmax returns the other one), so
+// a blown-up residual reaches the host's NaN check through a max-norm.
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || a > b) ? a : b; }
+
 // Launch policy of the calling host thread (set by the case around its
 // launch sequences, graph captures included).
 void set_pdl(bool on);

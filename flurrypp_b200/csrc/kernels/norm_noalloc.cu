@@ -13,19 +13,33 @@
 //
 // Usage rules:
 //   - The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress) with that device current and keeps it for the
+//     life of the process.  A cudaDeviceReset of that device reloads the
+//     module and leaves the kept address stale, so the function must not be
+//     called on a device after a cudaDeviceReset of it.
+//   - No call may be made while its stream is being captured into a CUDA
+//     graph: every call copies the weights from host memory and synchronises
+//     the stream before it returns.
 //   - Every call uses the same array.  Calls that overlap on the GPU (on
 //     different streams, or from different host threads) race on it; issue
 //     them one after another.
 //   - Each call writes every partial it later reads, so nothing has to be
 //     cleared between calls.
+//   - divF and detJ must be FP64 arrays.  The precision form's working
+//     arrays (which fr_device_ptr returns for a case created with
+//     FR_PREC_MIXED) are FP32; the library knows every FP32 array it
+//     allocated and refuses them with FR_ERR_ARG.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <mutex>
 
 #include "../../../include/fr_b200.h"
+#include "launch.cuh"
+
+// true when p lies inside an FP32 device array allocated by a live case of
+// this library (fr_case.cu)
+bool fr_internal_is_fp32(const void *p);
 
 namespace {
 
@@ -60,10 +74,10 @@ __global__ void __launch_bounds__(kThreads) k_norm_partial(const double *__restr
           r += fabs(d) * w[s];
         else if (resType == 2)
           r += d * d / detJ[(long long)s * E + e] * w[s];
-        else
-          r = fmax(fabs(d) / detJ[(long long)s * E + e], r);
+        else  // NaN-keeping maximum: a blown-up residual must reach the host check
+          r = frk::nan_max(fabs(d) / detJ[(long long)s * E + e], r);
       }
-      acc[k] = resType == 3 ? fmax(acc[k], r) : acc[k] + r;
+      acc[k] = resType == 3 ? frk::nan_max(r, acc[k]) : acc[k] + r;
     }
   }
   for (int k = 0; k < nF; k++) sh[threadIdx.x][k] = acc[k];
@@ -71,7 +85,7 @@ __global__ void __launch_bounds__(kThreads) k_norm_partial(const double *__restr
   for (int half = kThreads / 2; half > 0; half >>= 1) {
     if ((int)threadIdx.x < half)
       for (int k = 0; k < nF; k++)
-        sh[threadIdx.x][k] = resType == 3 ? fmax(sh[threadIdx.x][k], sh[threadIdx.x + half][k])
+        sh[threadIdx.x][k] = resType == 3 ? frk::nan_max(sh[threadIdx.x + half][k], sh[threadIdx.x][k])
                                           : sh[threadIdx.x][k] + sh[threadIdx.x + half][k];
     __syncthreads();
   }
@@ -85,7 +99,7 @@ __global__ void k_norm_final(int nBlocks, int nF, int resType, double *__restric
   double r = 0;
   for (int b = 0; b < nBlocks; b++) {
     const double v = scratch[b * kMaxFields + k];
-    r = resType == 3 ? fmax(r, v) : r + v;
+    r = resType == 3 ? frk::nan_max(v, r) : r + v;
   }
   scratch[kBlocks * kMaxFields + k] = resType == 2 ? sqrt(r) : r;
 }
@@ -121,6 +135,8 @@ extern "C" int fr_residual_norm_noalloc(const double *divF, const double *detJ, 
   if (!divF || !detJ || !out || (nDims != 2 && nDims != 3) || order < 0 || order > 5 || nFields != nDims + 2 ||
       resType < 1 || resType > 3 || nEles < 1 || nEles > FR_NOALLOC_MAX_ELES)
     return FR_ERR_ARG;
+  // FP32 working arrays of a precision-form case would be read as doubles
+  if (fr_internal_is_fp32(divF) || fr_internal_is_fp32(detJ)) return FR_ERR_ARG;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FR_ERR_CUDA;
   double *scratch;
@@ -148,10 +164,23 @@ extern "C" int fr_residual_norm_noalloc(const double *divF, const double *detJ, 
                       st) != cudaSuccess)
     return FR_ERR_CUDA;
   long long want = ((long long)nEles + kThreads - 1) / kThreads;
-  const int blocks = (int)(want < kBlocks ? want : kBlocks);
-  k_norm_partial<<<blocks, kThreads, 0, st>>>(divF, detJ, nS, (long long)nEles, nFields, resType, scratch);
-  k_norm_final<<<1, 32, 0, st>>>(blocks, nFields, resType, scratch);
-  if (cudaGetLastError() != cudaSuccess) return FR_ERR_CUDA;
+  int blocks = (int)(want < kBlocks ? want : kBlocks);
+  // launch results are taken from the launch calls themselves, so an error
+  // the caller left pending before this call is neither reported as this
+  // call's nor cleared
+  const cudaError_t pending = cudaPeekAtLastError();
+  long long nE = nEles;
+  int nSl = nS, nFl = nFields, rt = resType;
+  void *a1[] = {(void *)&divF, (void *)&detJ, &nSl, &nE, &nFl, &rt, &scratch};
+  cudaError_t le = cudaLaunchKernel((const void *)k_norm_partial, dim3(blocks), dim3(kThreads), a1, 0, st);
+  if (le == cudaSuccess) {
+    void *a2[] = {&blocks, &nFl, &rt, &scratch};
+    le = cudaLaunchKernel((const void *)k_norm_final, dim3(1), dim3(32), a2, 0, st);
+  }
+  if (le != cudaSuccess) {
+    if (pending == cudaSuccess) cudaGetLastError();  // clear only this call's launch error
+    return FR_ERR_CUDA;
+  }
   if (cudaMemcpyAsync(out, scratch + kBlocks * kMaxFields, nFields * sizeof(double), cudaMemcpyDeviceToHost, st) !=
           cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)

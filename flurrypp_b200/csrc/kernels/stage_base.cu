@@ -466,8 +466,8 @@ __global__ void k_residual_norm(int nS, int E, int nF, const R *__restrict__ div
         r += fabs(d) * w[s];
       else if (resType == 2)
         r += d * d / detJ[(long long)s * E + e] * w[s];
-      else
-        r = fmax(fabs(d) / detJ[(long long)s * E + e], r);
+      else  // a NaN anywhere makes the maximum NaN (fmax would drop it)
+        r = nan_max(fabs(d) / detJ[(long long)s * E + e], r);
     }
     eleRes[(long long)e * nF + k] = r;
   }

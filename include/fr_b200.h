@@ -236,7 +236,9 @@ int fr_write_data(fr_case *c, const char *path);
 int fr_read_restart(fr_case *c, const char *path);
 
 /* Device pointer of a state array ("U_spts", "U_fpts", "divF_0", ...) for
- * callers that keep data resident (no copy).  Valid until fr_destroy. */
+ * callers that keep data resident (no copy).  Valid until fr_destroy.  For a
+ * case created with FR_PREC_MIXED these are the precision form's FP32 working
+ * arrays (4 bytes per value; *bytes says so), not FP64. */
 int fr_device_ptr(fr_case *c, const char *name, void **ptr, size_t *bytes);
 
 /* Instrumentation: launches one kernel of the steady-state RK stage `reps`
@@ -303,15 +305,21 @@ int fr_stream_idle(fr_case *c);
  * cudaMalloc/cudaFree brings.  divF and detJ are device arrays in the
  * library's layout ([nSpts][nEles][nFields] and [nSpts][nEles]), nFields =
  * nDims + 2, order <= 5, nEles <= FR_NOALLOC_MAX_ELES; out is a host array of
- * nFields.  Partial sums live in one fixed static device array of
- * FR_NOALLOC_SCRATCH_BYTES per GPU, so:
+ * nFields.  divF and detJ must hold FP64 values: the FP32 working arrays of a
+ * precision-form case (what fr_device_ptr returns for FR_PREC_MIXED) are
+ * refused with FR_ERR_ARG.  Partial sums live in one fixed static device
+ * array of FR_NOALLOC_SCRATCH_BYTES per GPU, so:
  *   - the first call on a device (with that device current) looks up the
- *     array's address; make it before any stream capture;
+ *     array's address and keeps it; after a cudaDeviceReset of that device
+ *     the kept address is stale: do not call it on that device again;
+ *   - no call may be made while its stream is being captured into a CUDA
+ *     graph (each call copies from host memory and synchronises the stream);
  *   - calls that overlap in time (other streams, other host threads) race
  *     on the array: issue them one after another;
  *   - nothing needs zeroing: each call writes every partial it reads.
  * Returns when the result is in out (the stream is synchronised);
- * FR_ERR_ARG for sizes beyond the limits, FR_ERR_NONFINITE on a NaN norm. */
+ * FR_ERR_ARG for sizes beyond the limits or FP32 arrays, FR_ERR_NONFINITE
+ * when a norm is NaN (a NaN anywhere in divF, for every resType). */
 #define FR_NOALLOC_MAX_SPTS 216
 #define FR_NOALLOC_MAX_ELES 2147483647
 #define FR_NOALLOC_SCRATCH_BYTES ((1024 * 5 + 5 + FR_NOALLOC_MAX_SPTS) * 8)

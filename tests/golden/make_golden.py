@@ -7,7 +7,7 @@ setup arrays (operators, metrics, face connectivity), the initial state, the
 intermediates of one residual evaluation (U_fpts, F_spts, Fn_fpts,
 disFn_fpts, divF) and the state after N time steps.
 
-    make -C oracle && python tests/golden/make_golden.py [case ...]
+    make -C oracle REF=<FlurryPP sources> && python tests/golden/make_golden.py [case ...]
 
 Requires the reference build (this container); the committed .npz files are
 what the tests read.
@@ -286,7 +286,7 @@ def run_case(name: str) -> None:
 
 def main(argv: list[str]) -> None:
     if not os.path.exists(HARNESS):
-        sys.exit(f"{HARNESS} missing: run `make -C oracle` first")
+        sys.exit(f"{HARNESS} missing: run `make -C oracle REF=<FlurryPP sources>` first")
     write_meshes()
     for name in argv or list(CASES) + ["restart_p2_to_p3"]:
         if name == "restart_p2_to_p3":

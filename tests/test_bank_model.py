@@ -3,12 +3,9 @@
 model finds best for both FP64 tile shapes (2 and 4 elements per CTA)."""
 import os
 import re
-import sys
 
+import bank_model
 from conftest import ROOT
-
-sys.path.insert(0, os.path.join(ROOT, "flurrypp_b200", "csrc", "kernels"))
-import bank_model  # noqa: E402
 
 
 def kernel_padding():

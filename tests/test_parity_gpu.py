@@ -121,6 +121,23 @@ def test_residual_norm_matches_oracle():
         assert np.allclose(s.residual_norm(rt), c.residual_norm(a["divF_0"], rt), rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("prec", [fb.FR_PREC_FP64, fb.FR_PREC_MIXED])
+def test_nan_residual_fails_every_norm(prec):
+    """One NaN value of the state makes the residual NaN in a few elements;
+    every norm reports FR_ERR_NONFINITE, the maximum (resType 3) included,
+    as the reference's writeResidual stops on a NaN residual."""
+    a, meta = load_golden("vortex2d_p3_8")
+    s = fb.Solver(deck_path(meta), precision=prec)
+    U = a["U_init"].copy()
+    U[3, 5, 1] = np.nan
+    s.set_state(U)
+    s.calc_residual(0)
+    for rt in (1, 2, 3):
+        with pytest.raises(fb.FrError) as ei:
+            s.residual_norm(rt)
+        assert ei.value.code == fb.FR_ERR_NONFINITE, rt
+
+
 def test_nonfinite_state_is_reported():
     """Host-side fault injection: a poisoned state is caught, not trapped."""
     a, meta = load_golden("vortex2d_p3_8")

@@ -143,9 +143,15 @@ def test_two_gloo_ranks_exchange_traces_in_plan_order(deck):
     procs = [ctx.Process(target=_rank, args=(r, 2, port, deck, q)) for r in range(2)]
     for p in procs:
         p.start()
-    for p in procs:
-        p.join(180)
-        assert p.exitcode == 0
+    try:
+        for p in procs:
+            p.join(180)
+    finally:
+        for p in procs:  # a rank blocked on a dead peer must not outlive the test
+            if p.is_alive():
+                p.kill()
+                p.join(10)
+    assert all(p.exitcode == 0 for p in procs)
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert all(ok for _, ok, _ in got)
     assert got[0][2] == got[1][2] > 0

@@ -16,6 +16,7 @@ import flurrypp_b200 as fb
 from conftest import deck_path, load_golden, perturb_opts
 
 FR_OK, FR_ERR_ARG = 0, 1
+FR_ERR_NONFINITE = fb.FR_ERR_NONFINITE
 NORM_RTOL = 1e-12  # summation order differs (block tree vs element order)
 
 
@@ -41,7 +42,7 @@ def test_noalloc_refuses_sizes_beyond_the_static_array():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "p5_2d"])
+@pytest.mark.parametrize("case", ["vortex2d_p3_8", "tgv3d_p3_4_perturbed", "p5_2d", "lobatto_hu3d_p3"])
 def test_noalloc_norm_matches_residual_norm_twice(case):
     import torch
 
@@ -65,3 +66,47 @@ def test_noalloc_norm_matches_residual_norm_twice(case):
                    out.ctypes.data_as(ctypes.c_void_p), None)
             assert st == FR_OK, (call, st)
             assert np.allclose(out, want, rtol=NORM_RTOL, atol=0), (rt, call, out, want)
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_the_precision_forms_fp32_arrays():
+    """A precision-form case's divF_0 is FP32; read as FP64 it would be
+    garbage, so the entry point refuses it before any device work."""
+    a, meta = load_golden("vortex2d_p3_8")
+    s = fb.Solver(deck_path(meta), precision=fb.FR_PREC_MIXED)
+    s.set_state(a["U_init"])
+    s.calc_residual(0)
+    s.synchronize()
+    divF, nbytes = s.device_ptr("divF_0")
+    assert nbytes == s.nSpts * s.nEles * s.nFields * 4
+    out = np.zeros(s.nFields)
+    f = _entry()
+    fp64 = fb.Solver(deck_path(meta))  # a real FP64 detJ-sized array to pass beside it
+    fp64.set_state(a["U_init"])
+    fp64.calc_residual(0)
+    good, _ = fp64.device_ptr("divF_0")
+    st = f(divF, good, s.nDims, s.order, s.nEles, s.nFields, 2, out.ctypes.data_as(ctypes.c_void_p), None)
+    assert st == FR_ERR_ARG
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rt", [1, 2, 3])
+def test_noalloc_reports_a_nan_residual_for_every_norm(rt):
+    """One NaN value of the state gives NaN residuals in a few elements only;
+    every norm, the maximum included, must report it."""
+    import torch
+
+    a, meta = load_golden("vortex2d_p3_8")
+    s = fb.Solver(deck_path(meta))
+    U = a["U_init"].copy()
+    U[3, 5, 1] = np.nan
+    s.set_state(U)
+    s.calc_residual(0)
+    s.synchronize()
+    divF, _ = s.device_ptr("divF_0")
+    detJ = torch.from_numpy(s.get_array("detJac_spts")).to("cuda:0")
+    torch.cuda.synchronize()
+    out = np.zeros(s.nFields)
+    st = _entry()(divF, detJ.data_ptr(), s.nDims, s.order, s.nEles, s.nFields, rt,
+                  out.ctypes.data_as(ctypes.c_void_p), None)
+    assert st == FR_ERR_NONFINITE
