@@ -152,37 +152,85 @@ def whole_job_rate(world: int, dof: int, stages: int, steps: int, ms: float) -> 
     return world * dof * stages * steps / (ms / 1e3)
 
 
-def reference_sample(steps: int, warmup: int, threads: int):
-    """The reference's own CPU path (oracle/_ref, OpenMP build) on the bounded
-    sample: the same Taylor-Green problem on 16^3 hexes (same per-element work,
-    1/8 of the elements; the reference's O(n^2) setup makes 32^3 take ~25 min)."""
+TGV_ARGS = ["--ic", "tgv", "--tgv-mach", "0.1", "--cfl-dt", "0.5"]
+
+
+def cpu_info():
+    """The host CPU the reference runs on: model, logical CPUs, CPUs this
+    process may use."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    avail = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    return {"model": model, "logical_cpus": os.cpu_count(), "available_cpus": avail}
+
+
+def ref_threads(n_cols: int) -> int:
+    """OpenMP threads for the reference: the most that the available CPUs
+    allow among those that divide N = nEles*nFields (the reference's
+    omp_blocked_dgemm drops columns when the thread count does not divide N,
+    src/global.cpp:229-230)."""
+    avail = cpu_info()["available_cpus"]
+    return max(t for t in range(1, avail + 1) if n_cols % t == 0)
+
+
+def run_ref(deck: str, harness_args, steps: int, warmup: int, threads: int, time1: int = 0, cwd=None):
+    """One timed run of the reference's own CPU path (oracle/_ref, OpenMP
+    build): mesh setup, initial state, W untimed and K timed solver::update()
+    steps (the driver's loop, P-multigrid cycle included), and optionally K1
+    more on one thread.  Returns (the harness's JSON, None) or (None, why)."""
     if not os.path.exists(REF_BIN):
         return None, "oracle/_ref/fr_ref_harness_omp not built"
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
-    cmd = [REF_BIN, DECK_CPU, "-", "--ic", "tgv", "--tgv-mach", "0.1", "--cfl-dt", "0.5",
-           "--time", f"{steps},{warmup}", "--threads", str(threads)]
-    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    cmd = [REF_BIN, deck, "-", *harness_args, "--time", f"{steps},{warmup}", "--threads", str(threads)]
+    if time1:
+        cmd += ["--time1", str(time1)]
+    t0 = time.perf_counter()
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env, cwd=cwd)
     if r.returncode != 0:
         return None, f"reference harness failed: {r.stderr[-200:]}"
     line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
-    return json.loads(line), None
+    out = json.loads(line)
+    out["wall_s"] = time.perf_counter() - t0
+    return out, None
 
 
-def ref_threads():
-    n = os.cpu_count() or 1
-    # the reference's omp_blocked_dgemm drops columns unless the thread count
-    # divides N = nEles*nFields (global.cpp:229-230); 16^3*5 = 20480 = 2^12*5
-    t = 1
-    while t * 2 <= n and 20480 % (t * 2) == 0:
-        t *= 2
-    return t
+HEADLINE_ELES, HEADLINE_FIELDS = 32 ** 3, 5
+
+
+def headline_config(world: int) -> dict:
+    """The workload both arms measure (32^3 hexes, P3, TGV, RK4, FP64)."""
+    return {"workload": WORKLOAD, "nEles": HEADLINE_ELES, "order": 3, "dof": HEADLINE_ELES * 64 * HEADLINE_FIELDS,
+            "rk_stages": 4, "l2_flush": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def headline_reference(steps: int, warmup: int, time1: int = 1):
+    """The reference on the headline workload itself (32^3 hexes), all the
+    threads that divide N; its mesh setup (not timed) takes a minute or two."""
+    thr = ref_threads(HEADLINE_ELES * HEADLINE_FIELDS)
+    res, err = run_ref(DECK_GPU, TGV_ARGS, steps, warmup, thr, time1=time1)
+    if res is None:
+        return None, err
+    cpu = cpu_info()
+    res["cpu"] = cpu
+    res["sample"] = (f"the full workload (TGV P3 32^3 hexes), {res['steps']} RK4 steps after {warmup} warm-up, "
+                     f"OpenMP {res['threads']} threads (the most of {cpu['available_cpus']} available CPUs that "
+                     f"divide nEles*nFields), 1 BLAS thread; 1-thread figure over {res['steps_1thread']} step(s); "
+                     "mesh setup untimed")
+    return res, None
 
 
 def run_reference_arm(args, rank):
     if rank != 0:
         return
-    thr = ref_threads()
-    res, err = reference_sample(max(1, args.steps), max(1, args.warmup), thr)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    res, err = headline_reference(max(1, args.steps), max(1, args.warmup))
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
@@ -192,10 +240,10 @@ def run_reference_arm(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / res["steps"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (Taylor-Green initial condition)",
-        "config": {"workload": WORKLOAD, "sample": "16^3 hexes (reference CPU, OpenMP)"},
+        "config": headline_config(world),
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": res["threads"], "kind": "reference",
-                         "sample": f"TGV P3 16^3 hexes, {res['steps']} RK4 steps after {args.warmup} warm-up, "
-                                   f"OpenMP {res['threads']} threads, 1 BLAS thread"},
+                         "sample": res["sample"], "cpu": res["cpu"],
+                         "value_1thread": res["dof_stage_per_s_1thread"]},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -301,11 +349,81 @@ def form_ns_tgv40(args, fb, torch, stream):
         del c
     out["workload"] = ("3D Navier-Stokes TGV Re 1600 Pr 0.71 Mach 0.1, 40^3 hexes perturbed U(-0.05h,0.05h) "
                        "seed 2024, P=4, LDG tau 0.1 beta 0.5, Rusanov, RK4")
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = ns_reference(args)
     out["dof"] = dof
     out["dt"] = dt
     out["speedup_precision_vs_fp64"] = out["precision"]["value"] / out["fp64"]["value"]
     out["error_vs_fp64"] = dict(steps=args.ns_steps, **state_errors(states["precision"], states["fp64"]))
     return out
+
+
+def ns_reference(args):
+    """The reference's CPU path on the Navier-Stokes TGV per RK stage, on a
+    20^3 sample of the 40^3 mesh (same order, perturbation law and physics,
+    1/8 of the elements: the reference's mesh setup grows with the square of
+    the element count)."""
+    import tempfile
+
+    n = 20
+    src = open(DECK_NS).read()
+    for ax in ("nx", "ny", "nz"):
+        src = src.replace(f"{ax}            40", f"{ax}            {n}")
+    with tempfile.TemporaryDirectory() as td:
+        deck = os.path.join(td, "ns20.deck")
+        open(deck, "w").write(src)
+        thr = ref_threads(n ** 3 * 5)
+        res, err = run_ref(deck, ["--ic", "tgv", "--tgv-mach", "0.1", "--perturb", "2024,0.05",
+                                  "--mu-inf", repr(1.0 / 1600.0), "--cfl-dt", "0.5"], 3, 1, thr)
+    if res is None:
+        return {"value": None, "sample": err}
+    return {"value": res["dof_stage_per_s"], "unit": METRIC, "cores": res["threads"], "kind": "reference",
+            "sample": f"NS TGV P4 on 20^3 perturbed hexes (1/8 of the elements), {res['steps']} RK4 steps "
+                      f"after 1 warm-up, OpenMP {res['threads']} threads, per-stage rate"}
+
+
+def vortex32_form(args, fb, torch, stream):
+    """Config 1: 2-D Euler vortex (strength 5, Mach 0.5 along +x), periodic
+    [-5,5]^2, 32x32 quads, P3, RK4, fixed dt at CFL 0.5, 1000 steps: the FP64
+    GPU path and the reference's CPU path on the same run."""
+    deck = os.path.join(ROOT, "tests", "golden", "decks", "vortex2d_p3_32.deck")
+    s = fb.Solver(deck)
+    s.set_stream(stream.cuda_stream)
+    s.initialize_solution(fb.IC_VORTEX, (5.0, 0.0, 0.0, 0.5))
+    dt = s.calc_dt()
+    s.set_dt(dt)
+    dof, nrk = s.nSpts * s.nEles * s.nFields, s.nRKSteps
+    steps = 1000
+    s.run(3)
+    ms = dev_ms(torch, stream, lambda: s.run(steps))
+    out = {"workload": "2-D Euler vortex, 32x32 quads, P3, RK4, CFL 0.5 fixed dt, FP64", "dof": dof,
+           "value": dof * nrk * steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / steps, "steps": steps}
+    if not args.no_cpu_baseline:
+        thr = ref_threads(s.nEles * s.nFields)
+        res, err = run_ref(deck, ["--ic", "vortex", "--vortex", "5,0,0,0.5", "--cfl-dt", "0.5"], steps, 3, thr)
+        out["cpu_baseline"] = ({"value": res["dof_stage_per_s"], "unit": METRIC, "cores": res["threads"],
+                                "kind": "reference", "sample": f"the whole run: {steps} RK4 steps, OpenMP "
+                                                               f"{res['threads']} threads"}
+                               if res else {"value": None, "sample": err})
+    return out
+
+
+def batch_reference(specs, decks, k: int, steps: int):
+    """The reference's CPU path on the first k cases of the batch, one after
+    another, each over `steps` RK4 steps: its DOF-stage rate over them."""
+    dofs, secs, thr_used = 0.0, 0.0, set()
+    for (n, P, eps, xc, yc, M), deck in list(zip(specs, decks))[:k]:
+        thr = ref_threads(n * n * 4)
+        res, err = run_ref(deck, ["--ic", "vortex", "--vortex", f"{eps!r},{xc!r},{yc!r},{M!r}", "--cfl-dt", "0.5"],
+                           steps, 1, thr)
+        if res is None:
+            return {"value": None, "sample": err}
+        dofs += res["dof"] * res["stages"]
+        secs += res["seconds"]
+        thr_used.add(res["threads"])
+    return {"value": dofs / secs, "unit": METRIC, "cores": max(thr_used), "kind": "reference",
+            "sample": f"the first {k} of the cases, one after another, {steps} RK4 steps each, OpenMP "
+                      f"threads {sorted(thr_used)} (the most that divide each case's nEles*nFields)"}
 
 
 def form_batch256(args, fb, torch, stream):
@@ -325,9 +443,10 @@ def form_batch256(args, fb, torch, stream):
         specs.append((n, P, eps, xc, yc, M))
     tmp = tempfile.mkdtemp(prefix="fr_batch_")
     t0 = time.perf_counter()
-    c64, c32, dofs = [], [], []
+    c64, c32, dofs, decks = [], [], [], []
     for i, (n, P, eps, xc, yc, M) in enumerate(specs):
         deck = vortex_case(os.path.join(tmp, f"b{i}.deck"), n, P, M)
+        decks.append(deck)
         a = fb.Solver(deck)
         a.set_stream(stream.cuda_stream)
         a.initialize_solution(fb.IC_VORTEX, (eps, xc, yc, M))
@@ -350,8 +469,10 @@ def form_batch256(args, fb, torch, stream):
     for i, (n, P, eps, xc, yc, M) in enumerate(specs):
         c64[i].initialize_solution(fb.IC_VORTEX, (eps, xc, yc, M))
     res = {}
+    forms = {fb.FR_BATCH_GROUPS: "groups", fb.FR_BATCH_MANY_ORDER: "many_order"}
     for tag, cs in (("fp64_batched", c64), ("precision_batched", c32)):
-        bt = fb.Batch(cs)
+        bt = fb.Batch(cs)  # times both step forms on its own state and keeps the faster
+        chosen = bt.form()
         w = 3
         bt.run(w)
         torch.cuda.synchronize()
@@ -362,7 +483,18 @@ def form_batch256(args, fb, torch, stream):
         bt.gather()
         inf = bt.info()
         res[tag] = {"value": tot * nrk * (args.batch_steps - w) / sec, "unit": METRIC,
-                    "seconds": sec, "groups": inf["groups"]}
+                    "seconds": sec, "groups": inf["groups"], "form": forms[chosen["form"]],
+                    "autotune_ms_per_step": {"groups": chosen["ms_groups"], "many_order": chosen["ms_many_order"]}}
+        # the other form over 100 more steps (after the members took their state)
+        other = fb.FR_BATCH_MANY_ORDER if chosen["form"] == fb.FR_BATCH_GROUPS else fb.FR_BATCH_GROUPS
+        bt.set_form(other)
+        bt.run(3)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        bt.run(100)
+        torch.cuda.synchronize()
+        res[tag]["other_form"] = {"form": forms[other],
+                                  "value": tot * nrk * 100 / (time.perf_counter() - t2), "unit": METRIC}
         del bt
     errs = [state_errors(b.get_state(), a.get_state())["l2_rel"] for a, b in zip(c64, c32)]
     plain = tot * nrk * args.alone_steps / (ms_alone / 1e3)
@@ -374,6 +506,10 @@ def form_batch256(args, fb, torch, stream):
         "plain_fp64_case_by_case": {"value": plain, "unit": METRIC, "steps_timed_per_case": args.alone_steps},
         "fp64_batched": res["fp64_batched"], "precision_batched": res["precision_batched"],
         "speedup_precision_batched_vs_plain_fp64": res["precision_batched"]["value"] / plain,
+        # the same batching on both sides: what the precision form alone gains
+        "speedup_precision_batched_vs_fp64_batched": (res["precision_batched"]["value"]
+                                                      / res["fp64_batched"]["value"]),
+        "cpu_baseline": (batch_reference(specs, decks, 8, 10) if not args.no_cpu_baseline else None),
         "timer": "host clock around a synchronized batch run (order groups run on their own streams)",
         "error_vs_fp64": {"steps": args.batch_steps, "l2_rel_max": max(errs),
                           "l2_rel_median": float(np.median(errs))},
@@ -389,7 +525,7 @@ def form_serve(args, fb, torch):
 
     rng = np.random.default_rng(args.serve_seed)
     tmp = tempfile.mkdtemp(prefix="fr_serve_")
-    reqs = []
+    reqs, n_eles = [], {}
     for i in range(args.serve_requests):
         h = float(rng.uniform(0.02, 0.1))
         nx = int(rng.integers(24, 97))
@@ -406,6 +542,7 @@ def form_serve(args, fb, torch):
         all_dof = dof * 5 + sum(nx * (nx // 3) * (p + 1) ** 2 * 4 * (1 + 2 * 2 * 4 + (1 if p > 0 else 0))
                                 for p in range(P))
         reqs.append((channel_case(os.path.join(tmp, f"bump{i}.deck"), msh, P, M), dof, all_dof))
+        n_eles[reqs[-1][0]] = nx * (nx // 3)
 
     def serve(subset, max_inflight, rate, precision=fb.FR_PREC_FP64):
         srv = fb.Server(budget_bytes=args.serve_budget_gb << 30, max_inflight=max_inflight, check_every=10,
@@ -417,13 +554,14 @@ def form_serve(args, fb, torch):
             if rate:
                 time.sleep(float(gaps[k]))
             ids.append(srv.submit(deck, tol=1e-8, max_steps=args.serve_max_steps))
-        polls = []
+        polls, forms = [], []
         for r in ids:
             try:
                 srv.wait(r, 3600)
             except fb.FrError:
                 pass
             polls.append(srv.poll(r))
+            forms.append(srv.poll_form(r))
         sec = time.perf_counter() - t0
         srv.close()
         lat = [p["latency_s"] for p in polls]
@@ -431,21 +569,29 @@ def form_serve(args, fb, torch):
         stages = sum(4 * p["steps"] * dof for p, (_, dof, _) in zip(polls, subset))
         all_stages = sum(p["steps"] * all_dof for p, (_, _, all_dof) in zip(polls, subset))
         return {"solves_per_s": len(done) / sec, "seconds": sec, "completed": len(done),
+                "steps_each": [p["steps"] for p in polls],
                 "converged_1e-8": sum(1 for p in done if p["res_ratio"] <= 1e-8),
                 "median_residual_drop": float(np.median([p["res_ratio"] for p in done])) if done else None,
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                 "steps_mean": float(np.mean([p["steps"] for p in polls])),
+                "steps_fp32_share": (sum(f["steps_fp32"] for f in forms) / max(1, sum(p["steps"] for p in polls))),
                 "fine_dof_stage_per_s": stages / sec, "all_level_dof_stage_per_s": all_stages / sec}
 
     sweep = {}
     for rate in args.serve_rates:
         sweep[f"rate_{rate:g}_per_s"] = dict(max_inflight=args.serve_inflight, **serve(reqs, args.serve_inflight, rate))
+        sweep[f"rate_{rate:g}_per_s"].pop("steps_each")
     top = max(args.serve_rates)
     precision = dict(max_inflight=args.serve_inflight, rate_per_s=top,
-                     **serve(reqs, args.serve_inflight, top, fb.FR_PREC_MIXED))
+                     form="FR_PREC_MIXED_REFINE: precision form until the FP32 residual stops falling, then FP64",
+                     **serve(reqs, args.serve_inflight, top, fb.FR_PREC_MIXED_REFINE))
     k = min(args.serve_alone, len(reqs))
     alone = serve(reqs[:k], 1, 0.0)
     alone["sample"] = f"the first {k} requests, submitted together, one in flight"
+    if not args.no_cpu_baseline:
+        alone["cpu_baseline"] = serve_reference(reqs[:k], alone.pop("steps_each"), n_eles)
+    else:
+        alone.pop("steps_each")
     best = max(v["solves_per_s"] for v in sweep.values())
     return {
         "workload": (f"{len(reqs)} channel-over-bump requests, seed {args.serve_seed}, Poisson arrivals, "
@@ -459,10 +605,36 @@ def form_serve(args, fb, torch):
     }
 
 
+def serve_reference(subset, steps_each, n_eles):
+    """The same requests solved serially by the reference's CPU path, one at a
+    time: each request's time per driver step (update + P-multigrid cycle,
+    the reference's own loop) over a sample of steps, times the steps the
+    request took to converge here, gives its solve time; latencies are the
+    completion times of the requests submitted together."""
+    import numpy as np
+
+    per_req = []
+    for (deck, _, _), n in zip(subset, steps_each):
+        thr = ref_threads(n_eles[deck] * 4)
+        sample = 20
+        res, err = run_ref(os.path.basename(deck), [], sample, 2, thr, cwd=os.path.dirname(deck))
+        if res is None:
+            return {"value": None, "sample": err}
+        per_req.append(res["seconds"] / res["steps"] * n)
+    done = np.cumsum(per_req)
+    return {"solves_per_s": len(per_req) / float(done[-1]), "p50_latency_s": float(np.percentile(done, 50)),
+            "p99_latency_s": float(np.percentile(done, 99)), "kind": "reference",
+            "sample": f"the same {len(per_req)} requests, serially: the reference's time per driver step "
+                      "(update + P-multigrid cycle) over 20 steps after 2 warm-up, times the steps each request "
+                      "took to reach the 1e-8 drop here (extrapolated, not run to convergence on the CPU)",
+            "solve_s_each": per_req}
+
+
 def run_forms(args, fb, torch, stream, dt):
     forms = {}
     want = set(args.forms.split(",")) if args.forms else set()
-    jobs = [("precision_tgv32", lambda: form_precision_tgv32(args, fb, torch, stream, dt)),
+    jobs = [("vortex32_1000", lambda: vortex32_form(args, fb, torch, stream)),
+            ("precision_tgv32", lambda: form_precision_tgv32(args, fb, torch, stream, dt)),
             ("precision_ns_tgv40", lambda: form_ns_tgv40(args, fb, torch, stream)),
             ("batch256", lambda: form_batch256(args, fb, torch, stream)),
             ("serve", lambda: form_serve(args, fb, torch))]
@@ -539,9 +711,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=12)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="precision_tgv32,precision_ns_tgv40,batch256,serve",
+    ap.add_argument("--forms", default="vortex32_1000,precision_tgv32,precision_ns_tgv40,batch256,serve",
                     help="comma list of extra workloads measured at N=1 ('' for none)")
     ap.add_argument("--err-steps", type=int, default=200)
     ap.add_argument("--ns-steps", type=int, default=500)
@@ -722,9 +894,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (Taylor-Green initial condition, seeded-free analytic field)",
-            "config": {"workload": WORKLOAD, "nEles": E, "order": s.order, "dof": dof, "rk_stages": nrk,
-                       "dt": dt, "l2_flush": "inputs larger than L2 (no flush)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": headline_config(world), "dt": dt,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8,
                     "cases_in_flight": E2E_CASES, "steps": args.e2e_steps,
                     "copy_bound": e2e_copy_bound, "frac_of_copy_bound": e2e / e2e_copy_bound},
@@ -741,13 +911,11 @@ def main():
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:
-            thr = ref_threads()
-            res, err = reference_sample(args.cpu_steps, 1, thr)
+            res, err = headline_reference(args.cpu_steps, 2)
             if res:
                 out["cpu_baseline"] = {
                     "value": res["dof_stage_per_s"], "unit": METRIC, "cores": res["threads"], "kind": "reference",
-                    "sample": f"reference CPU (OpenMP {res['threads']} threads), TGV P3 16^3 hexes, "
-                              f"{res['steps']} RK4 steps"}
+                    "sample": res["sample"], "cpu": res["cpu"], "value_1thread": res["dof_stage_per_s_1thread"]}
             else:
                 out["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
                                        "sample": err}

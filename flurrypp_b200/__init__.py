@@ -37,8 +37,10 @@ FR_ERR_TIMEOUT = 6
 FR_ERR_UNSUPPORTED = 7
 FR_ERR_STATE = 8
 
+FR_BATCH_GROUPS, FR_BATCH_MANY_ORDER = 0, 1
 FR_PREC_FP64 = 0
 FR_PREC_MIXED = 1
+FR_PREC_MIXED_REFINE = 2  # server: precision form until the FP32 floor, then FP64 to the target
 
 IC_DECK, IC_VORTEX, IC_TGV, IC_UNIFORM = 0, 1, 2, 3
 
@@ -158,17 +160,36 @@ def _load() -> ctypes.CDLL:
         "fr_batch_residual_norms": (i, [P, i, dp, i]),
         "fr_batch_info": (i, [P, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]),
         "fr_batch_last_error": (ctypes.c_char_p, [P]),
+        "fr_batch_form": (i, [P, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+        "fr_batch_set_form": (i, [P, i]),
         "fr_batch_destroy": (None, [P]),
         "fr_server_create": (i, [sz, i, i, i, ctypes.POINTER(P)]),
         "fr_server_submit": (i, [P, ctypes.c_char_p, ctypes.POINTER(Mesh), i, dp, i, ctypes.c_double, i,
                                  ctypes.POINTER(ctypes.c_longlong)]),
         "fr_server_poll": (i, [P, ctypes.c_longlong, ctypes.POINTER(i), dp, ctypes.POINTER(i), dp]),
         "fr_server_wait": (i, [P, ctypes.c_longlong, ctypes.c_double]),
+        "fr_server_poll_form": (i, [P, ctypes.c_longlong, ctypes.POINTER(i), ctypes.POINTER(i)]),
         "fr_server_result": (i, [P, ctypes.c_longlong, dp, sz]),
         "fr_server_cancel": (i, [P, ctypes.c_longlong]),
         "fr_server_stats": (i, [P, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(sz)]),
         "fr_server_destroy": (None, [P]),
         "fr_server_set_precision": (i, [P, i]),
+        "fr_shard_create": (i, [ctypes.c_char_p, ctypes.POINTER(SetupOpts), i, ctypes.POINTER(P)]),
+        "fr_part_create": (i, [ctypes.c_char_p, ctypes.POINTER(SetupOpts), i, i, P, ctypes.POINTER(P)]),
+        "fr_part_nccl_ok": (i, [P]),
+        "fr_nccl_unique_id": (i, [ctypes.c_char_p]),
+        "fr_nccl_comm_init": (i, [i, ctypes.c_char_p, i, i, ctypes.POINTER(P)]),
+        "fr_nccl_comm_destroy": (i, [P]),
+        "fr_shard_info": (i, [P, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]),
+        "fr_shard_set_state": (i, [P, dp, sz]),
+        "fr_shard_get_state": (i, [P, dp, sz]),
+        "fr_shard_set_dt": (i, [P, ctypes.c_double]),
+        "fr_shard_calc_residual": (i, [P, i]),
+        "fr_shard_get_residual": (i, [P, i, dp, sz]),
+        "fr_shard_run": (i, [P, i]),
+        "fr_shard_time": (i, [P, dp, dp]),
+        "fr_shard_last_error": (ctypes.c_char_p, [P]),
+        "fr_shard_destroy": (None, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -195,10 +216,15 @@ def _dptr(a: np.ndarray):
 class Solver:
     """One FR case on the GPU (the reference ``solver`` + its ``input``)."""
 
-    def __init__(self, deck: str, mesh: dict | None = None, **opts):
+    def __init__(self, deck: str, mesh: dict | None = None, part=None, **opts):
+        """part = (nparts, rank, nccl_comm): this rank's part of the case split
+        by the partition of shard_plan (fr_part_create)."""
         self._c = ctypes.c_void_p()
         o = default_opts(**opts)
-        if mesh is None:
+        if part is not None:
+            nparts, rank, comm = part
+            st = lib.fr_part_create(deck.encode(), ctypes.byref(o), nparts, rank, comm, ctypes.byref(self._c))
+        elif mesh is None:
             st = lib.fr_create_from_deck(deck.encode(), ctypes.byref(o), ctypes.byref(self._c))
         else:
             self._mesh_keep = m = _make_mesh(mesh)
@@ -364,6 +390,87 @@ class Solver:
         return p.value, b.value
 
 
+def nccl_comm(nranks: int, rank: int, device: int, unique_id: bytes | None = None):
+    """An NCCL communicator through the library (fr_nccl_*): rank 0 passes
+    unique_id=None and shares the returned id with the others, which pass it.
+    Returns (comm, id)."""
+    idb = ctypes.create_string_buffer(128)
+    if unique_id is None:
+        st = lib.fr_nccl_unique_id(idb)
+        if st != FR_OK:
+            raise FrError(st, "ncclGetUniqueId")
+    else:
+        ctypes.memmove(idb, unique_id, 128)
+    comm = ctypes.c_void_p()
+    st = lib.fr_nccl_comm_init(nranks, idb, rank, device, ctypes.byref(comm))
+    if st != FR_OK:
+        raise FrError(st, "ncclCommInitRank")
+    return comm, idb.raw
+
+
+class Shard:
+    """One case split into `nparts` parts on one device (fr_shard_*): the
+    partition of Solver.shard_plan, the cut faces' traces exchanged between
+    the parts at every stage.  State and residual in the whole case's layout."""
+
+    def __init__(self, deck: str, nparts: int, **opts):
+        o = default_opts(**opts)
+        self._s = ctypes.c_void_p()
+        st = lib.fr_shard_create(deck.encode(), ctypes.byref(o), nparts, ctypes.byref(self._s))
+        if st != FR_OK:
+            msg = lib.fr_shard_last_error(self._s).decode() if self._s else "shard create failed"
+            lib.fr_shard_destroy(self._s)
+            self._s = None
+            raise FrError(st, msg)
+        self.nparts = nparts
+        self.host = Solver(deck, device=-1, **{k: v for k, v in opts.items() if k != "device"})
+        self.shape = self.host.shape
+
+    def __del__(self):
+        if getattr(self, "_s", None):
+            lib.fr_shard_destroy(self._s)
+            self._s = None
+
+    def _check(self, st):
+        if st != FR_OK:
+            raise FrError(st, lib.fr_shard_last_error(self._s).decode())
+
+    def info(self):
+        n = ctypes.c_int()
+        owned = (ctypes.c_int * self.nparts)()
+        cut = (ctypes.c_longlong * self.nparts)()
+        self._check(lib.fr_shard_info(self._s, ctypes.byref(n), owned, cut))
+        return {"nparts": n.value, "owned": list(owned), "cut_points": list(cut)}
+
+    def set_state(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self._check(lib.fr_shard_set_state(self._s, _dptr(U), U.size))
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        self._check(lib.fr_shard_get_state(self._s, _dptr(out), out.size))
+        return out
+
+    def set_dt(self, dt: float):
+        self._check(lib.fr_shard_set_dt(self._s, dt))
+
+    def calc_residual(self, step: int = 0):
+        self._check(lib.fr_shard_calc_residual(self._s, step))
+
+    def get_residual(self, step: int = 0) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        self._check(lib.fr_shard_get_residual(self._s, step, _dptr(out), out.size))
+        return out
+
+    def run(self, nsteps: int):
+        self._check(lib.fr_shard_run(self._s, nsteps))
+
+    def time(self):
+        t, d = ctypes.c_double(), ctypes.c_double()
+        self._check(lib.fr_shard_time(self._s, ctypes.byref(t), ctypes.byref(d)))
+        return t.value, d.value
+
+
 class Batch:
     """Many independent cases advanced together (fr_batch_*): same-order cases
     merged into one group, one face + one element launch per stage per order."""
@@ -400,6 +507,16 @@ class Batch:
         out = np.empty((len(self.solvers), nf), dtype=np.float64)
         self._check(lib.fr_batch_residual_norms(self._b, res_type, _dptr(out), nf))
         return out
+
+    def form(self) -> dict:
+        """The step form in use (FR_BATCH_GROUPS / FR_BATCH_MANY_ORDER) and the
+        ms per step each form measured at creation (-1: not timed)."""
+        f, a, b = ctypes.c_int(), ctypes.c_float(), ctypes.c_float()
+        self._check(lib.fr_batch_form(self._b, ctypes.byref(f), ctypes.byref(a), ctypes.byref(b)))
+        return {"form": f.value, "ms_groups": a.value, "ms_many_order": b.value}
+
+    def set_form(self, form: int):
+        self._check(lib.fr_batch_set_form(self._b, form))
 
     def info(self):
         g = ctypes.c_int()
@@ -448,6 +565,14 @@ class Server:
                                   ctypes.byref(ratio))
         return {"status": stt.value, "latency_s": lat.value, "steps": steps.value, "res_ratio": ratio.value,
                 "code": code}
+
+    def poll_form(self, rid: int) -> dict:
+        """Form the request runs in and its steps in the precision form."""
+        prec, n32 = ctypes.c_int(), ctypes.c_int()
+        st = lib.fr_server_poll_form(self._s, rid, ctypes.byref(prec), ctypes.byref(n32))
+        if st != FR_OK:
+            raise FrError(st, "poll_form failed")
+        return {"precision": prec.value, "steps_fp32": n32.value}
 
     def wait(self, rid: int, timeout_s: float = 600.0):
         st = lib.fr_server_wait(self._s, rid, timeout_s)

@@ -21,6 +21,9 @@
 #include <type_traits>
 #include <vector>
 
+#include <dlfcn.h>
+#include <nccl.h>
+
 #include "../../include/fr_b200.h"
 #include "host/fr_host.hpp"
 #include "kernels/launch.cuh"
@@ -56,6 +59,41 @@ bool fr_internal_is_fp32(const void *p) {
   if (it == g_fp32Arrays.begin()) return false;
   --it;
   return a >= it->first && a < it->second;
+}
+
+// NCCL, resolved at run time from the libnccl.so.2 the process already has
+// (a torch process loads its own) or the system's, so that the library never
+// brings a second NCCL into a process.  Used only by parts of a case split
+// across ranks (fr_part_create).
+struct NcclApi {
+  bool ok = false;
+  decltype(&ncclSend) send = nullptr;
+  decltype(&ncclRecv) recv = nullptr;
+  decltype(&ncclGroupStart) groupStart = nullptr;
+  decltype(&ncclGroupEnd) groupEnd = nullptr;
+  decltype(&ncclAllReduce) allReduce = nullptr;
+  decltype(&ncclGetUniqueId) uniqueId = nullptr;
+  decltype(&ncclCommInitRank) initRank = nullptr;
+  decltype(&ncclCommDestroy) destroy = nullptr;
+};
+static const NcclApi &nccl_api() {
+  static NcclApi api = [] {
+    NcclApi a;
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) return a;
+    a.send = (decltype(a.send))dlsym(h, "ncclSend");
+    a.recv = (decltype(a.recv))dlsym(h, "ncclRecv");
+    a.groupStart = (decltype(a.groupStart))dlsym(h, "ncclGroupStart");
+    a.groupEnd = (decltype(a.groupEnd))dlsym(h, "ncclGroupEnd");
+    a.allReduce = (decltype(a.allReduce))dlsym(h, "ncclAllReduce");
+    a.uniqueId = (decltype(a.uniqueId))dlsym(h, "ncclGetUniqueId");
+    a.initRank = (decltype(a.initRank))dlsym(h, "ncclCommInitRank");
+    a.destroy = (decltype(a.destroy))dlsym(h, "ncclCommDestroy");
+    a.ok = a.send && a.recv && a.groupStart && a.groupEnd && a.allReduce && a.uniqueId && a.initRank && a.destroy;
+    return a;
+  }();
+  return api;
 }
 
 // cases with fewer solution points than this do not time tile variants
@@ -152,6 +190,33 @@ struct fr_case {
   } errT[2];
   double *errXv = nullptr, *errElem = nullptr, *errOut = nullptr;
   double *monPart = nullptr, *monOut = nullptr;  // boundary monitors: per-point parts, totals
+
+  // one part of a case split by a partition (fr_shard_*): the face points
+  // the partition cuts; their right traces arrive in cut.recv before every
+  // face pass (the shard packs and exchanges them for all parts)
+  frk::CutTableT<double> cut;
+  std::vector<int> cutPeer;  // peer part of every cut point (sorted by peer)
+  // a part on its own rank (fr_part_create): the traces travel by NCCL
+  // send/receive pairs on the case's stream at every face pass, and dt is
+  // the NCCL minimum over the ranks; the in-process shard leaves this null
+  // and exchanges itself
+  ncclComm_t comm = nullptr;
+  std::vector<int> segPeer;
+  std::vector<long long> segOff, segCount;
+  bool ncclOk = true;
+  void exchange_nccl() {
+    const NcclApi &api = nccl_api();
+    frk::launch_pack_cut<double>(nF, cut, Ufpts, stream);
+    launches++;
+    api.groupStart();
+    for (size_t i = 0; i < segPeer.size(); i++) {
+      const size_t n = (size_t)segCount[i] * nF;
+      if (api.send(cut.send + segOff[i] * nF, n, ncclDouble, segPeer[i], comm, stream) != ncclSuccess ||
+          api.recv(cut.recv + segOff[i] * nF, n, ncclDouble, segPeer[i], comm, stream) != ncclSuccess)
+        ncclOk = false;
+    }
+    if (api.groupEnd() != ncclSuccess) ncclOk = false;
+  }
 
   // wall forces and mass flux from the face data of the last residual
   // evaluation (boundFace::computeWallForce / computeMassFlux)
@@ -294,7 +359,9 @@ struct fr_case {
       ownedStream = stream;
     }
     if (o.precision != FR_PREC_FP64 && o.precision != FR_PREC_MIXED)
-      return fail(FR_ERR_UNSUPPORTED, "unknown precision");
+      return fail(FR_ERR_UNSUPPORTED, o.precision == FR_PREC_MIXED_REFINE
+                                          ? "FR_PREC_MIXED_REFINE is a form of the solve server"
+                                          : "unknown precision");
     mixed = o.precision == FR_PREC_MIXED;
     if (!setup_host()) return false;
     return setup_device();
@@ -1232,6 +1299,105 @@ struct fr_case {
     return true;
   }
 
+  // Part r of a case split by the element partition `part` (fr_shard_*):
+  // the part's elements (ascending global ids; local id = rank among them),
+  // its metric arrays sliced from the whole case's, the faces between two of
+  // its elements and its boundary faces, renumbered, and its cut face points
+  // (a face whose other element is in another part): each with this part's
+  // element as the left side, listed by peer part and, per peer, by face
+  // (the whole case's face order) and by the face's left point order, the
+  // order fr_shard_plan gives and both sides of a cut share.  Plain form,
+  // inviscid, static mesh, no P-multigrid (the creator checks).
+  bool split_from(const fr_case &full, const std::vector<int> &part, int r, cudaStream_t st) {
+    opts = full.opts;
+    opts.no_pdl = 1;  // parts run in one stream with copies between their kernels
+    in = full.in;
+    nDims = full.nDims;
+    nF = full.nF;
+    nRK = full.nRK;
+    nS = full.nS;
+    nFp = full.nFp;
+    nPF = full.nPF;
+    op = full.op;
+    const int Ef = full.E;
+    std::vector<int> owned, local(Ef, -1);
+    for (int e = 0; e < Ef; e++)
+      if (part[e] == r) {
+        local[e] = (int)owned.size();
+        owned.push_back(e);
+      }
+    E = (int)owned.size();
+    if (E == 0) return fail(FR_ERR_ARG, "empty part");
+    mesh.nDims = nDims;
+    mesh.nEles = E;
+    auto sel = [&](const std::vector<double> &src, size_t A, size_t B) {
+      std::vector<double> out(A * (size_t)E * B);
+      for (size_t a = 0; a < A; a++)
+        for (int el = 0; el < E; el++)
+          for (size_t b = 0; b < B; b++) out[(a * E + el) * B + b] = src[(a * Ef + owned[el]) * B + b];
+      return out;
+    };
+    geo.pos_spts = sel(full.geo.pos_spts, nS, nDims);
+    geo.pos_fpts = sel(full.geo.pos_fpts, nFp, nDims);
+    geo.detJac_spts = sel(full.geo.detJac_spts, nS, 1);
+    geo.detJac_fpts = sel(full.geo.detJac_fpts, nFp, 1);
+    geo.JGinv_spts = sel(full.geo.JGinv_spts, (size_t)nDims * nS, nDims);
+    geo.norm_fpts = sel(full.geo.norm_fpts, nFp, nDims);
+    geo.dA_fpts = sel(full.geo.dA_fpts, nFp, 1);
+    struct CutPt {
+      int peer, slot, left;
+    };
+    std::vector<CutPt> cuts;
+    faces.clear();
+    for (const fr::Face &f : full.faces) {
+      const bool mineL = part[f.eL] == r, mineR = f.eR >= 0 && part[f.eR] == r;
+      if (f.eR < 0 || (mineL && mineR)) {
+        if (!mineL) continue;
+        fr::Face g = f;
+        g.eL = local[f.eL];
+        if (f.eR >= 0) g.eR = local[f.eR];
+        faces.push_back(std::move(g));
+      } else if (mineL || mineR) {
+        for (int j = 0; j < nPF; j++) {
+          if (mineL)
+            cuts.push_back({part[f.eR], (f.locL * nPF + j) * E + local[f.eL], 1});
+          else
+            cuts.push_back({part[f.eL], f.fptR[j] * E + local[f.eR], 0});
+        }
+      }
+    }
+    std::stable_sort(cuts.begin(), cuts.end(), [](const CutPt &a, const CutPt &b) { return a.peer < b.peer; });
+    stream = st;
+    ownStream = false;
+    if (!setup_device()) return false;
+    if (!cuts.empty()) {
+      const size_t n = cuts.size();
+      std::vector<int> sl(n), lf(n);
+      std::vector<double> nv(n * nDims), da(n);
+      cutPeer.resize(n);
+      for (size_t i = 0; i < n; i++) {
+        sl[i] = cuts[i].slot;
+        lf[i] = cuts[i].left;
+        cutPeer[i] = cuts[i].peer;
+        for (int d = 0; d < nDims; d++) nv[i * nDims + d] = geo.norm_fpts[(size_t)sl[i] * nDims + d];
+        da[i] = geo.dA_fpts[sl[i]];
+      }
+      int *dsl, *dlf;
+      double *dnv, *dda, *snd, *rcv;
+      if (!upload(dsl, sl) || !upload(dlf, lf) || !upload(dnv, nv) || !upload(dda, da) || !alloc(snd, n * nF) ||
+          !alloc(rcv, n * nF))
+        return false;
+      cut.n = (int)n;
+      cut.slot = dsl;
+      cut.left = dlf;
+      cut.nrm = dnv;
+      cut.dA = dda;
+      cut.send = snd;
+      cut.recv = rcv;
+    }
+    return sync();
+  }
+
   // rows [nS] of m elements: dst[s][dOff..dOff+m) = src[s][sOff..sOff+m), all
   // fields, arrays of dE / sE elements per row
   template <typename T>
@@ -1326,6 +1492,8 @@ struct fr_case {
     launches++;
     frk::launch_element_dt_min(nS, nFp, nPF, E, detJ, wSpt, wSurf, waveSp, dA, in.CFL * fr::cfl_limit(in.order),
                                eleDt, dtBits, dtCount, dt, stream);
+    // a part on its own rank: the minimum over the ranks (solver.cpp:462-465)
+    if (comm && nccl_api().allReduce(dt, dt, 1, ncclDouble, ncclMin, comm, stream) != ncclSuccess) ncclOk = false;
   }
 
   // Everything of a stage before the element kernel: the common flux Fn (and,
@@ -1351,8 +1519,13 @@ struct fr_case {
       return;
     }
     if (!in.viscous) {
+      if (comm && cut.n > 0) exchange_nccl();
       frk::launch_faces_inviscid(nDims, ft, Ufpts, Fn, wave_out(), ph, stream);
       launches += nkInv;
+      if (cut.n > 0) {
+        frk::launch_faces_cut<double>(nDims, cut, Ufpts, Fn, wave_out(), ph, stream);
+        launches++;
+      }
       return;
     }
     frk::launch_faces_ldg(nDims, ft, Ufpts, dUc, ph, stream);
@@ -1431,28 +1604,33 @@ struct fr_case {
   }
   // one element-kernel launch of an RK stage in the working precision;
   // divF of the stage is kept when keepDivF (into divF[0])
+  frk::ElemArgs stage_args64(int mode, int stage, double rka, double rkb, bool keepDivF, bool pmgSource) {
+    frk::ElemArgs a = elem_args();
+    a.mode = mode;
+    a.stage = stage;
+    a.rka_next = rka;
+    a.rkb = rkb;
+    a.divF_out = keepDivF ? divF[0] : nullptr;
+    a.src = pmgSource ? src : nullptr;
+    a.Ufpts_out = Ufpts;
+    return a;
+  }
+  frk::ElemArgsT<float> stage_args32(int mode, int stage, double rka, double rkb, bool keepDivF, bool pmgSource) {
+    frk::ElemArgsT<float> a = elem_args32();
+    a.mode = mode;
+    a.stage = stage;
+    a.rka_next = rka;
+    a.rkb = rkb;
+    a.divF_out = keepDivF ? f32.divF[0] : nullptr;
+    a.src = pmgSource ? src32 : nullptr;
+    a.Ufpts_out = f32.Ufpts;
+    return a;
+  }
   void element_stage(int mode, int stage, double rka, double rkb, bool keepDivF, bool pmgSource) {
-    if (!mixed) {
-      frk::ElemArgs a = elem_args();
-      a.mode = mode;
-      a.stage = stage;
-      a.rka_next = rka;
-      a.rkb = rkb;
-      a.divF_out = keepDivF ? divF[0] : nullptr;
-      a.src = pmgSource ? src : nullptr;
-      a.Ufpts_out = Ufpts;
-      element(a);
-    } else {
-      frk::ElemArgsT<float> a = elem_args32();
-      a.mode = mode;
-      a.stage = stage;
-      a.rka_next = rka;
-      a.rkb = rkb;
-      a.divF_out = keepDivF ? f32.divF[0] : nullptr;
-      a.src = pmgSource ? src32 : nullptr;
-      a.Ufpts_out = f32.Ufpts;
-      element32(a);
-    }
+    if (!mixed)
+      element(stage_args64(mode, stage, rka, rkb, keepDivF, pmgSource));
+    else
+      element32(stage_args32(mode, stage, rka, rkb, keepDivF, pmgSource));
   }
 
   bool calc_residual(int step) {
@@ -1584,6 +1762,15 @@ struct fr_case {
   bool timedOut = false;
 };
 
+namespace {
+// launch policy of a case's calls: PDL on for small cases, restored on exit
+struct PdlScope {
+  bool prev;
+  explicit PdlScope(const fr_case *c) : prev(frk::pdl_enabled()) { frk::set_pdl(c && c->usePdl); }
+  ~PdlScope() { frk::set_pdl(prev); }
+};
+}  // namespace
+
 // Many independent cases advanced together: same-order cases are merged into
 // one group case (elements concatenated, faces offset), so each RK stage is
 // one face launch and one element launch per order present, and a whole step
@@ -1596,16 +1783,379 @@ struct fr_batch {
   std::vector<std::vector<int>> groupMembers;     // member indices per group
   std::vector<std::vector<int>> groupOffsets;     // element offset of each member
   long long steps = 0;
+
+  // Many-order form (FR_BATCH_MANY_ORDER): one face launch and one
+  // persistent element launch per RK stage for all groups, on one stream
+  // (the first group's), a whole step replayed as one CUDA graph.  The
+  // merged-group form (FR_BATCH_GROUPS) runs each group's own step graph on
+  // its own stream.  fr_batch_create times both and keeps the faster.
+  int form = FR_BATCH_GROUPS;
+  float formMs[2] = {-1.0f, -1.0f};  // ms per step measured at creation
+  unsigned int *ctr = nullptr;        // work counters of the element launch
+  std::vector<cudaStream_t> ownStreams;
+  cudaGraphExec_t mgraph = nullptr;
+
+  ~fr_batch() {
+    if (!groups.empty()) cudaStreamSynchronize(ownStreams.empty() ? groups[0]->stream : ownStreams[0]);
+    if (mgraph) cudaGraphExecDestroy(mgraph);
+    if (ctr) cudaFree(ctr);
+    // the groups own their streams again before they are released
+    for (size_t g = 0; g < groups.size() && g < ownStreams.size(); g++) groups[g]->stream = ownStreams[g];
+  }
+
+  bool many_order_capable() const {
+    if (groups.empty() || (int)groups.size() > frk::kMaxOrderGroups) return false;
+    for (auto &g : groups)
+      if (!g->useTp || g->in.viscous || g->nDims != groups[0]->nDims || g->mixed != groups[0]->mixed) return false;
+    return true;
+  }
+  void use_streams(bool shared) {
+    for (size_t g = 0; g < groups.size(); g++) groups[g]->stream = shared ? ownStreams[0] : ownStreams[g];
+  }
+  template <typename R>
+  void many_faces() {
+    frk::MultiFaceArgsT<R> m;
+    m.nGroups = (int)groups.size();
+    for (int gi = 0; gi < m.nGroups; gi++) {
+      fr_case &g = *groups[gi];
+      if constexpr (std::is_same<R, double>::value) {
+        m.ft[gi] = g.ft;
+        m.Uf[gi] = g.Ufpts;
+        m.Fn[gi] = g.Fn;
+      } else {
+        m.ft[gi] = g.f32.ft;
+        m.Uf[gi] = g.f32.Ufpts;
+        m.Fn[gi] = g.f32.Fn;
+      }
+      m.wave[gi] = g.wave_out();
+      m.istart[gi + 1] = m.istart[gi] + m.ft[gi].nInterior;
+      m.bstart[gi + 1] = m.bstart[gi] + (m.ft[gi].n - m.ft[gi].nInterior);
+      g.launches++;  // counted once per group: the launch does every group's faces
+    }
+    frk::launch_faces_multi<R>(groups[0]->nDims, m, groups[0]->ph, ownStreams[0]);
+  }
+  template <typename R>
+  void many_elements(int mode, int stage, double rka, double rkb, bool keepDivF, bool finalStage) {
+    frk::MultiElemArgsT<R> m;
+    m.nGroups = (int)groups.size();
+    for (int gi = 0; gi < m.nGroups; gi++) {
+      fr_case &g = *groups[gi];
+      if constexpr (std::is_same<R, double>::value) {
+        m.a[gi] = g.stage_args64(mode, stage, rka, rkb, keepDivF, false);
+        m.t[gi] = g.tp;
+      } else {
+        m.a[gi] = g.stage_args32(mode, stage, rka, rkb, keepDivF, false);
+        m.t[gi] = g.f32.tp;
+      }
+      m.order[gi] = g.in.order;
+      const int eb = frk::tp_elems_per_block<R>(g.nDims, g.in.order);
+      m.start[gi + 1] = m.start[gi] + (g.E + eb - 1) / eb;
+      m.timeAcc[gi] = g.timeAcc;
+      g.launches++;
+    }
+    m.total = m.start[m.nGroups];
+    m.next = ctr;
+    m.done = ctr + 1;
+    m.finalStage = finalStage ? 1 : 0;
+    frk::launch_element_stage_multi<R>(groups[0]->nDims, m, ownStreams[0]);
+  }
+  // solver::update (src/solver.cpp:319-363) for every group at once
+  template <typename R>
+  void many_step() {
+    fr_case &g0 = *groups[0];
+    const int nRK = g0.nRK;
+    const bool jameson = g0.in.timeType >= 5;
+    for (auto &g : groups)
+      if (!g->fptsFresh) g->extrapolate();
+    for (int st = 0; st < nRK - 1; st++) {
+      many_faces<R>();
+      many_elements<R>(jameson ? frk::MODE_JAMESON : frk::MODE_RK_STAGE, st, g0.in.RKa[st + 1],
+                       jameson ? 0.0 : g0.in.RKb[st], st == 0, false);
+    }
+    many_faces<R>();
+    if (jameson)
+      many_elements<R>(frk::MODE_JAMESON, nRK - 1, g0.in.RKa[nRK], 0.0, nRK == 1, true);
+    else
+      many_elements<R>(frk::MODE_RK_FINAL, nRK - 1, 0.0, g0.in.RKb[nRK - 1], nRK == 1, true);
+    for (auto &g : groups) g->fptsFresh = true;
+  }
+  bool many_run(int n) {
+    if (n <= 0) return true;
+    for (auto &g : groups)
+      if (!g->sync()) return fail(g->err);
+    use_streams(true);
+    const bool f32 = groups[0]->mixed;
+    // a step with no stale traces is the steady one: capture it once
+    for (auto &g : groups)
+      if (!g->fptsFresh) {
+        f32 ? many_step<float>() : many_step<double>();
+        for (auto &h : groups) h->iter++;
+        n--;
+        break;
+      }
+    bool ok = true;
+    if (n > 0 && !mgraph) {
+      cudaGraph_t gr;
+      std::vector<long long> l0;
+      for (auto &g : groups) l0.push_back(g->launches);
+      if (cudaStreamBeginCapture(ownStreams[0], cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        use_streams(false);
+        return fail("begin capture");
+      }
+      f32 ? many_step<float>() : many_step<double>();
+      for (size_t i = 0; i < groups.size(); i++) {
+        graphLaunches.push_back(groups[i]->launches - l0[i]);
+        groups[i]->launches = l0[i];
+      }
+      if (cudaStreamEndCapture(ownStreams[0], &gr) != cudaSuccess) ok = fail("end capture");
+      if (ok && cudaGraphInstantiate(&mgraph, gr, 0) != cudaSuccess) ok = fail("graph instantiate");
+      if (ok) cudaGraphDestroy(gr);
+    }
+    for (int i = 0; ok && i < n; i++) {
+      if (cudaGraphLaunch(mgraph, ownStreams[0]) != cudaSuccess) ok = fail("graph launch");
+      for (size_t gi = 0; gi < groups.size(); gi++) {
+        groups[gi]->iter++;
+        groups[gi]->launches += graphLaunches[gi];
+      }
+    }
+    use_streams(false);
+    // every group's own stream waits for the steps issued on the first one
+    cudaEvent_t ev;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail("event");
+    cudaEventRecord(ev, ownStreams[0]);
+    for (size_t i = 1; i < ownStreams.size(); i++) cudaStreamWaitEvent(ownStreams[i], ev, 0);
+    cudaEventDestroy(ev);
+    return ok;
+  }
+  std::vector<long long> graphLaunches;
+  bool groups_run(int n) {
+    for (auto &g : groups) {
+      PdlScope pdlScope(g.get());
+      if (!g->run(n)) return fail(g->err);
+    }
+    return true;
+  }
+  bool run(int n) { return form == FR_BATCH_MANY_ORDER ? many_run(n) : groups_run(n); }
+  bool fail(const std::string &m) {
+    err = m;
+    return false;
+  }
+
+  // Times `steps` steps of each form on the batch's own state and keeps the
+  // faster; the state and time are restored afterwards, so the choice
+  // changes the speed only.
+  bool autotune_form(int steps) {
+    if (!many_order_capable()) return true;
+    struct Saved {
+      void *U = nullptr, *C = nullptr;
+      double t = 0.0;
+      long long iter = 0;
+    };
+    std::vector<Saved> sv(groups.size());
+    auto bytesU = [&](fr_case &g) { return (size_t)g.nS * g.E * g.nF * (g.mixed ? sizeof(float) : sizeof(double)); };
+    bool ok = true;
+    for (size_t i = 0; ok && i < groups.size(); i++) {
+      fr_case &g = *groups[i];
+      if (!g.sync() || cudaMalloc(&sv[i].U, bytesU(g)) != cudaSuccess ||
+          (g.mixed && cudaMalloc(&sv[i].C, bytesU(g)) != cudaSuccess)) {
+        ok = fail("autotune: state copy");
+        break;
+      }
+      cudaMemcpy(sv[i].U, g.mixed ? (void *)g.f32.U : (void *)g.U, bytesU(g), cudaMemcpyDeviceToDevice);
+      if (g.mixed) cudaMemcpy(sv[i].C, g.f32.comp, bytesU(g), cudaMemcpyDeviceToDevice);
+      cudaMemcpy(&sv[i].t, g.timeAcc, sizeof(double), cudaMemcpyDeviceToHost);
+      sv[i].iter = g.iter;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ok && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) ok = fail("events");
+    for (int f = 0; ok && f < 2; f++) {
+      form = f;
+      if (!run(1)) {
+        ok = false;
+        break;
+      }
+      for (auto &g : groups) g->sync();
+      cudaEventRecord(e0, ownStreams[0]);
+      // the groups' own streams join the first one, so e1 closes every group's steps
+      for (size_t i = 1; i < groups.size(); i++) cudaStreamWaitEvent(ownStreams[i], e0, 0);
+      if (!run(steps)) {
+        ok = false;
+        break;
+      }
+      for (size_t i = 1; i < groups.size(); i++) {
+        cudaEvent_t ev;
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        cudaEventRecord(ev, ownStreams[i]);
+        cudaStreamWaitEvent(ownStreams[0], ev, 0);
+        cudaEventDestroy(ev);
+      }
+      cudaEventRecord(e1, ownStreams[0]);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        ok = fail("autotune: sync");
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      formMs[f] = ms / steps;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    form = (ok && formMs[1] > 0.0f && formMs[1] < formMs[0]) ? FR_BATCH_MANY_ORDER : FR_BATCH_GROUPS;
+    for (size_t i = 0; i < groups.size(); i++) {
+      fr_case &g = *groups[i];
+      if (sv[i].U) {
+        g.sync();
+        cudaMemcpy(g.mixed ? (void *)g.f32.U : (void *)g.U, sv[i].U, bytesU(g), cudaMemcpyDeviceToDevice);
+        if (g.mixed) cudaMemcpy(g.f32.comp, sv[i].C, bytesU(g), cudaMemcpyDeviceToDevice);
+        cudaMemcpy(g.timeAcc, &sv[i].t, sizeof(double), cudaMemcpyHostToDevice);
+        g.iter = sv[i].iter;
+        g.fptsFresh = false;
+      }
+      cudaFree(sv[i].U);
+      cudaFree(sv[i].C);
+    }
+    return ok;
+  }
+};
+
+// One case split into parts by a partition of its elements, all parts on
+// one device and one stream, exchanging the traces of the faces the
+// partition cuts through device buffers at every stage: the stepping of the
+// reference's MPI runs (mpiFace::communicate / getRightState,
+// src/mpiFace.cpp:122-175; the dt MPI_Allreduce, src/solver.cpp:462-465)
+// with device-to-device copies in place of the messages.
+struct fr_shard {
+  std::string err;
+  std::unique_ptr<fr_case> full;  // host-side setup of the whole case
+  std::vector<int> part;          // part of every element
+  std::vector<std::vector<int>> owned;
+  std::vector<std::unique_ptr<fr_case>> parts;
+  struct Copy {
+    int dst, src;
+    long long dOff, sOff, n;  // in cut points
+  };
+  std::vector<Copy> copies;
+  std::vector<double *> dts;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  long long iter = 0;
+  bool stateSet = false;
+
+  ~fr_shard() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    parts.clear();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  bool fail(const std::string &m) {
+    err = m;
+    return false;
+  }
+
+  // the traces of every part's cut points into its send buffer, then each
+  // part's receive segment from each peer copied from that peer's send segment
+  void exchange() {
+    for (auto &p : parts)
+      if (p->cut.n > 0) {
+        frk::launch_pack_cut<double>(p->nF, p->cut, p->Ufpts, stream);
+        p->launches++;
+      }
+    const int nF = parts[0]->nF;
+    for (const Copy &c : copies)
+      cudaMemcpyAsync(parts[c.dst]->cut.recv + c.dOff * nF, parts[c.src]->cut.send + c.sOff * nF,
+                      (size_t)c.n * nF * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+  }
+  void global_dt() {
+    for (auto &p : parts) p->calc_dt_dev();
+    frk::launch_min_dt(dts.data(), (int)dts.size(), stream);
+  }
+  bool residual(int step) {
+    for (auto &p : parts)
+      if (!p->fptsFresh) p->extrapolate();
+    exchange();
+    for (auto &p : parts) {
+      p->faces_pass();
+      frk::ElemArgs a = p->elem_args();
+      a.mode = frk::MODE_RESIDUAL;
+      a.divF_out = p->divF[step];
+      p->element(a);
+    }
+    for (auto &p : parts)
+      if (!p->cuda_ok("shard residual")) return fail(p->err);
+    return true;
+  }
+  // solver::update (src/solver.cpp:319-363) over all parts, stage by stage
+  bool step_once() {
+    fr_case &p0 = *parts[0];
+    const int nRK = p0.nRK;
+    const bool jameson = p0.in.timeType >= 5;
+    for (auto &p : parts)
+      if (!p->fptsFresh) p->extrapolate();
+    for (int st = 0; st < nRK - 1; st++) {
+      if (st == 0 && p0.in.dtType != 0) global_dt();
+      exchange();
+      for (auto &p : parts) {
+        p->faces_pass();
+        p->element_stage(jameson ? frk::MODE_JAMESON : frk::MODE_RK_STAGE, st, p->in.RKa[st + 1],
+                         jameson ? 0.0 : p->in.RKb[st], st == 0, false);
+      }
+    }
+    exchange();
+    for (auto &p : parts) p->faces_pass();
+    if (nRK == 1 && p0.in.dtType != 0) global_dt();
+    for (auto &p : parts) {
+      if (jameson)
+        p->element_stage(frk::MODE_JAMESON, nRK - 1, p->in.RKa[nRK], 0.0, nRK == 1, false);
+      else
+        p->element_stage(frk::MODE_RK_FINAL, nRK - 1, 0.0, p->in.RKb[nRK - 1], nRK == 1, false);
+      frk::launch_add_time(p->dt, p->timeAcc, stream);
+      p->launches++;
+      p->fptsFresh = true;
+    }
+    return true;
+  }
+  void set_iter(long long it) {
+    iter = it;
+    for (auto &p : parts) p->iter = it;
+  }
+  // n driver steps; after the first (which initialises the wave speeds) the
+  // step of every part is replayed from one CUDA graph
+  bool run(int n) {
+    while (n > 0 && iter < 1) {
+      set_iter(iter + 1);
+      if (!step_once()) return false;
+      n--;
+    }
+    if (n <= 0) return sync();
+    if (!graph) {
+      cudaGraph_t g;
+      const long long save = iter;
+      set_iter(2);  // steady-state branch
+      if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail("begin capture");
+      step_once();
+      if (cudaStreamEndCapture(stream, &g) != cudaSuccess) return fail("end capture");
+      set_iter(save);
+      if (cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail("graph instantiate");
+      }
+      cudaGraphDestroy(g);
+    }
+    for (int i = 0; i < n; i++) {
+      set_iter(iter + 1);
+      if (cudaGraphLaunch(graph, stream) != cudaSuccess) return fail("graph launch");
+    }
+    return sync();
+  }
+  bool sync() {
+    for (auto &p : parts)
+      if (!p->sync()) return fail(p->err);
+    return true;
+  }
 };
 
 namespace {
-
-// launch policy of a case's calls: PDL on for small cases, restored on exit
-struct PdlScope {
-  bool prev;
-  explicit PdlScope(const fr_case *c) : prev(frk::pdl_enabled()) { frk::set_pdl(c && c->usePdl); }
-  ~PdlScope() { frk::set_pdl(prev); }
-};
 
 int status_of(fr_case *c, bool ok, int code = FR_ERR_CUDA) {
   if (ok) return FR_OK;
@@ -2236,23 +2786,50 @@ int fr_batch_create(fr_case *const *cases, int n, fr_batch **out) {
       (*out)->err = g->err;
       return FR_ERR_CUDA;
     }
+    b->ownStreams.push_back(g->stream);
     b->groups.push_back(std::move(g));
     b->groupMembers.push_back(idx);
     b->groupOffsets.push_back(offs);
+  }
+  if (b->many_order_capable()) {
+    if (cudaMalloc(&b->ctr, 2 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMemset(b->ctr, 0, 2 * sizeof(unsigned int)) != cudaSuccess) {
+      b->err = "work counters";
+      *out = b.release();
+      return FR_ERR_CUDA;
+    }
+    if (!b->autotune_form(3)) {
+      *out = b.release();
+      return FR_ERR_CUDA;
+    }
   }
   *out = b.release();
   return FR_OK;
 }
 
+int fr_batch_form(fr_batch *b, int *form, float *ms_groups, float *ms_many_order) {
+  if (!b) return FR_ERR_ARG;
+  if (form) *form = b->form;
+  if (ms_groups) *ms_groups = b->formMs[0];
+  if (ms_many_order) *ms_many_order = b->formMs[1];
+  return FR_OK;
+}
+
+int fr_batch_set_form(fr_batch *b, int form) {
+  if (!b || (form != FR_BATCH_GROUPS && form != FR_BATCH_MANY_ORDER)) return FR_ERR_ARG;
+  if (form == FR_BATCH_MANY_ORDER && !b->many_order_capable()) {
+    b->err = "the many-order form needs inviscid tensor-product groups of one precision (at most 6 orders)";
+    return FR_ERR_UNSUPPORTED;
+  }
+  for (auto &g : b->groups)
+    if (!g->sync()) return FR_ERR_CUDA;
+  b->form = form;
+  return FR_OK;
+}
+
 int fr_batch_run(fr_batch *b, int nsteps) {
   if (!b || nsteps < 0) return FR_ERR_ARG;
-  for (auto &g : b->groups) {
-    PdlScope pdlScope(g.get());
-    if (!g->run(nsteps)) {
-      b->err = g->err;
-      return FR_ERR_CUDA;
-    }
-  }
+  if (!b->run(nsteps)) return FR_ERR_CUDA;
   for (auto &g : b->groups)
     if (!g->sync()) {
       b->err = g->err;
@@ -2654,6 +3231,289 @@ int fr_shard_plan(fr_case *c, int nparts, int rank, int *part, int *n_owned, lon
     std::copy(peer.begin(), peer.end(), halo_peer);
     std::copy(slot.begin(), slot.end(), halo_slot);
   }
+  return FR_OK;
+}
+
+int fr_shard_create(const char *deck_path, const fr_setup_opts *opts, int nparts, fr_shard **out) {
+  if (!deck_path || !out || nparts < 1 || nparts > frk::kMaxParts) return FR_ERR_ARG;
+  *out = nullptr;
+  fr_setup_opts o;
+  if (opts)
+    o = *opts;
+  else
+    fr_setup_opts_default(&o);
+  const int device = o.device;
+  if (device < 0) return FR_ERR_ARG;
+  std::unique_ptr<fr_shard> sh(new fr_shard());
+  fr_setup_opts ho = o;
+  ho.device = -1;  // the whole case on the host only: mesh, faces, metrics, operators
+  fr_case *f = nullptr;
+  int st = create_common(deck_path, nullptr, &ho, &f);
+  sh->full.reset(f);
+  if (st != FR_OK) {
+    sh->err = f ? f->err : "setup failed";
+    *out = sh.release();
+    return st;
+  }
+  fr_case &F = *sh->full;
+  if (o.precision != FR_PREC_FP64 || F.in.viscous || F.in.PMG || F.in.motion) {
+    sh->err = "sharded cases: plain form (FP64), inviscid, static mesh, no P-multigrid";
+    *out = sh.release();
+    return FR_ERR_UNSUPPORTED;
+  }
+  if (nparts > F.E || !fr::partition_elements(F.mesh, nparts, sh->part, sh->err)) {
+    if (sh->err.empty()) sh->err = "more parts than elements";
+    *out = sh.release();
+    return FR_ERR_ARG;
+  }
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&sh->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    sh->err = "stream create";
+    *out = sh.release();
+    return FR_ERR_CUDA;
+  }
+  sh->owned.assign(nparts, {});
+  for (int e = 0; e < F.E; e++) sh->owned[sh->part[e]].push_back(e);
+  for (int r = 0; r < nparts; r++) {
+    std::unique_ptr<fr_case> p(new fr_case());
+    if (!p->split_from(F, sh->part, r, sh->stream)) {
+      sh->err = "part " + std::to_string(r) + ": " + p->err;
+      *out = sh.release();
+      return FR_ERR_CUDA;
+    }
+    sh->dts.push_back(p->dt);
+    sh->parts.push_back(std::move(p));
+  }
+  // copies: part r's segment from peer q <- q's segment for r (same length)
+  auto segment = [&](int r, int q, long long &off, long long &n) {
+    const auto &cp = sh->parts[r]->cutPeer;
+    auto lo = std::lower_bound(cp.begin(), cp.end(), q), hi = std::upper_bound(cp.begin(), cp.end(), q);
+    off = lo - cp.begin();
+    n = hi - lo;
+  };
+  for (int r = 0; r < nparts; r++)
+    for (int q = 0; q < nparts; q++) {
+      if (q == r) continue;
+      long long dOff, n1, sOff, n2;
+      segment(r, q, dOff, n1);
+      segment(q, r, sOff, n2);
+      if (n1 != n2) {
+        sh->err = "cut lists of two parts disagree";
+        *out = sh.release();
+        return FR_ERR_SETUP;
+      }
+      if (n1 > 0) sh->copies.push_back({r, q, dOff, sOff, n1});
+    }
+  *out = sh.release();
+  return FR_OK;
+}
+
+int fr_part_create(const char *deck_path, const fr_setup_opts *opts, int nparts, int rank, void *nccl_comm,
+                   fr_case **out) {
+  if (!deck_path || !out || nparts < 1 || rank < 0 || rank >= nparts || (nparts > 1 && !nccl_comm))
+    return FR_ERR_ARG;
+  *out = nullptr;
+  fr_setup_opts o;
+  if (opts)
+    o = *opts;
+  else
+    fr_setup_opts_default(&o);
+  if (o.device < 0) return FR_ERR_ARG;
+  fr_setup_opts ho = o;
+  ho.device = -1;
+  fr_case *f = nullptr;
+  int st = create_common(deck_path, nullptr, &ho, &f);
+  std::unique_ptr<fr_case> full(f);
+  std::unique_ptr<fr_case> p(new fr_case());
+  auto give = [&](int code, const std::string &m) {
+    p->err = m;
+    *out = p.release();
+    return code;
+  };
+  if (st != FR_OK) return give(st, f ? f->err : "setup failed");
+  if (o.precision != FR_PREC_FP64 || full->in.viscous || full->in.PMG || full->in.motion)
+    return give(FR_ERR_UNSUPPORTED, "parts: plain form (FP64), inviscid, static mesh, no P-multigrid");
+  if (nparts > 1 && !nccl_api().ok) return give(FR_ERR_UNSUPPORTED, "libnccl.so.2 not found");
+  std::vector<int> part;
+  std::string e;
+  if (nparts > full->E || !fr::partition_elements(full->mesh, nparts, part, e)) return give(FR_ERR_ARG, e);
+  cudaStream_t stream = nullptr;
+  if (cudaSetDevice(o.device) != cudaSuccess || cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess)
+    return give(FR_ERR_CUDA, "stream create");
+  p->ownStream = true;
+  p->ownedStream = stream;
+  if (!p->split_from(*full, part, rank, stream)) return give(FR_ERR_CUDA, p->err);
+  p->opts.no_pdl = o.no_pdl;  // a part on its own stream may use PDL like any case
+  p->usePdl = false;          // NCCL calls sit between its kernels
+  p->comm = static_cast<ncclComm_t>(nccl_comm);
+  for (size_t i = 0; i < p->cutPeer.size();) {
+    size_t j = i;
+    while (j < p->cutPeer.size() && p->cutPeer[j] == p->cutPeer[i]) j++;
+    p->segPeer.push_back(p->cutPeer[i]);
+    p->segOff.push_back((long long)i);
+    p->segCount.push_back((long long)(j - i));
+    i = j;
+  }
+  *out = p.release();
+  return FR_OK;
+}
+
+int fr_part_nccl_ok(fr_case *c) {
+  if (!c) return FR_ERR_ARG;
+  return c->ncclOk ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_nccl_unique_id(void *id128) {
+  if (!id128) return FR_ERR_ARG;
+  if (!nccl_api().ok) return FR_ERR_UNSUPPORTED;
+  ncclUniqueId u;
+  if (nccl_api().uniqueId(&u) != ncclSuccess) return FR_ERR_CUDA;
+  std::memcpy(id128, &u, sizeof(u));
+  return FR_OK;
+}
+
+int fr_nccl_comm_init(int nranks, const void *id128, int rank, int device, void **comm) {
+  if (!id128 || !comm || nranks < 1 || rank < 0 || rank >= nranks) return FR_ERR_ARG;
+  if (!nccl_api().ok) return FR_ERR_UNSUPPORTED;
+  if (cudaSetDevice(device) != cudaSuccess) return FR_ERR_CUDA;
+  ncclUniqueId u;
+  std::memcpy(&u, id128, sizeof(u));
+  ncclComm_t c = nullptr;
+  if (nccl_api().initRank(&c, nranks, u, rank) != ncclSuccess) return FR_ERR_CUDA;
+  *comm = c;
+  return FR_OK;
+}
+
+int fr_nccl_comm_destroy(void *comm) {
+  if (!comm) return FR_ERR_ARG;
+  if (!nccl_api().ok) return FR_ERR_UNSUPPORTED;
+  return nccl_api().destroy(static_cast<ncclComm_t>(comm)) == ncclSuccess ? FR_OK : FR_ERR_CUDA;
+}
+
+const char *fr_shard_last_error(const fr_shard *s) { return s ? s->err.c_str() : "null shard"; }
+
+void fr_shard_destroy(fr_shard *s) { delete s; }
+
+int fr_shard_info(fr_shard *s, int *nparts, int *owned, long long *cut_points) {
+  if (!s || !nparts) return FR_ERR_ARG;
+  *nparts = (int)s->parts.size();
+  for (size_t r = 0; r < s->parts.size(); r++) {
+    if (owned) owned[r] = s->parts[r]->E;
+    if (cut_points) cut_points[r] = s->parts[r]->cut.n;
+  }
+  return FR_OK;
+}
+
+namespace {
+// whole-case array [nS][E][nF] <-> part r's [nS][E_r][nF]
+void to_part(const fr_shard &s, int r, const double *U, std::vector<double> &out) {
+  const fr_case &p = *s.parts[r];
+  const int Ef = s.full->E, nS = p.nS, nF = p.nF;
+  const auto &ow = s.owned[r];
+  out.resize((size_t)nS * p.E * nF);
+  for (int sp = 0; sp < nS; sp++)
+    for (int el = 0; el < p.E; el++)
+      std::memcpy(&out[((size_t)sp * p.E + el) * nF], &U[((size_t)sp * Ef + ow[el]) * nF], nF * sizeof(double));
+}
+void from_part(const fr_shard &s, int r, const std::vector<double> &in, double *U) {
+  const fr_case &p = *s.parts[r];
+  const int Ef = s.full->E, nS = p.nS, nF = p.nF;
+  const auto &ow = s.owned[r];
+  for (int sp = 0; sp < nS; sp++)
+    for (int el = 0; el < p.E; el++)
+      std::memcpy(&U[((size_t)sp * Ef + ow[el]) * nF], &in[((size_t)sp * p.E + el) * nF], nF * sizeof(double));
+}
+}  // namespace
+
+int fr_shard_set_state(fr_shard *s, const double *U, size_t count) {
+  if (!s || !U) return FR_ERR_ARG;
+  const fr_case &F = *s->full;
+  if (count != (size_t)F.nS * F.E * F.nF) return FR_ERR_ARG;
+  frk::set_pdl(false);
+  std::vector<double> buf;
+  for (size_t r = 0; r < s->parts.size(); r++) {
+    to_part(*s, (int)r, U, buf);
+    if (!s->parts[r]->set_state_host(buf.data()) || !s->parts[r]->sync()) {
+      s->err = s->parts[r]->err;
+      return FR_ERR_CUDA;
+    }
+  }
+  s->stateSet = true;
+  return FR_OK;
+}
+
+int fr_shard_get_state(fr_shard *s, double *U, size_t count) {
+  if (!s || !U) return FR_ERR_ARG;
+  const fr_case &F = *s->full;
+  if (count != (size_t)F.nS * F.E * F.nF) return FR_ERR_ARG;
+  std::vector<double> buf;
+  for (size_t r = 0; r < s->parts.size(); r++) {
+    fr_case &p = *s->parts[r];
+    buf.resize((size_t)p.nS * p.E * p.nF);
+    if (!p.sync() || cudaMemcpy(buf.data(), p.U, buf.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      s->err = "state read-back failed";
+      return FR_ERR_CUDA;
+    }
+    from_part(*s, (int)r, buf, U);
+  }
+  return FR_OK;
+}
+
+int fr_shard_set_dt(fr_shard *s, double dt) {
+  if (!s || !(dt > 0)) return FR_ERR_ARG;
+  for (auto &p : s->parts)
+    if (fr_set_dt(p.get(), dt) != FR_OK) {
+      s->err = p->err;
+      return FR_ERR_CUDA;
+    }
+  return FR_OK;
+}
+
+int fr_shard_calc_residual(fr_shard *s, int step) {
+  if (!s) return FR_ERR_ARG;
+  if (!s->stateSet) {
+    s->err = "no state set";
+    return FR_ERR_STATE;
+  }
+  if (step < 0 || step >= s->parts[0]->nRK) return FR_ERR_ARG;
+  frk::set_pdl(false);
+  return s->residual(step) && s->sync() ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_shard_get_residual(fr_shard *s, int step, double *divF, size_t count) {
+  if (!s || !divF || step < 0 || step >= s->parts[0]->nRK) return FR_ERR_ARG;
+  const fr_case &F = *s->full;
+  if (count != (size_t)F.nS * F.E * F.nF) return FR_ERR_ARG;
+  std::vector<double> buf;
+  for (size_t r = 0; r < s->parts.size(); r++) {
+    fr_case &p = *s->parts[r];
+    buf.resize((size_t)p.nS * p.E * p.nF);
+    if (!p.sync() ||
+        cudaMemcpy(buf.data(), p.divF[step], buf.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      s->err = "residual read-back failed";
+      return FR_ERR_CUDA;
+    }
+    from_part(*s, (int)r, buf, divF);
+  }
+  return FR_OK;
+}
+
+int fr_shard_run(fr_shard *s, int nsteps) {
+  if (!s || nsteps < 0) return FR_ERR_ARG;
+  if (!s->stateSet) {
+    s->err = "no state set";
+    return FR_ERR_STATE;
+  }
+  frk::set_pdl(false);
+  return s->run(nsteps) ? FR_OK : FR_ERR_CUDA;
+}
+
+int fr_shard_time(fr_shard *s, double *time, double *dt) {
+  if (!s) return FR_ERR_ARG;
+  fr_case &p = *s->parts[0];
+  if (!s->sync()) return FR_ERR_CUDA;
+  if (time) cudaMemcpy(time, p.timeAcc, sizeof(double), cudaMemcpyDeviceToHost);
+  if (dt) cudaMemcpy(dt, p.dt, sizeof(double), cudaMemcpyDeviceToHost);
   return FR_OK;
 }
 

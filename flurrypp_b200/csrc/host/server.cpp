@@ -47,6 +47,12 @@ struct Request {
   int pending = 0;  // steps issued and not yet seen complete
   int nFields = 0;
   std::vector<double> res0;
+  // FR_PREC_MIXED_REFINE: in the precision form until the residual stops
+  // falling, then in FP64
+  bool refine = false, fp32 = false;
+  int form = FR_PREC_FP64;
+  double best = 0.0;
+  int sinceBest = 0, stepsFp32 = 0;
   // result
   int status = 0;  // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
   int code = FR_OK;
@@ -82,17 +88,60 @@ struct fr_server {
     return words * sizeof(double) * 2;  // coarse P levels and tables: at most as much again
   }
 
+  static fr_case *create(Request &r, int device, int prec, int &st) {
+    fr_setup_opts o;
+    fr_setup_opts_default(&o);
+    o.device = device;
+    o.precision = prec;
+    fr_case *c = nullptr;
+    st = r.hasMesh ? fr_create_with_mesh(r.deck.c_str(), &r.mesh, &o, &c)
+                   : fr_create_from_deck(r.deck.c_str(), &o, &c);
+    return c;
+  }
+
+  // The precision form's residual stops falling at its FP32 floor (about
+  // 1e-7 of the flux terms, scaled by the operators): a request of the
+  // refining form goes on from its state in FP64.  The case is set up again
+  // in FP64 (same deck and mesh) and given the state; its coarse P-multigrid
+  // levels start as at any setup.  The request keeps its steps and its
+  // residual normalisation.
+  static constexpr int kStallChecks = 20;     // checks without a new best
+  static constexpr double kStallGain = 0.8;   // a new best is 20% below the last
+  bool to_fp64(Request &r) {
+    fr_info inf;
+    if (fr_get_info(r.c, &inf) != FR_OK) return false;
+    std::vector<double> U((size_t)inf.nSpts * inf.nEles * inf.nFields);
+    if (fr_get_state(r.c, U.data(), U.size()) != FR_OK) return false;
+    int st = FR_OK;
+    fr_case *c = create(r, device, FR_PREC_FP64, st);
+    if (st != FR_OK || fr_set_state(c, U.data(), U.size()) != FR_OK) {
+      fr_destroy(c);
+      return false;
+    }
+    fr_destroy(r.c);
+    r.c = c;
+    const size_t b = case_bytes(c);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      inflightBytes += b;
+      inflightBytes -= r.bytes;
+    }
+    r.bytes = b;
+    r.fp32 = false;
+    r.form = FR_PREC_FP64;
+    r.stepsFp32 = r.steps;
+    return true;
+  }
+
   bool admit_one() {
     // caller holds mu; setup runs without it
     long long id = queue.front();
     Request &r = *reqs[id];
-    fr_setup_opts o;
-    fr_setup_opts_default(&o);
-    o.device = device;
-    o.precision = precision;
-    fr_case *c = nullptr;
-    int st = r.hasMesh ? fr_create_with_mesh(r.deck.c_str(), &r.mesh, &o, &c)
-                       : fr_create_from_deck(r.deck.c_str(), &o, &c);
+    r.refine = precision == FR_PREC_MIXED_REFINE;
+    r.form = r.refine ? FR_PREC_MIXED : precision;
+    r.fp32 = r.form == FR_PREC_MIXED;
+    int st = FR_OK;
+    fr_case *c = create(r, device, r.form, st);
     if (st == FR_OK) st = fr_init_solution(c, r.icKind, r.icPrm.empty() ? nullptr : r.icPrm.data(), (int)r.icPrm.size());
     if (st != FR_OK) {
       r.status = 3;
@@ -186,8 +235,18 @@ struct fr_server {
         for (int k = 0; k < r.nFields; k++)
           ratio = std::max(ratio, r.res0[k] > 0 ? res[k] / r.res0[k] : 0.0);
         r.finalRatio = ratio;
-        if (ratio <= r.tol) done.push_back({id, 2});
-        else if (r.steps >= r.maxSteps) done.push_back({id, 2});
+        if (ratio <= r.tol) {
+          done.push_back({id, 2});
+        } else if (r.steps >= r.maxSteps) {
+          done.push_back({id, 2});
+        } else if (r.refine && r.fp32) {
+          if (r.best == 0.0 || ratio < kStallGain * r.best) {
+            r.best = ratio;
+            r.sinceBest = 0;
+          } else if (++r.sinceBest >= kStallChecks && !to_fp64(r)) {
+            done.push_back({id, 3});
+          }
+        }
       }
       if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
       lk.lock();
@@ -230,7 +289,8 @@ int fr_server_create(size_t budget_bytes, int max_inflight, int check_every, int
 }
 
 int fr_server_set_precision(fr_server *s, int precision) {
-  if (!s || (precision != FR_PREC_FP64 && precision != FR_PREC_MIXED)) return FR_ERR_ARG;
+  if (!s || (precision != FR_PREC_FP64 && precision != FR_PREC_MIXED && precision != FR_PREC_MIXED_REFINE))
+    return FR_ERR_ARG;
   std::lock_guard<std::mutex> lk(s->mu);
   s->precision = precision;
   return FR_OK;
@@ -278,6 +338,17 @@ int fr_server_poll(fr_server *s, long long id, int *status, double *latency_s, i
   if (steps) *steps = r.steps;
   if (res_ratio) *res_ratio = r.finalRatio;
   return r.status == 3 ? r.code : FR_OK;
+}
+
+int fr_server_poll_form(fr_server *s, long long id, int *precision, int *steps_fp32) {
+  if (!s) return FR_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return FR_ERR_ARG;
+  Request &r = *it->second;
+  if (precision) *precision = r.form;
+  if (steps_fp32) *steps_fp32 = r.fp32 ? r.steps : r.stepsFp32;
+  return FR_OK;
 }
 
 int fr_server_wait(fr_server *s, long long id, double timeout_s) {

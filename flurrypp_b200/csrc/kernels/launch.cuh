@@ -25,6 +25,40 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 // a blown-up residual reaches the host's NaN check through a max-norm.
 __device__ __forceinline__ double nan_max(double a, double b) { return (a != a || a > b) ? a : b; }
 
+// Asynchronous copy of one 8-byte (double) or 4-byte (float) word global ->
+// shared (cp.async); a thread's copies complete in commit-group order.
+template <typename R>
+__device__ __forceinline__ void cp_async_word(R *dst, const R *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(R) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most N of this thread's newest groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+inline int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+// streaming multiprocessors of device d (queried once per device)
+inline int sm_count(int d) {
+  static std::atomic<int> cache[64];
+  if (d < 0 || d >= 64) return 148;
+  int v = cache[d].load(std::memory_order_relaxed);
+  if (v > 0) return v;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+  if (v <= 0) v = 148;
+  cache[d].store(v, std::memory_order_relaxed);
+  return v;
+}
+
 // Launch policy of the calling host thread (set by the case around its
 // launch sequences, graph captures included).
 void set_pdl(bool on);

@@ -54,6 +54,36 @@ template <typename R>
 void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R *Fn, double *waveSp,
                            const Phys &ph, cudaStream_t st);
 
+// One part of a case split by a partition of its elements (emulated ranks on
+// one device, or one rank): the face points the partition cuts, each formed
+// with this part's element as the left side and the peer's trace, received
+// for every stage, as the right state (mpiFace::getRightState,
+// src/mpiFace.cpp:158-175).  Points are listed by peer part, and per peer in
+// the order both sides share (by face, then by the face's left point order),
+// so the k-th trace one side sends is the k-th the other receives.
+constexpr int kMaxParts = 64;
+template <typename R>
+struct CutTableT {
+  int n = 0;
+  const int *slot = nullptr;  // fpt*E + e of this part's side
+  const int *left = nullptr;  // 1 where this side is the face's left side in the unsplit mesh
+  const R *nrm = nullptr;     // [n][nDims] this side's unit normal
+  const R *dA = nullptr;      // [n] this side's dA
+  R *send = nullptr;          // [n][nF] this side's traces, packed for every stage
+  R *recv = nullptr;          // [n][nF] the peers' traces at the same points
+};
+
+// send[i] = U_fpts at slot[i], all fields.
+template <typename R>
+void launch_pack_cut(int nF, const CutTableT<R> &c, const R *Ufpts, cudaStream_t st);
+// Common flux at the cut points from this side's trace and recv (Rusanov,
+// or 2-D Roe), written to this side's Fn; wave speed where `left`.
+template <typename R>
+void launch_faces_cut(int nDims, const CutTableT<R> &c, const R *Ufpts, R *Fn, double *waveSp, const Phys &ph,
+                      cudaStream_t st);
+// dts[0..n) (device scalars, n <= kMaxParts) all set to their minimum.
+void launch_min_dt(double *const *dts, int n, cudaStream_t st);
+
 enum ElemMode : int {
   MODE_RESIDUAL = 0,  // calcResidual only: divF -> divF_out
   MODE_RK_STAGE = 1,  // standard RK intermediate stage (timeStepA + running timeStepB)
@@ -124,6 +154,43 @@ struct TpTablesT {
 };
 using TpTables = TpTablesT<double>;
 bool tp_supported(int nDims, int order);
+
+// Many cases of uneven order advanced by one element launch per RK stage
+// (the batch's many-order form): a persistent kernel whose CTAs take element
+// blocks of every order group from a device work counter and run the
+// tensor-product stage of that group's order on each (CTAs have the threads
+// and shared memory of the largest block).  The last CTA to finish resets the
+// counters and, on the last stage of a step, advances every group's time.
+constexpr int kMaxOrderGroups = 6;
+template <typename R>
+struct MultiElemArgsT {
+  int nGroups = 0;
+  int total = 0;                         // element blocks over all groups
+  int order[kMaxOrderGroups] = {};
+  int start[kMaxOrderGroups + 1] = {};   // first work item of each group
+  ElemArgsT<R> a[kMaxOrderGroups];
+  TpTablesT<R> t[kMaxOrderGroups];
+  unsigned int *next = nullptr, *done = nullptr;  // zero between launches
+  double *timeAcc[kMaxOrderGroups] = {};          // final stage: timeAcc += *dt per group
+  int finalStage = 0;
+};
+// The face points of all groups in one launch: interior points of group g
+// are work items istart[g] .. istart[g+1]-1, its boundary points follow all
+// interior ones at bstart[g].
+template <typename R>
+struct MultiFaceArgsT {
+  int nGroups = 0;
+  int istart[kMaxOrderGroups + 1] = {}, bstart[kMaxOrderGroups + 1] = {};
+  FaceTableT<R> ft[kMaxOrderGroups];
+  const R *Uf[kMaxOrderGroups] = {};
+  R *Fn[kMaxOrderGroups] = {};
+  double *wave[kMaxOrderGroups] = {};
+};
+template <typename R>
+void launch_element_stage_multi(int nDims, const MultiElemArgsT<R> &m, cudaStream_t st);
+template <typename R>
+void launch_faces_multi(int nDims, const MultiFaceArgsT<R> &m, const Phys &ph, cudaStream_t st);
+
 
 // TMA descriptors of the tiles the TMA element kernel moves (one row block of
 // points x EB elements of the reference layout per copy).

@@ -13,6 +13,8 @@
 // Operators are applied through their nonzero entries (Csr), which for the
 // tensor-product quad/hex operators removes the structural zeros of the
 // reference's dense cblas_dgemm without changing any sum.
+#include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "launch.cuh"
@@ -119,6 +121,7 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
 // (measured: 3-D FP64 faces 0.090 -> 0.083 ms, FP32 0.054 -> 0.050 ms).
 constexpr int kFacePpt = 2, kFaceNt = 128;
 
+
 template <int ND, typename R, int PPT>
 __global__ void __launch_bounds__(kFaceNt) k_faces_interior_ilp(int n, const int *__restrict__ slotL,
                                                            const int *__restrict__ slotR, const R *__restrict__ nrm,
@@ -193,6 +196,96 @@ __global__ void k_faces_all(int nI, int n, const int *__restrict__ slotL, const 
     face_interior<ND, R>(i, slotL, slotR, nrm, dAL, dAR, Uf, Fn, waveSp, R(ph.gamma), ND == 2 && ph.riemannType == 1);
   else
     face_boundary<ND, R>(i, slotL, slotR, nrm, dAL, Uf, Fn, waveSp, ph);
+}
+
+// Face points of many order groups in one launch: interior points of all
+// groups first (work items istart[g] ..), then their boundary points
+// (bstart[g] ..); each point as face_interior / face_boundary on its group's
+// arrays.
+template <int ND, typename R>
+__global__ void k_faces_multi(const __grid_constant__ MultiFaceArgsT<R> m, Phys ph) {
+  pdl_wait();
+  pdl_trigger();
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const int G = m.nGroups;
+  if (w < m.istart[G]) {
+    int g = 0;
+    while (g + 1 < G && w >= m.istart[g + 1]) g++;
+    const FaceTableT<R> &f = m.ft[g];
+    face_interior<ND, R>(w - m.istart[g], f.slotL, f.slotR, f.nrm, f.dAL, f.dAR, m.Uf[g], m.Fn[g], m.wave[g],
+                         R(ph.gamma), ND == 2 && ph.riemannType == 1);
+  } else if (w < m.istart[G] + m.bstart[G]) {
+    const int v = w - m.istart[G];
+    int g = 0;
+    while (g + 1 < G && v >= m.bstart[g + 1]) g++;
+    const FaceTableT<R> &f = m.ft[g];
+    face_boundary<ND, R>(f.nInterior + v - m.bstart[g], f.slotL, f.slotR, f.nrm, f.dAL, m.Uf[g], m.Fn[g], m.wave[g],
+                         ph);
+  }
+}
+
+// A part of a case split by a partition: the traces at its cut face points,
+// packed in its cut order for the peers (send[i] = U_fpts at slot[i]).
+template <typename R>
+__global__ void k_pack_cut(long long n, int nF, const int *__restrict__ slot, const R *__restrict__ Uf,
+                           R *__restrict__ send) {
+  pdl_wait();
+  pdl_trigger();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nF) return;
+  const long long i = t / nF;
+  const int k = (int)(t - i * nF);
+  send[t] = Uf[(long long)slot[i] * nF + k];
+}
+
+// Cut face point i: the common flux with this part's element as the left
+// side and the peer's trace at the same point as the right state
+// (mpiFace::getRightState, src/mpiFace.cpp:158-175, then the interior flux
+// of face::calcInviscidFlux, face.cpp:163-208), written to this side only.
+// The wave speed goes to this side only where it was the face's left side in
+// the whole mesh, as the unsplit face writes it (face.cpp:372).
+template <int ND, typename R>
+__global__ void k_faces_cut(int n, const int *__restrict__ slot, const int *__restrict__ left,
+                            const R *__restrict__ nrm, const R *__restrict__ dA, const R *__restrict__ Uf,
+                            const R *__restrict__ recv, R *__restrict__ Fn, double *__restrict__ waveSp, R gam,
+                            int roe) {
+  pdl_wait();
+  pdl_trigger();
+  constexpr int NF = ND + 2;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = slot[i];
+  R UL[NF], UR[NF], nv[ND], F[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)s * NF + k];
+#pragma unroll
+  for (int k = 0; k < NF; k++) UR[k] = recv[(long long)i * NF + k];
+#pragma unroll
+  for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
+  if (ND == 2 && roe) {
+    roe2d<R>(UL, UR, nv, gam, F);
+  } else {
+    const R ws = rusanov<ND, R>(UL, UR, nv, gam, F);
+    if (waveSp && left[i]) waveSp[s] = ws;
+  }
+  const R a = dA[i];
+#pragma unroll
+  for (int k = 0; k < NF; k++) Fn[(long long)s * NF + k] = F[k] * a;
+}
+
+// Every device scalar dt[0..n) set to their minimum (the time step of a
+// case split into parts, MPI_Allreduce(MIN) in solver::calcDt,
+// src/solver.cpp:462-465).
+struct DtPtrs {
+  double *p[kMaxParts];
+};
+__global__ void k_min_dt(DtPtrs d, int n) {
+  pdl_wait();
+  pdl_trigger();
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double m = *d.p[0];
+  for (int i = 1; i < n; i++) m = fmin(m, *d.p[i]);
+  for (int i = 0; i < n; i++) *d.p[i] = m;
 }
 
 __device__ __forceinline__ double csr_dot(const Csr &A, int row, const double *__restrict__ x,
@@ -573,8 +666,8 @@ void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R
                waveSp, ph);
     return;
   }
-  // two points per thread except 2-D FP32, where one measured faster
   if (nI > 0 && (nDims == 3 || sizeof(R) == 8)) {
+    // two points per thread except 2-D FP32, where one measured faster
     const int per = kFaceNt * kFacePpt;
     const int g = (nI + per - 1) / per;
     if (nDims == 2)
@@ -696,6 +789,43 @@ void launch_widen(long long n, const float *in, double *out, cudaStream_t st) {
   if (n > 0) launch_k(k_widen, (unsigned)((n + 255) / 256), 256, 0, st, n, in, out);
 }
 
+template <typename R>
+void launch_faces_multi(int nDims, const MultiFaceArgsT<R> &m, const Phys &ph, cudaStream_t st) {
+  const int n = m.istart[m.nGroups] + m.bstart[m.nGroups];
+  if (n <= 0) return;
+  const int b = 128, g = (n + b - 1) / b;
+  if (nDims == 2)
+    launch_k(k_faces_multi<2, R>, g, b, 0, st, m, ph);
+  else
+    launch_k(k_faces_multi<3, R>, g, b, 0, st, m, ph);
+}
+
+template <typename R>
+void launch_pack_cut(int nF, const CutTableT<R> &c, const R *Ufpts, cudaStream_t st) {
+  const long long n = (long long)c.n * nF;
+  if (n > 0) launch_k(k_pack_cut<R>, (unsigned)((n + 255) / 256), 256, 0, st, (long long)c.n, nF, c.slot, Ufpts, c.send);
+}
+
+template <typename R>
+void launch_faces_cut(int nDims, const CutTableT<R> &c, const R *Ufpts, R *Fn, double *waveSp, const Phys &ph,
+                      cudaStream_t st) {
+  if (c.n <= 0) return;
+  const int b = 128, g = (c.n + b - 1) / b;
+  if (nDims == 2)
+    launch_k(k_faces_cut<2, R>, g, b, 0, st, c.n, c.slot, c.left, c.nrm, c.dA, Ufpts, c.recv, Fn, waveSp,
+             R(ph.gamma), ph.riemannType == 1);
+  else
+    launch_k(k_faces_cut<3, R>, g, b, 0, st, c.n, c.slot, c.left, c.nrm, c.dA, Ufpts, c.recv, Fn, waveSp,
+             R(ph.gamma), 0);
+}
+
+void launch_min_dt(double *const *dts, int n, cudaStream_t st) {
+  if (n <= 1) return;
+  DtPtrs d{};
+  for (int i = 0; i < n && i < kMaxParts; i++) d.p[i] = dts[i];
+  launch_k(k_min_dt, 1, 32, 0, st, d, n < kMaxParts ? n : kMaxParts);
+}
+
 #define FR_BASE_INST(R)                                                                                        \
   template void launch_apply_op_t<R>(const Csr &, const R *, R *, long long, cudaStream_t);                   \
   template void launch_faces_inviscid<R>(int, const FaceTableT<R> &, const R *, R *, double *, const Phys &,  \
@@ -703,7 +833,11 @@ void launch_widen(long long n, const float *in, double *out, cudaStream_t st) {
   template void launch_wavesp_init<R>(int, int, int, const R *, const double *, double, double *, cudaStream_t); \
   template void launch_residual_norm<R>(int, int, int, const R *, const double *, const double *, int, double *, \
                                         cudaStream_t);                                                        \
-  template void launch_check_state<R>(int, int, int, const R *, unsigned int *, cudaStream_t);
+  template void launch_check_state<R>(int, int, int, const R *, unsigned int *, cudaStream_t);               \
+  template void launch_pack_cut<R>(int, const CutTableT<R> &, const R *, cudaStream_t);                     \
+  template void launch_faces_multi<R>(int, const MultiFaceArgsT<R> &, const Phys &, cudaStream_t);          \
+  template void launch_faces_cut<R>(int, const CutTableT<R> &, const R *, R *, double *, const Phys &,      \
+                                    cudaStream_t);
 FR_BASE_INST(double)
 FR_BASE_INST(float)
 #undef FR_BASE_INST

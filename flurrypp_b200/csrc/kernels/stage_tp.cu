@@ -8,6 +8,8 @@
 // element), all fields in registers, the 1-D operator tables in shared
 // memory.  Every sum is the one the dense operator would form, over its
 // nonzero terms in ascending column order.
+#include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "launch.cuh"
@@ -39,14 +41,15 @@ __device__ __forceinline__ void two_sum_tp(float a, float b, float &s, float &e)
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
+// One element block (EB elements from element blk * EB) of the stage; the
+// block's threads are threads 0..NT-1 of the CTA, and further threads of a
+// larger CTA (the many-order kernel below) only take part in its barriers.
 template <int ND, int P, bool VISC, typename R>
-__global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, TpTablesT<R> t) {
-  pdl_wait();
-  pdl_trigger();
+__device__ __forceinline__ void elem_tp_block(const ElemArgsT<R> &a, const TpTablesT<R> &t, int blk,
+                                              unsigned char *smem_bytes) {
   using T = Tp<ND, P, R>;
   constexpr bool F32 = std::is_same<R, float>::value;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
-  extern __shared__ __align__(16) unsigned char smem_bytes[];
   R *smem = reinterpret_cast<R *>(smem_bytes);
   R *sU = smem;                 // [NS][EB][NF]
   R *sF = sU + NS * ROW;        // [ND][NS][EB][NF]
@@ -56,24 +59,27 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
   R *sEF = sE + 2 * N;          // [2][N]
 
   const int E = a.E;
-  const int e0 = blockIdx.x * EB;
+  const int e0 = blk * EB;
   const int nValid = min(EB, E - e0);
   const int tid = threadIdx.x;
-  const int s = tid / EB, el = tid - (tid / EB) * EB;
+  const bool act = tid < NT;  // a thread of this block's NT
+  const int s = act ? tid / EB : 0, el = act ? tid - (tid / EB) * EB : 0;
   const int e = e0 + el;
-  const bool valid = el < nValid;
+  const bool valid = act && el < nValid;
   // the time step, loaded early so its latency overlaps the tile loads
   const double dtIn = a.eleDt ? (valid ? a.eleDt[e] : 0.0) : (a.mode != MODE_RESIDUAL ? *a.dt : 0.0);
 
-  for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
-  for (int i = tid; i < 2 * N; i += NT) {
-    sE[i] = t.E1[i];
-    sEF[i] = t.EFn1[i];
-  }
-  // A: state tile, coalesced along (element, field)
-  for (int idx = tid; idx < NS * ROW; idx += NT) {
-    const int ss = idx / ROW, r = idx - ss * ROW;
-    sU[idx] = (r < nValid * NF) ? a.U[((long long)ss * E + e0) * NF + r] : R(1.0);
+  if (act) {
+    for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
+    for (int i = tid; i < 2 * N; i += NT) {
+      sE[i] = t.E1[i];
+      sEF[i] = t.EFn1[i];
+    }
+    // A: state tile, coalesced along (element, field)
+    for (int idx = tid; idx < NS * ROW; idx += NT) {
+      const int ss = idx / ROW, r = idx - ss * ROW;
+      sU[idx] = (r < nValid * NF) ? a.U[((long long)ss * E + e0) * NF + r] : R(1.0);
+    }
   }
   R J[ND][ND];
 #pragma unroll
@@ -84,7 +90,7 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
   __syncthreads();
 
   // B: reference-space flux at (s, el)
-  {
+  if (act) {
     R Fp[ND][NF];
     const R *u = &sU[s * ROW + el * NF];
     if (valid) {
@@ -122,7 +128,8 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
   }
   __syncthreads();
 
-  // C1: divergence at (s, el): sum over d of D-lines
+  // C1: divergence at (s, el): sum over d of D-lines (threads past NT read
+  // the first point's lines and use nothing)
   int idx3[3];
   idx3[0] = s % N;
   idx3[1] = ND > 1 ? (s / N) % N : 0;
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
   }
 
   // C2: Fn - extrapolated normal flux at every (fpt, el)
-  for (int it = tid; it < NFP * EB; it += NT) {
+  for (int it = tid; act && it < NFP * EB; it += NT) {
     const int f = it / EB, fe = it - (it / EB) * EB;
     const int ee = e0 + fe;
     const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
@@ -243,7 +250,7 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
   __syncthreads();
 
   // E: new state at the flux points
-  for (int it = tid; it < NFP * EB; it += NT) {
+  for (int it = tid; act && it < NFP * EB; it += NT) {
     const int f = it / EB, fe = it - (it / EB) * EB;
     if (fe >= nValid) continue;
     const int ee = e0 + fe;
@@ -262,6 +269,88 @@ __global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, Tp
 #pragma unroll
     for (int k = 0; k < NF; k++) a.Ufpts_out[((long long)f * E + ee) * NF + k] = acc[k];
   }
+}
+
+template <int ND, int P, bool VISC, typename R>
+__global__ void __launch_bounds__(Tp<ND, P, R>::NT) k_elem_tp(ElemArgsT<R> a, TpTablesT<R> t) {
+  pdl_wait();
+  pdl_trigger();
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  elem_tp_block<ND, P, VISC, R>(a, t, blockIdx.x, smem_bytes);
+}
+
+constexpr int kMultiNT = 256;  // threads of a many-order CTA: at least every order's NT
+static_assert(Tp<2, 0>::NT <= kMultiNT && Tp<2, 5>::NT <= kMultiNT && Tp<3, 3>::NT <= kMultiNT &&
+                  Tp<3, 5>::NT <= kMultiNT && Tp<2, 2, float>::NT <= kMultiNT,
+              "a tensor-product block exceeds the many-order CTA");
+
+template <int ND, typename R>
+__global__ void __launch_bounds__(kMultiNT) k_elem_multi(const __grid_constant__ MultiElemArgsT<R> m) {
+  pdl_wait();
+  pdl_trigger();
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = (int)atomicAdd(m.next, 1u);
+    __syncthreads();
+    const int w = item;
+    __syncthreads();  // every thread has the item before thread 0 takes the next
+    if (w >= m.total) break;
+    int g = 0;
+    while (g + 1 < m.nGroups && w >= m.start[g + 1]) g++;
+    const int blk = w - m.start[g];
+    switch (m.order[g]) {
+      case 0: elem_tp_block<ND, 0, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 1: elem_tp_block<ND, 1, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 2: elem_tp_block<ND, 2, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 3: elem_tp_block<ND, 3, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 4: elem_tp_block<ND, 4, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+      default: elem_tp_block<ND, 5, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+    }
+    __syncthreads();  // the next block reuses the shared memory
+  }
+  // the last CTA out resets the counters for the next launch (all CTAs have
+  // taken their last item by then) and, after a step's last stage, advances
+  // the time of every group
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(m.done, 1u) == gridDim.x - 1) {
+      *m.next = 0u;
+      *m.done = 0u;
+      if (m.finalStage)
+        for (int g = 0; g < m.nGroups; g++) *m.timeAcc[g] += *m.a[g].dt;
+      __threadfence();
+    }
+  }
+}
+
+template <int ND, typename R>
+size_t multi_smem(const MultiElemArgsT<R> &m) {
+  size_t b = 0;
+  for (int g = 0; g < m.nGroups; g++) {
+    size_t x = 0;
+    switch (m.order[g]) {
+      case 0: x = Tp<ND, 0, R>::SMEM; break;
+      case 1: x = Tp<ND, 1, R>::SMEM; break;
+      case 2: x = Tp<ND, 2, R>::SMEM; break;
+      case 3: x = Tp<ND, 3, R>::SMEM; break;
+      case 4: x = Tp<ND, 4, R>::SMEM; break;
+      default: x = Tp<ND, 5, R>::SMEM; break;
+    }
+    b = x > b ? x : b;
+  }
+  return b;
+}
+
+template <int ND, typename R>
+void launch_multi(const MultiElemArgsT<R> &m, cudaStream_t st) {
+  const int smem = (int)multi_smem<ND, R>(m);
+  static std::atomic<unsigned long long> attrDev{0};
+  smem_attr(k_elem_multi<ND, R>, 227 * 1024, attrDev);
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_elem_multi<ND, R>, kMultiNT, smem);
+  const int g = std::max(1, std::min(m.total, std::max(per, 1) * sm_count(current_device())));
+  launch_k(k_elem_multi<ND, R>, g, kMultiNT, smem, st, m);
 }
 
 template <int ND, int P, typename R, bool VISC = false>
@@ -306,6 +395,17 @@ void launch_element_stage_tp_visc(int nDims, int order, const ElemArgsT<R> &a, c
   FR_TP_ORDERS(FR_TPV_CASE)
 #undef FR_TPV_CASE
 }
+
+template <typename R>
+void launch_element_stage_multi(int nDims, const MultiElemArgsT<R> &m, cudaStream_t st) {
+  if (m.total <= 0) return;
+  if (nDims == 2)
+    launch_multi<2, R>(m, st);
+  else
+    launch_multi<3, R>(m, st);
+}
+template void launch_element_stage_multi<double>(int, const MultiElemArgsT<double> &, cudaStream_t);
+template void launch_element_stage_multi<float>(int, const MultiElemArgsT<float> &, cudaStream_t);
 
 template int tp_elems_per_block<double>(int, int);
 template int tp_elems_per_block<float>(int, int);

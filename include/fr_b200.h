@@ -41,8 +41,11 @@ enum {
 
 /* Arithmetic of the path. */
 enum {
-  FR_PREC_FP64 = 0, /* plain form: everything in FP64 (the correctness oracle) */
-  FR_PREC_MIXED = 1 /* precision form: FP32 state/fluxes, split-precision operators */
+  FR_PREC_FP64 = 0,        /* plain form: everything in FP64 (the correctness oracle) */
+  FR_PREC_MIXED = 1,       /* precision form: FP32 state/fluxes, split-precision operators */
+  FR_PREC_MIXED_REFINE = 2 /* solve server only: a request runs in the precision form until its
+                              residual stops falling (the FP32 floor), then goes on in FP64 from
+                              that state to the residual-drop target */
 };
 
 typedef struct fr_case fr_case;
@@ -263,8 +266,77 @@ int fr_batch_gather(fr_batch *b);
 /* writeResidual norms of every member: out[n][nFields]. */
 int fr_batch_residual_norms(fr_batch *b, int resType, double *out, int nFields);
 int fr_batch_info(fr_batch *b, int *nGroups, long long *launches);
+/* Forms of a batch's step.  FR_BATCH_GROUPS: each order group's step graph
+ * (one face and one element launch per stage) on the group's own stream.
+ * FR_BATCH_MANY_ORDER: one face launch and one persistent element launch per
+ * RK stage for all groups: CTAs take element blocks of every order from a
+ * device work counter and run the tensor-product stage of each block's order
+ * (inviscid groups of one precision, at most 6 orders).  fr_batch_create
+ * times both on the batch's own state (3 steps each, state restored) and
+ * keeps the faster; fr_batch_form reports the choice and the measured ms per
+ * step of each (-1: not timed), fr_batch_set_form forces one. */
+enum { FR_BATCH_GROUPS = 0, FR_BATCH_MANY_ORDER = 1 };
+int fr_batch_form(fr_batch *b, int *form, float *ms_groups, float *ms_many_order);
+int fr_batch_set_form(fr_batch *b, int form);
 const char *fr_batch_last_error(const fr_batch *b);
 void fr_batch_destroy(fr_batch *b);
+
+/* ---- One case split into parts (sharding) ---------------------------------
+ * The reference runs one case on several MPI ranks: geo::partitionMesh splits
+ * the elements (METIS, src/geo.cpp:2380-2470), every face the split cuts
+ * becomes an mpiFace whose right trace comes from the rank across it at every
+ * stage (mpiFace::communicate / getRightState, src/mpiFace.cpp:122-175), each
+ * side forming the common flux as its own left side, and calcDt takes the
+ * minimum over ranks (src/solver.cpp:462-465).  A shard is that run with its
+ * parts on one device: the partition of fr_shard_plan, one fr_case per part
+ * (its elements, faces, metrics sliced from the whole case's), the cut traces
+ * packed by a kernel and exchanged by device copies at every stage, the cut
+ * faces formed by their own kernel, dt reduced over the parts on the device,
+ * and a whole step of all parts replayed as one CUDA graph.  Its residual and
+ * steps equal the unsplit case's to round-off (each side of a cut uses its
+ * own normal), also for CFL time steps: a cut face writes its wave speed only
+ * to the side that was the face's left side (face.cpp:372), where the
+ * reference's mpiFace writes it to both sides.  Plain form (FP64), inviscid,
+ * static mesh, no P-multigrid; nparts <= 64. */
+typedef struct fr_shard fr_shard;
+int fr_shard_create(const char *deck_path, const fr_setup_opts *opts, int nparts, fr_shard **out);
+/* Parts, elements owned by each (owned[nparts]) and cut face points of each
+ * (cut_points[nparts]); arrays may be null. */
+int fr_shard_info(fr_shard *s, int *nparts, int *owned, long long *cut_points);
+/* State and residual in the whole case's layout [nSpts][nEles][nFields]. */
+int fr_shard_set_state(fr_shard *s, const double *U, size_t count);
+int fr_shard_get_state(fr_shard *s, double *U, size_t count);
+int fr_shard_set_dt(fr_shard *s, double dt);
+int fr_shard_calc_residual(fr_shard *s, int step);
+int fr_shard_get_residual(fr_shard *s, int step, double *divF, size_t count);
+/* nsteps of solver::update over all parts (a CUDA graph after the first). */
+int fr_shard_run(fr_shard *s, int nsteps);
+/* Simulation time and the last dt (equal on every part). */
+int fr_shard_time(fr_shard *s, double *time, double *dt);
+const char *fr_shard_last_error(const fr_shard *s);
+void fr_shard_destroy(fr_shard *s);
+
+/* A part of a split case on its own rank: one process and one GPU per rank,
+ * as the reference's MPI ranks.  Part `rank` of the partition of fr_shard_plan
+ * (its elements in ascending global order; local state [nSpts][nOwned][nFields]
+ * through fr_set_state / fr_get_state), stepped by fr_update / fr_run /
+ * fr_calc_residual like any case: every face pass packs the part's cut traces
+ * and exchanges them with each peer by grouped ncclSend/ncclRecv on the case's
+ * stream, and dt (dtType 1, 2) is an ncclAllReduce(min).  nccl_comm is an
+ * ncclComm_t of the nparts ranks (fr_nccl_comm_init makes one; it may be null
+ * for nparts 1).  NCCL is resolved at run time (the process's libnccl.so.2).
+ * Plain form, inviscid, static mesh, no P-multigrid.  The in-process shard
+ * (fr_shard_*) runs the same parts, kernels and exchange order on one device. */
+int fr_part_create(const char *deck_path, const fr_setup_opts *opts, int nparts, int rank, void *nccl_comm,
+                   fr_case **out);
+/* FR_ERR_CUDA if an NCCL call of the part's exchange reported an error. */
+int fr_part_nccl_ok(fr_case *c);
+/* NCCL communicator set-up for callers without NCCL bindings: rank 0 makes
+ * the 128-byte id, every rank receives it (any transport) and calls
+ * fr_nccl_comm_init with its device. */
+int fr_nccl_unique_id(void *id128);
+int fr_nccl_comm_init(int nranks, const void *id128, int rank, int device, void **comm);
+int fr_nccl_comm_destroy(void *comm);
 
 /* ---- Serving: a request loop with continuous batching --------------------
  * Requests (deck, optional mesh, initial condition, residual-drop target)
@@ -275,13 +347,16 @@ void fr_batch_destroy(fr_batch *b);
  * waiting requests take its place.  No reference counterpart. */
 typedef struct fr_server fr_server;
 int fr_server_create(size_t budget_bytes, int max_inflight, int check_every, int device, fr_server **out);
-/* Form (FR_PREC_FP64 or FR_PREC_MIXED) of the requests the server admits
+/* Form (FR_PREC_FP64, FR_PREC_MIXED or FR_PREC_MIXED_REFINE) of the requests the server admits
  * from now on (default FP64).  No reference counterpart. */
 int fr_server_set_precision(fr_server *s, int precision);
 int fr_server_submit(fr_server *s, const char *deck, const fr_mesh *mesh, int ic_kind, const double *ic_prm,
                      int n_prm, double tol, int max_steps, long long *id);
 /* status: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled; latency from submission. */
 int fr_server_poll(fr_server *s, long long id, int *status, double *latency_s, int *steps, double *res_ratio);
+/* Form a request runs (or finished) in, and the steps it ran in the
+ * precision form (FR_PREC_MIXED_REFINE: before it went on in FP64). */
+int fr_server_poll_form(fr_server *s, long long id, int *precision, int *steps_fp32);
 /* Waits (bounded) for a request to finish; FR_ERR_TIMEOUT if it has not. */
 int fr_server_wait(fr_server *s, long long id, double timeout_s);
 /* Final state of a finished request, [nSpts][nEles][nFields]. */

@@ -23,6 +23,8 @@
  *   --cfl-dt CFL                  fixed dt from the CFL formula on the IC
  *   --steps N                     time steps after the residual dump
  *   --time K,W                    W untimed then K timed steps, print JSON
+ *   --time1 K                     after --time, K more steps timed on one
+ *                                 OpenMP thread (the 1-thread figure)
  *   --threads T                   OpenMP threads (omp build)
  *   --monitors                    after the steps, calcResidual(0) and dump the
  *                                 wall-force coefficients writeResidual prints
@@ -30,6 +32,10 @@
  *                                 errorNorm 0, 1, 2 (mass_flux [3][nF])
  *   --error                       after the steps, dump solver::integrateError
  *                                 for errorNorm 0, 1, 2 (err_integrals [3][nF])
+ *   --norms                       dump writeResidual's residual norms of the
+ *                                 initial state's residual for resType 1, 2, 3
+ *                                 (res_norms [3][nF]) and, after the steps, of
+ *                                 the state's residual then (res_norms_final)
  *   --write-vtu PREFIX            after the steps, writeData with dataFileName
  *                                 PREFIX (the deck's plotType: 1 ParaView
  *                                 PREFIX_<iter>.vtu, 0 CSV PREFIX.csv.<iter>)
@@ -106,11 +112,12 @@ struct Opts {
   double mu = 0.0;
   double cflDt = -1.0;
   int steps = 0;
-  int timeK = 0, timeW = 0;
+  int timeK = 0, timeW = 0, time1 = 0;
   int threads = 0;
   std::string vtu;
   bool error = false;
   bool monitors = false;
+  bool norms = false;
 };
 
 /* Uniform double in [0,1) from the top 53 bits of a 64-bit Mersenne twister
@@ -255,6 +262,24 @@ static void dump_setup(solver &S, input &p) {
   dumpi("face_fptR", fptR, {(size_t)nF, (size_t)nPF});
 }
 
+/* writeResidual's norm of divF_spts[0] (src/output.cpp:1011-1090): the
+ * per-element ele::getNormResidual (src/ele.cpp:1922-1944) summed over the
+ * elements (resType 1, 2) or their maximum (3), the square root for 2. */
+static std::vector<double> residual_norms(solver &S, input &p) {
+  std::vector<double> out;
+  for (int rt = 1; rt <= 3; rt++) {
+    std::vector<double> res(p.nFields, 0.0);
+    for (auto &e : S.eles) {
+      std::vector<double> r = e->getNormResidual(rt);
+      for (int i = 0; i < p.nFields; i++) res[i] = rt == 3 ? std::max(res[i], r[i]) : res[i] + r[i];
+    }
+    if (rt == 2)
+      for (auto &v : res) v = std::sqrt(v);
+    out.insert(out.end(), res.begin(), res.end());
+  }
+  return out;
+}
+
 static void dump_residual_parts(solver &S, input &p) {
   dumpA("U_fpts", S.U_fpts, 3);
   dumpA("F_spts", S.F_spts, 4);
@@ -296,10 +321,12 @@ int main(int argc, char **argv) {
     else if (a == "--steps") o.steps = atoi(next());
     else if (a == "--time") {
       if (sscanf(next(), "%d,%d", &o.timeK, &o.timeW) != 2) exit(2);
-    } else if (a == "--threads") o.threads = atoi(next());
+    } else if (a == "--time1") o.time1 = atoi(next());
+    else if (a == "--threads") o.threads = atoi(next());
     else if (a == "--write-vtu") o.vtu = next();
     else if (a == "--error") o.error = true;
     else if (a == "--monitors") o.monitors = true;
+    else if (a == "--norms") o.norms = true;
     else { fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
   }
   fr_refshim_blas_threads(1);
@@ -355,6 +382,7 @@ int main(int argc, char **argv) {
     /* one residual evaluation on the initial state (solver.cpp:366-445) */
     S.calcResidual(0);
     dump_residual_parts(S, params);
+    if (o.norms) dumpd("res_norms", residual_norms(S, params), {3, (size_t)S.nFields});
   }
 
   if (o.steps > 0) {
@@ -366,6 +394,11 @@ int main(int argc, char **argv) {
       if (params.PMG) pmg.cycle(S);
     }
     dumpA("U_final", S.U_spts, 3);
+    if (o.norms && g_manifest) {
+      /* the residual of the final state, as the next writeResidual sees it */
+      S.calcResidual(0);
+      dumpd("res_norms_final", residual_norms(S, params), {3, (size_t)S.nFields});
+    }
     std::vector<double> t = {params.time, params.dt};
     dumpd("time_dt", t, {2});
     if (params.dtType == 2) {
@@ -426,9 +459,21 @@ int main(int argc, char **argv) {
 #ifdef _OMP
     threads = omp_get_max_threads();
 #endif
+    double rate1 = 0.0, sec1 = 0.0;
+    if (o.time1 > 0) {
+#ifdef _OMP
+      omp_set_num_threads(1);
+#endif
+      auto u0 = std::chrono::steady_clock::now();
+      for (int s = 0; s < o.time1; s++) { iter++; S.update(); if (params.PMG) pmg.cycle(S); }
+      auto u1 = std::chrono::steady_clock::now();
+      sec1 = std::chrono::duration<double>(u1 - u0).count();
+      rate1 = dof * (double)o.time1 * params.nRKSteps / sec1;
+    }
     printf("{\"seconds\": %.6f, \"steps\": %d, \"stages\": %.0f, \"dof\": %.0f, "
-           "\"dof_stage_per_s\": %.6e, \"threads\": %d}\n",
-           sec, o.timeK, stages, dof, dof * stages / sec, threads);
+           "\"dof_stage_per_s\": %.6e, \"threads\": %d, \"steps_1thread\": %d, "
+           "\"seconds_1thread\": %.6f, \"dof_stage_per_s_1thread\": %.6e}\n",
+           sec, o.timeK, stages, dof, dof * stages / sec, threads, o.time1, sec1, rate1);
   }
   if (g_manifest) fclose(g_manifest);
   return 0;

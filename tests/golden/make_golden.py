@@ -284,13 +284,61 @@ def run_case(name: str) -> None:
     print(f"{name}: {len(out) - 1} arrays, {os.path.getsize(os.path.join(HERE, name + '.npz')) / 1e3:.0f} kB")
 
 
+# writeResidual's norms (resType 1, 2, 3; src/output.cpp:1011-1090) of the
+# initial state's residual and of the final state's, as the reference computes
+# them, for cases of each kind: 2-D/3-D, Legendre/Lobatto, P-multigrid with
+# walls and far field, perturbed hexes, viscous, high order
+NORM_CASES = ["vortex2d_p3_8", "lobatto_hu3d_p3", "chbump_p2_pmg", "tgv3d_p3_4_perturbed", "ns_tgv3d_p3_3",
+              "p5_2d"]
+
+
+def reference_norms() -> None:
+    out = {}
+    for name in NORM_CASES:
+        deck, args, steps, _ = CASES[name]
+        with tempfile.TemporaryDirectory() as td, tempfile.TemporaryDirectory() as wd:
+            cmd = [HARNESS, stage_deck(deck, wd), td] + args + ["--steps", str(steps), "--norms"]
+            subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=wd)
+            arrays, _ = read_dump(td)
+        out[name + "__initial"] = arrays["res_norms"]
+        out[name + "__final"] = arrays["res_norms_final"]
+    np.savez_compressed(os.path.join(HERE, "res_norms.npz"), **out)
+    print(f"res_norms: {len(NORM_CASES)} cases")
+
+
+# 3-D Taylor-Green vortex on 16^3 hexes, P3, FP64: 4,096 elements (many
+# waves of element blocks) and 196,608 interior face points, too large to
+# keep whole, so kept as per-element sums over the solution points of the
+# initial state, the initial residual and the state after 5 RK4 steps, with
+# the residual norms
+def large_tgv16() -> None:
+    args = ["--ic", "tgv", "--tgv-mach", "0.1", "--cfl-dt", "0.5"]
+    steps = 5
+    with tempfile.TemporaryDirectory() as td, tempfile.TemporaryDirectory() as wd:
+        cmd = [HARNESS, stage_deck("tgv3d_p3_16", wd), td] + args + ["--steps", str(steps), "--norms"]
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        arrays, meta = read_dump(td)
+    out = {"divF_0_elem_sum": arrays["divF_0"].sum(axis=0), "U_init_elem_sum": arrays["U_init"].sum(axis=0),
+           "U_final_elem_sum": arrays["U_final"].sum(axis=0), "divF_0_absmax": np.abs(arrays["divF_0"]).max(axis=(0, 1)),
+           "F_spts_absmax": np.abs(arrays["F_spts"]).max(axis=(0, 1, 2)), "time_dt": arrays["time_dt"],
+           "res_norms": arrays["res_norms"], "res_norms_final": arrays["res_norms_final"]}
+    meta.update({"case": "tgv3d_p3_16_sums", "deck": "tgv3d_p3_16", "harness_args": args, "steps": steps})
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "tgv3d_p3_16_sums.npz"), **out)
+    print(f"tgv3d_p3_16_sums: {os.path.getsize(os.path.join(HERE, 'tgv3d_p3_16_sums.npz')) / 1e3:.0f} kB")
+
+
+EXTRA = {"restart_p2_to_p3": lambda: restart_across_orders(), "res_norms": reference_norms,
+         "tgv3d_p3_16_sums": large_tgv16}
+
+
 def main(argv: list[str]) -> None:
     if not os.path.exists(HARNESS):
         sys.exit(f"{HARNESS} missing: run `make -C oracle REF=<FlurryPP sources>` first")
     write_meshes()
-    for name in argv or list(CASES) + ["restart_p2_to_p3"]:
-        if name == "restart_p2_to_p3":
-            restart_across_orders()
+    for name in argv or list(CASES) + list(EXTRA):
+        if name in EXTRA:
+            EXTRA[name]()
         else:
             run_case(name)
 

@@ -58,3 +58,40 @@ def test_batch_rejects_unsupported(tmp_path):
     with pytest.raises(fb.FrError) as ei:
         fb.Batch([s, h])
     assert ei.value.code == fb.FR_ERR_STATE
+
+
+@pytest.mark.parametrize("prec", [fb.FR_PREC_FP64, fb.FR_PREC_MIXED])
+def test_many_order_form_equals_alone(tmp_path, prec):
+    """The many-order form (one face launch and one persistent element launch
+    per RK stage for every order, blocks taken from a device work counter)
+    gives, case by case, what each case gives alone; the creation-time choice
+    between the forms is reported with both timings."""
+    specs = make_cases(tmp_path, n_cases=9, seed=11)
+    assert len({sp[1] for sp in specs}) >= 3
+    steps = 10
+
+    def built(i, sp):
+        s = build(tmp_path, sp, i)
+        if prec == fb.FR_PREC_FP64:
+            return s
+        m = fb.Solver(str(tmp_path / f"c{i}.deck"), precision=prec)
+        m.initialize_solution(fb.IC_VORTEX, sp[2:])
+        m.set_dt(s.calc_dt())
+        return m
+
+    alone = []
+    for i, sp in enumerate(specs):
+        s = built(i, sp)
+        s.run(steps)
+        alone.append(s.get_state())
+    members = [built(i, sp) for i, sp in enumerate(specs)]
+    b = fb.Batch(members)
+    f = b.form()
+    assert f["ms_groups"] > 0 and f["ms_many_order"] > 0
+    b.set_form(fb.FR_BATCH_MANY_ORDER)
+    b.run(steps)
+    b.gather()
+    tol = 1e-13 if prec == fb.FR_PREC_FP64 else 1e-5  # FP32: the two element kernels round alike only to FP32
+    for i, s in enumerate(members):
+        U, Ua = s.get_state(), alone[i]
+        assert np.max(np.abs(U - Ua)) <= tol * np.max(np.abs(Ua)), i

@@ -4,11 +4,15 @@ This pins the oracle: its residual of the fixture's initial state and its
 state after the fixture's N time steps must reproduce what the reference
 solver (built from its sources) produced on the same mesh and state.
 """
+import os
+
 import numpy as np
 import pytest
 
 import fr_oracle as O
-from conftest import deck_path, golden_cases, has_motion, has_pmg, load_golden, rel_err
+from conftest import ROOT, deck_path, golden_cases, has_motion, has_pmg, load_golden, rel_err
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 # The residual is a difference of flux terms; rounding is relative to their
 # size (the reference's own BLAS order is not reproducible), so residual
@@ -85,3 +89,18 @@ def test_residual_norm_definition():
     w = O.spt_weights(2, 3)
     ref = np.sqrt(sum(d[s] ** 2 / a["detJac_spts"][s][:, None] * w[s] for s in range(d.shape[0])).sum(axis=0))
     assert np.allclose(r2, ref, rtol=1e-14)
+
+
+NORM_CASES = ["vortex2d_p3_8", "lobatto_hu3d_p3", "chbump_p2_pmg", "tgv3d_p3_4_perturbed", "ns_tgv3d_p3_3", "p5_2d"]
+
+
+@pytest.mark.parametrize("case", NORM_CASES)
+def test_oracle_residual_norm_matches_reference(case):
+    """The oracle's residual norm (resType 1, 2, 3) of the reference's own
+    residual against writeResidual's norm as the reference computed it
+    (ele::getNormResidual summed or maximised over the elements)."""
+    a, meta = load_golden(case)
+    ref = np.load(os.path.join(GOLDEN, "res_norms.npz"))[case + "__initial"]
+    c = oracle_for(a, meta)
+    for rt in (1, 2, 3):
+        assert np.allclose(c.residual_norm(a["divF_0"], rt), ref[rt - 1], rtol=1e-13, atol=0), rt

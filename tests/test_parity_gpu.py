@@ -340,3 +340,58 @@ def test_boundary_monitors_match_reference(case):
         got = s.mass_flux(norm)
         assert np.max(np.abs(got - flux[norm])) <= 1e-10 * max(1.0, np.max(np.abs(flux[norm]))), \
             (norm, got, flux[norm])
+
+
+NORM_CASES = ["vortex2d_p3_8", "lobatto_hu3d_p3", "chbump_p2_pmg", "tgv3d_p3_4_perturbed", "ns_tgv3d_p3_3", "p5_2d"]
+
+
+@pytest.mark.parametrize("case", NORM_CASES)
+def test_residual_norm_matches_reference(case):
+    """fr_residual_norm (resType 1, 2, 3) against the norms the reference's
+    writeResidual computes, on the residual of the fixture's initial state and
+    on that of its state after the fixture's N steps.  The residual itself
+    agrees to 1e-12 of the flux scale, and the norms are of residuals up to
+    two orders below that scale, hence the relative bounds."""
+    import os
+
+    from conftest import ROOT
+
+    a, meta = load_golden(case)
+    z = np.load(os.path.join(ROOT, "tests", "golden", "res_norms.npz"))
+    s = gpu_case(meta)
+    s.set_state(a["U_init"])
+    s.calc_residual(0)
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), z[case + "__initial"][rt - 1], rtol=1e-9, atol=0), rt
+    s.run(meta["steps"])  # update() and, with PMG, the V-cycle: the reference driver's step
+    s.calc_residual(0)
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), z[case + "__final"][rt - 1], rtol=1e-7, atol=0), rt
+
+
+def test_tgv16_matches_reference_element_sums():
+    """3-D Taylor-Green vortex, 16^3 hexes, P3, FP64, from the product's own
+    initial condition: per-element sums of the initial state (1e-14), of the
+    residual (1e-12 of the flux scale) and of the state after 5 RK4 steps
+    (1e-10) against the reference's, and the residual norms."""
+    import json
+    import os
+
+    from conftest import ROOT
+
+    z = np.load(os.path.join(ROOT, "tests", "golden", "tgv3d_p3_16_sums.npz"))
+    meta = json.loads(str(z["meta"]))
+    s = fb.Solver(deck_path(meta))
+    s.initialize_solution(fb.IC_TGV, (0.1,))
+    s.set_dt(meta["dt"])
+    assert rel_err(s.get_state().sum(axis=0), z["U_init_elem_sum"]) < 1e-14
+    s.calc_residual(0)
+    fscale = 64 * max(float(z["divF_0_absmax"].max()), float(z["F_spts_absmax"].max()))
+    assert rel_err(s.get_residual(0).sum(axis=0), z["divF_0_elem_sum"], fscale) < RESID_TOL
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), z["res_norms"][rt - 1], rtol=1e-9, atol=0), rt
+    s.run(meta["steps"])
+    assert rel_err(s.get_state().sum(axis=0), z["U_final_elem_sum"]) < STEP_TOL
+    s.calc_residual(0)
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), z["res_norms_final"][rt - 1], rtol=1e-7, atol=0), rt

@@ -1,0 +1,48 @@
+"""The two builds of the reference under oracle/_ref set meshes up alike.
+
+The timing build (fr_ref_harness_omp) replaces the reference's O(n^2) row
+de-duplication by a hashed one (oracle/refshim/fast_unique.cpp) so that its
+32^3 mesh sets up in minutes; the parity build (fr_ref_harness) keeps the
+reference's own.  Both must give the same face connectivity on every kind of
+mesh the benchmarks use: periodic 2-D and 3-D boxes, and a Gmsh mesh with
+walls and far-field boundaries.  CPU only; skipped where the reference was not
+built.
+"""
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+import make_golden as MG  # noqa: E402
+
+O2 = os.path.join(ROOT, "oracle", "_ref", "fr_ref_harness")
+OMP = os.path.join(ROOT, "oracle", "_ref", "fr_ref_harness_omp")
+FACE = ["face_type", "face_eL", "face_locL", "face_eR", "face_locR", "face_relRot", "face_bc", "face_fptR"]
+
+pytestmark = pytest.mark.skipif(not (os.path.exists(O2) and os.path.exists(OMP)),
+                                reason="reference builds (oracle/_ref) not present")
+
+
+def dump_faces(binary, deck):
+    with tempfile.TemporaryDirectory() as td, tempfile.TemporaryDirectory() as wd:
+        path = MG.stage_deck(deck, wd)
+        env = dict(os.environ, OMP_NUM_THREADS="2")
+        subprocess.run([binary, path, td], check=True, stdout=subprocess.DEVNULL, cwd=wd, env=env)
+        arrays, meta = MG.read_dump(td)
+    return {k: arrays[k] for k in FACE}, meta
+
+
+@pytest.mark.parametrize("deck", ["tgv3d_p3_4", "vortex2d_p3_8", "chbump_p2_pmg", "wallchar3d_p2"])
+def test_timing_build_sets_up_the_same_faces(deck):
+    a, ma = dump_faces(O2, deck)
+    b, mb = dump_faces(OMP, deck)
+    assert ma["nFaces"] == mb["nFaces"] and ma["nEles"] == mb["nEles"]
+    for k in FACE:
+        assert np.array_equal(a[k], b[k]), k

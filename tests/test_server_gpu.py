@@ -119,3 +119,25 @@ def test_precision_form_served(tmp_path):
     d.run(pa["steps"])
     ud = d.get_state()
     assert np.linalg.norm(ua - ud) / np.linalg.norm(ud) < 1e-6
+
+
+def test_refining_precision_form_reaches_the_tight_drop(tmp_path):
+    """FR_PREC_MIXED_REFINE served to a 1e-8 residual drop: the request runs
+    in the precision form until its FP32 residual stops falling, then goes on
+    in FP64; it reaches the drop, as the FP64 form does, and the FP64 steady
+    state (L2 within 1e-6).  The all-FP32 form stays at its floor."""
+    deck = make_case(tmp_path, 0, *SPECS[0])
+    res = {}
+    for prec in (fb.FR_PREC_FP64, fb.FR_PREC_MIXED_REFINE, fb.FR_PREC_MIXED):
+        srv = fb.Server(budget_bytes=8 << 30, max_inflight=1, check_every=10, precision=prec)
+        rid = srv.submit(deck, tol=1e-8, max_steps=20000)
+        srv.wait(rid, 600)
+        res[prec] = (srv.result(rid, shape_of(deck)), srv.poll(rid), srv.poll_form(rid))
+        srv.close()
+    (u64, p64, _), (umx, pmx, fmx), (_, p32, f32) = (res[fb.FR_PREC_FP64], res[fb.FR_PREC_MIXED_REFINE],
+                                                      res[fb.FR_PREC_MIXED])
+    assert p64["status"] == 2 and p64["res_ratio"] <= 1e-8
+    assert pmx["status"] == 2 and pmx["res_ratio"] <= 1e-8, pmx
+    assert fmx["precision"] == fb.FR_PREC_FP64 and 0 < fmx["steps_fp32"] < pmx["steps"], fmx
+    assert np.linalg.norm(umx - u64) / np.linalg.norm(u64) < 1e-6
+    assert f32["precision"] == fb.FR_PREC_MIXED and p32["res_ratio"] > 1e-8

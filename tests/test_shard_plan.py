@@ -155,3 +155,117 @@ def test_two_gloo_ranks_exchange_traces_in_plan_order(deck):
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert all(ok for _, ok, _ in got)
     assert got[0][2] == got[1][2] > 0
+
+
+def part_oracle(a, meta, part, rank, peer, slot):
+    """The numpy oracle on one part: the fixture's arrays sliced to the part's
+    elements, its interior and boundary faces renumbered, and its cut face
+    points (halo order, stably sorted by peer as the library lists them), each
+    formed with the part's own element as the left side and the received
+    trace as the right state."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fr_oracle as O
+    from conftest import deck_path
+
+    owned = np.nonzero(part == rank)[0]
+    local = -np.ones(part.size, dtype=np.int64)
+    local[owned] = np.arange(owned.size)
+    b = {k: v for k, v in a.items() if k.startswith("opp_")}
+    b["detJac_spts"] = a["detJac_spts"][:, owned]
+    b["JGinv_spts"] = a["JGinv_spts"][:, :, owned, :]
+    b["norm_fpts"] = a["norm_fpts"][:, owned, :]
+    b["dA_fpts"] = a["dA_fpts"][:, owned]
+    eL, eR = a["face_eL"], a["face_eR"]
+    keep = (part[eL] == rank) & ((eR < 0) | (part[np.maximum(eR, 0)] == rank))
+    b["face_eL"] = local[eL[keep]]
+    b["face_locL"] = a["face_locL"][keep]
+    b["face_eR"] = np.where(eR[keep] >= 0, local[np.maximum(eR[keep], 0)], -1)
+    b["face_fptR"] = a["face_fptR"].reshape(eL.size, -1)[keep]
+    b["face_bc"] = a["face_bc"][keep]
+    p = O.params_from_deck(deck_path(meta))
+    p["dt"] = meta["dt"]
+    c = O.OracleCase(b, p)
+    order = np.argsort(peer, kind="stable")
+    c.cut_slot, c.cut_peer = slot[order], peer[order]
+    base_faces = c.faces
+
+    def faces(Uf):
+        Fn = base_faces(Uf).reshape(-1, c.nF)
+        Ufl = Uf.reshape(-1, c.nF)
+        n = c.norm.reshape(-1, c.nd)[c.cut_slot]
+        UL = Ufl[c.cut_slot]
+        if c.nd == 2 and int(p.get("riemannType", 0)) == 1:
+            F = O.roe2d(UL, c.recv, n, p["gamma"])
+        else:
+            F, _ = O.rusanov(UL, c.recv, n, p["gamma"])
+        Fn[c.cut_slot] = F * c.dA.ravel()[c.cut_slot][:, None]
+        return Fn.reshape(Uf.shape)
+
+    c.faces = faces
+    return c, owned
+
+
+def _rank_residual(rank, world, port, case, q):
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fr_oracle as O
+    from conftest import deck_path, load_golden
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        a, meta = load_golden(case)
+        s = fb.Solver(deck_path(meta), device=-1)
+        part, _, peer, slot = s.shard_plan(world, rank)
+        c, owned = part_oracle(a, meta, part, rank, peer, slot)
+        U = a["U_init"][:, owned, :]
+        Uf = c.extrapolate(U).reshape(-1, c.nF)
+        send = torch.from_numpy(np.ascontiguousarray(Uf[c.cut_slot]))
+        recv = torch.empty_like(send)
+        other = 1 - rank
+        if rank == 0:
+            dist.send(send, other)
+            dist.recv(recv, other)
+        else:
+            dist.recv(recv, other)
+            dist.send(send, other)
+        c.recv = recv.numpy()
+        d_part = c.residual(U)
+        p = O.params_from_deck(deck_path(meta))
+        p["dt"] = meta["dt"]
+        d_full = O.OracleCase(a, p).residual(a["U_init"])[:, owned, :]
+        fscale = float(np.max(np.abs(a["F_spts"])))
+        err = float(np.max(np.abs(d_part - d_full))) / max(fscale, float(np.max(np.abs(d_full))))
+        q.put((rank, err, int(c.cut_slot.size)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case", ["tgv3d_p3_4", "chbump_p3", "roe2d_p2"])
+def test_two_gloo_ranks_residual_through_the_partition(case):
+    """Each of two gloo ranks computes the residual of its part with the numpy
+    oracle, the right traces of its cut faces received from the other rank in
+    the plan's order: together they give the whole case's residual (to the
+    round-off of each side using its own normal)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_residual, args=(r, 2, port, case, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        for p in procs:
+            p.join(180)
+    finally:
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+                p.join(10)
+    assert all(p.exitcode == 0 for p in procs)
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    assert got[0][2] == got[1][2] > 0
+    for _, err, _ in got:
+        assert err < 1e-14, err
