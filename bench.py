@@ -386,11 +386,15 @@ def vortex32_form(args, fb, torch, stream):
     """Config 1: 2-D Euler vortex (strength 5, Mach 0.5 along +x), periodic
     [-5,5]^2, 32x32 quads, P3, RK4, fixed dt at CFL 0.5, 1000 steps: the FP64
     GPU path and the reference's CPU path on the same run."""
-    deck = os.path.join(ROOT, "tests", "golden", "decks", "vortex2d_p3_32.deck")
+    import tempfile
+
+    from flurrypp_b200.decks import vortex_case
+
+    deck = vortex_case(os.path.join(tempfile.mkdtemp(prefix="fr_v32_"), "vortex32.deck"), 32, 3, 0.5)
     s = fb.Solver(deck)
     s.set_stream(stream.cuda_stream)
     s.initialize_solution(fb.IC_VORTEX, (5.0, 0.0, 0.0, 0.5))
-    dt = s.calc_dt()
+    dt = s.calc_dt()  # the CFL formula at CFL 0.5 on the initial state, then fixed
     s.set_dt(dt)
     dof, nrk = s.nSpts * s.nEles * s.nFields, s.nRKSteps
     steps = 1000
@@ -585,6 +589,7 @@ def form_serve(args, fb, torch):
     precision = dict(max_inflight=args.serve_inflight, rate_per_s=top,
                      form="FR_PREC_MIXED_REFINE: precision form until the FP32 residual stops falling, then FP64",
                      **serve(reqs, args.serve_inflight, top, fb.FR_PREC_MIXED_REFINE))
+    precision.pop("steps_each")
     k = min(args.serve_alone, len(reqs))
     alone = serve(reqs[:k], 1, 0.0)
     alone["sample"] = f"the first {k} requests, submitted together, one in flight"

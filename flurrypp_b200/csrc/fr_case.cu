@@ -1919,6 +1919,10 @@ struct fr_batch {
       }
     }
     use_streams(false);
+    if (ok) {
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) ok = fail(std::string("many-order step: ") + cudaGetErrorString(e));
+    }
     // every group's own stream waits for the steps issued on the first one
     cudaEvent_t ev;
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail("event");

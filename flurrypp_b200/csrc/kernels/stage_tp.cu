@@ -284,6 +284,10 @@ static_assert(Tp<2, 0>::NT <= kMultiNT && Tp<2, 5>::NT <= kMultiNT && Tp<3, 3>::
                   Tp<3, 5>::NT <= kMultiNT && Tp<2, 2, float>::NT <= kMultiNT,
               "a tensor-product block exceeds the many-order CTA");
 
+// the arguments travel as one kernel parameter (above the classic 4 KB,
+// within the 32,764 bytes sm_70+ take since CUDA 12.1)
+static_assert(sizeof(MultiElemArgsT<double>) < 32000, "many-order arguments exceed the kernel parameter space");
+
 template <int ND, typename R>
 __global__ void __launch_bounds__(kMultiNT) k_elem_multi(const __grid_constant__ MultiElemArgsT<R> m) {
   pdl_wait();
@@ -342,11 +346,24 @@ size_t multi_smem(const MultiElemArgsT<R> &m) {
   return b;
 }
 
+// the largest block's shared memory over all orders (the attribute is set
+// once per device, whichever orders a batch holds)
+template <int ND, typename R>
+constexpr size_t multi_smem_max() {
+  size_t b = Tp<ND, 0, R>::SMEM;
+  b = Tp<ND, 1, R>::SMEM > b ? Tp<ND, 1, R>::SMEM : b;
+  b = Tp<ND, 2, R>::SMEM > b ? Tp<ND, 2, R>::SMEM : b;
+  b = Tp<ND, 3, R>::SMEM > b ? Tp<ND, 3, R>::SMEM : b;
+  b = Tp<ND, 4, R>::SMEM > b ? Tp<ND, 4, R>::SMEM : b;
+  b = Tp<ND, 5, R>::SMEM > b ? Tp<ND, 5, R>::SMEM : b;
+  return b;
+}
+
 template <int ND, typename R>
 void launch_multi(const MultiElemArgsT<R> &m, cudaStream_t st) {
   const int smem = (int)multi_smem<ND, R>(m);
   static std::atomic<unsigned long long> attrDev{0};
-  smem_attr(k_elem_multi<ND, R>, 227 * 1024, attrDev);
+  smem_attr(k_elem_multi<ND, R>, (int)multi_smem_max<ND, R>(), attrDev);
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_elem_multi<ND, R>, kMultiNT, smem);
   const int g = std::max(1, std::min(m.total, std::max(per, 1) * sm_count(current_device())));

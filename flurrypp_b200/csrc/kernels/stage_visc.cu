@@ -8,9 +8,6 @@
 //   k_faces_visc_*  inviscid + LDG viscous common flux, times dA, at both sides
 //                   (face.cpp:163-186, 210-311; boundFace.cpp:316-350).
 // The viscous flux at the solution points is added in the element kernel.
-#include <algorithm>
-#include <atomic>
-
 #include "launch.cuh"
 #include "stage.hpp"
 
@@ -151,110 +148,6 @@ __global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, cons
     Fn[(long long)sL * NF + k] = F[k] * aL;
     Fn[(long long)sR * NF + k] = -F[k] * aR;
   }
-}
-
-// Interior face points of a viscous stage with the gathers in flight through
-// shared memory (the pattern of k_faces_interior_async): persistent CTAs walk
-// chunks of kViscChunk points, one point per thread, and issue every chunk's
-// gathers (both traces, both gradients, the normal, both dA) as cp.async
-// copies into one of two shared buffers, one chunk ahead of the chunk being
-// computed.  The flux is the one of k_faces_visc_interior from the same
-// values by the same code: results are bit-identical.
-constexpr int kViscChunk = 128;
-
-template <int ND, typename R>
-__global__ void __launch_bounds__(kViscChunk) k_faces_visc_interior_async(
-    int n, const int *__restrict__ slotL, const int *__restrict__ slotR, const R *__restrict__ nrm,
-    const R *__restrict__ dAL, const R *__restrict__ dAR, const R *__restrict__ Uf, const R *__restrict__ dUf,
-    long long dStride, R *__restrict__ Fn, double *__restrict__ waveSp, Phys ph) {
-  pdl_wait();
-  pdl_trigger();
-  constexpr int NF = ND + 2;
-  constexpr int O_G = 2 * NF, O_N = O_G + 2 * ND * NF, W = O_N + ND + 2;
-  extern __shared__ __align__(16) unsigned char vsm_raw[];
-  R *buf = reinterpret_cast<R *>(vsm_raw);  // [2][kViscChunk][W]
-  const int t = threadIdx.x;
-  const int nChunks = (n + kViscChunk - 1) / kViscChunk;
-  int c = blockIdx.x;
-  if (c >= nChunks) return;
-  auto issue = [&](int chunk, int sl, int sr, int b) {
-    const int i = chunk * kViscChunk + t;
-    if (chunk < nChunks && i < n) {
-      R *d = buf + ((size_t)b * kViscChunk + t) * W;
-#pragma unroll
-      for (int k = 0; k < NF; k++) {
-        cp_async_word<R>(d + k, Uf + (long long)sl * NF + k);
-        cp_async_word<R>(d + NF + k, Uf + (long long)sr * NF + k);
-      }
-#pragma unroll
-      for (int q = 0; q < ND; q++)
-#pragma unroll
-        for (int k = 0; k < NF; k++) {
-          cp_async_word<R>(d + O_G + q * NF + k, dUf + q * dStride + (long long)sl * NF + k);
-          cp_async_word<R>(d + O_G + (ND + q) * NF + k, dUf + q * dStride + (long long)sr * NF + k);
-        }
-#pragma unroll
-      for (int q = 0; q < ND; q++) cp_async_word<R>(d + O_N + q, nrm + (long long)i * ND + q);
-      cp_async_word<R>(d + O_N + ND, dAL + i);
-      cp_async_word<R>(d + O_N + ND + 1, dAR + i);
-    }
-    cp_async_commit();
-  };
-  auto slots = [&](int chunk, int &sl, int &sr) {
-    const int i = chunk * kViscChunk + t;
-    if (chunk < nChunks && i < n) {
-      sl = slotL[i];
-      sr = slotR[i];
-    } else {
-      sl = sr = 0;
-    }
-  };
-  int sl0, sr0, sl1, sr1;
-  slots(c, sl0, sr0);
-  issue(c, sl0, sr0, 0);
-  const int cs = (int)gridDim.x;
-  slots(c + cs, sl1, sr1);
-  for (int it = 0; c < nChunks; it++, c += cs) {
-    issue(c + cs, sl1, sr1, (it + 1) & 1);
-    int sl2, sr2;
-    slots(c + 2 * cs, sl2, sr2);
-    cp_async_wait<1>();
-    const int i = c * kViscChunk + t;
-    if (i < n) {
-      const R *d = buf + ((size_t)(it & 1) * kViscChunk + t) * W;
-      R UL[NF], UR[NF], nv[ND], F[NF], gL[ND][NF], gR[ND][NF];
-#pragma unroll
-      for (int k = 0; k < NF; k++) {
-        UL[k] = d[k];
-        UR[k] = d[NF + k];
-      }
-#pragma unroll
-      for (int q = 0; q < ND; q++) {
-        nv[q] = d[O_N + q];
-#pragma unroll
-        for (int k = 0; k < NF; k++) {
-          gL[q][k] = d[O_G + q * NF + k];
-          gR[q][k] = d[O_G + (ND + q) * NF + k];
-        }
-      }
-      const int sL = sl0, sR = sr0;
-      if (ND == 2 && ph.riemannType == 1) {
-        roe2d<R>(UL, UR, nv, R(ph.gamma), F);
-      } else {
-        const R ws = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
-        if (waveSp) waveSp[sL] = ws;
-      }
-      ldg_interior_flux<ND, R>(UL, UR, gL, gR, nv, ph, F);
-      const R aL = d[O_N + ND], aR = d[O_N + ND + 1];
-#pragma unroll
-      for (int k = 0; k < NF; k++) {
-        Fn[(long long)sL * NF + k] = F[k] * aL;
-        Fn[(long long)sR * NF + k] = -F[k] * aR;
-      }
-    }
-    sl0 = sl1, sr0 = sr1, sl1 = sl2, sr1 = sr2;
-  }
-  cp_async_wait<0>();
 }
 
 template <int ND, typename R>
@@ -481,27 +374,7 @@ template <typename R>
 void launch_faces_visc(int nDims, const FaceTableT<R> &ft, const R *Ufpts, const R *dUf, long long fStride, R *Fn,
                        double *waveSp, const Phys &ph, cudaStream_t st) {
   const int b = 128, nI = ft.nInterior, nB = ft.n - ft.nInterior;
-  if (nI >= (1 << 16)) {  // large: gathers in flight through shared memory
-    const int W = 2 * (nDims + 2) + 2 * nDims * (nDims + 2) + nDims + 2;
-    const int smem = 2 * kViscChunk * W * (int)sizeof(R);
-    static std::atomic<unsigned long long> done2[2], done3[2];
-    int per = 0;
-    if (nDims == 2) {
-      smem_attr(k_faces_visc_interior_async<2, R>, smem, done2[sizeof(R) == 8]);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_faces_visc_interior_async<2, R>, kViscChunk, smem);
-    } else {
-      smem_attr(k_faces_visc_interior_async<3, R>, smem, done3[sizeof(R) == 8]);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_faces_visc_interior_async<3, R>, kViscChunk, smem);
-    }
-    const int chunks = (nI + kViscChunk - 1) / kViscChunk;
-    const int g = std::max(1, std::min(chunks, std::max(per, 1) * sm_count(current_device())));
-    if (nDims == 2)
-      launch_k(k_faces_visc_interior_async<2, R>, g, kViscChunk, smem, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL,
-               ft.dAR, Ufpts, dUf, fStride, Fn, waveSp, ph);
-    else
-      launch_k(k_faces_visc_interior_async<3, R>, g, kViscChunk, smem, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL,
-               ft.dAR, Ufpts, dUf, fStride, Fn, waveSp, ph);
-  } else if (nI > 0) {
+  if (nI > 0) {
     if (nDims == 2)
       launch_k(k_faces_visc_interior<2, R>, (nI + b - 1) / b, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts,
                                                                dUf, fStride, Fn, waveSp, ph);
