@@ -665,9 +665,53 @@ PROFILE_CASES = {
 }
 
 
+def profile_shard(fb, torch, nparts=4):
+    """One RK step of the 16^3 P3 Taylor-Green case split into parts on this
+    device (cut-face pack, exchange and flux kernels among the stage kernels)."""
+    sh = fb.Shard(DECK_CPU, nparts)
+    one = fb.Solver(DECK_CPU)
+    one.initialize_solution(fb.IC_TGV, (0.1,))
+    sh.set_state(one.get_state())
+    sh.set_dt(one.calc_dt())
+    sh.run(2)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    sh.run(1)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return {"nparts": nparts, **sh.info()}
+
+
+def profile_many_order(fb, torch, tmp):
+    """One RK step of 32 vortex cases of orders 2..5 in the many-order batch
+    form (one face and one element launch per stage for all orders)."""
+    import numpy as np
+    from flurrypp_b200.decks import vortex_case
+
+    rng = np.random.default_rng(5)
+    cs = []
+    for i in range(32):
+        n, P = int(rng.integers(16, 49)), 2 + i % 4
+        s = fb.Solver(vortex_case(os.path.join(tmp, f"m{i}.deck"), n, P, 0.4))
+        s.initialize_solution(fb.IC_VORTEX, (3.0, 0.0, 0.0, 0.4))
+        s.set_dt(s.calc_dt())
+        cs.append(s)
+    b = fb.Batch(cs)
+    b.set_form(fb.FR_BATCH_MANY_ORDER)
+    b.run(2)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    b.run(1)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return {"cases": len(cs), "dof": int(sum(c.nSpts * c.nEles * c.nFields for c in cs)), **b.form()}
+
+
 def run_profile(names):
     """Set each case up, then launch its element stage and face pass once
-    between cudaProfilerStart/Stop (for `ncu --profile-from-start off`)."""
+    between cudaProfilerStart/Stop (for `ncu --profile-from-start off`);
+    `shard4_tgv16` and `many_order_batch` profile one step of a split case
+    and of the many-order batch form."""
     import tempfile
 
     import torch
@@ -677,6 +721,12 @@ def run_profile(names):
     tmp = tempfile.mkdtemp(prefix="fr_prof_")
     out = {}
     for name in names.split(","):
+        if name == "shard4_tgv16":
+            out[name] = profile_shard(fb, torch)
+            continue
+        if name == "many_order_batch":
+            out[name] = profile_many_order(fb, torch, tmp)
+            continue
         kind, P, n, prec, var = PROFILE_CASES[name]
         opts = dict(precision=prec, tile_variant=var)
         if kind == "tgv":
