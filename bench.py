@@ -778,7 +778,7 @@ def main():
     ap.add_argument("--alone-steps", type=int, default=20)
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[2.0, 32.0])
-    ap.add_argument("--serve-alone", type=int, default=3)
+    ap.add_argument("--serve-alone", type=int, default=8)
     ap.add_argument("--serve-seed", type=int, default=7)
     ap.add_argument("--serve-max-steps", type=int, default=12000)
     ap.add_argument("--serve-inflight", type=int, default=16)
