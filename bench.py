@@ -660,6 +660,8 @@ PROFILE_CASES = {
     "fp32_tgv32_p3": ("tgv", 3, 32, 1, -1),
     "fp32_vortex256_p3": ("vortex", 3, 256, 1, -1),
     "tc_vortex256_p3": ("vortex", 3, 256, 1, 3),
+    "fp32_tgv64_p1": ("tgv", 1, 64, 1, -1),
+    "tc_tgv64_p1": ("tgv", 1, 64, 1, 3),
     "fp32_ns_tgv24_p4": ("ns", 4, 24, 1, -1),
     "fp64_ns_tgv24_p4": ("ns", 4, 24, 0, -1),
 }
@@ -730,7 +732,14 @@ def run_profile(names):
         kind, P, n, prec, var = PROFILE_CASES[name]
         opts = dict(precision=prec, tile_variant=var)
         if kind == "tgv":
-            deck, ic = DECK_GPU if n == 32 else None, (fb.IC_TGV, (0.1,))
+            ic = (fb.IC_TGV, (0.1,))
+            deck = DECK_GPU
+            if n != 32 or P != 3:
+                src = open(DECK_GPU).read().replace("order         3", f"order         {P}")
+                for ax in ("nx", "ny", "nz"):
+                    src = src.replace(f"{ax} 32", f"{ax} {n}")
+                deck = os.path.join(tmp, f"{name}.deck")
+                open(deck, "w").write(src)
         elif kind == "vortex":
             deck, ic = vortex_case(os.path.join(tmp, f"{name}.deck"), n, P, 0.5), (fb.IC_VORTEX, (5.0, 0.0, 0.0, 0.5))
         else:

@@ -1003,12 +1003,12 @@ struct fr_case {
   // variant computes each point with the same operations, so the choice
   // changes the speed only, never the result.
   bool autotune_tiles() {
-    const bool tc = frk::tc2d_supported(nDims, in.order) && !opts.no_tensor_cores;
+    const bool tc = frk::tc_supported(nDims, in.order) && !opts.no_tensor_cores;
     if (tc && !f32.tcOps) {
-      const double *g[2] = {op.grad[0].data(), op.grad[1].data()};
-      const double *x[2] = {op.extFn[0].data(), op.extFn[1].data()};
+      const double *g[3] = {op.grad[0].data(), op.grad[1].data(), nDims == 3 ? op.grad[2].data() : nullptr};
+      const double *x[3] = {op.extFn[0].data(), op.extFn[1].data(), nDims == 3 ? op.extFn[2].data() : nullptr};
       std::vector<float> blob;
-      if (!frk::tc2d_pack_ops(in.order, g, x, op.corr.data(), op.ext.data(), blob) || !upload(f32.tcOps, blob))
+      if (!frk::tc_pack_ops(nDims, in.order, g, x, op.corr.data(), op.ext.data(), blob) || !upload(f32.tcOps, blob))
         return fail(FR_ERR_CUDA, "tensor-core operator upload");
     }
     const int nv = frk::tma_variants(true) + (tc ? 1 : 0);
@@ -1587,7 +1587,7 @@ struct fr_case {
   // 0 .. tma_variants-1, then the 2-D tensor-core one
   void launch_tma32(const frk::ElemArgsT<float> &a, int v) {
     if (v == frk::tma_variants(true))
-      frk::launch_element_stage_tc2d(in.order, a, f32.tcOps, f32.tm, stream);
+      frk::launch_element_stage_tc(nDims, in.order, a, f32.tcOps, f32.tm, stream);
     else
       frk::launch_element_stage_tma<float>(nDims, in.order, a, f32.tp, f32.tm, stream, v);
   }

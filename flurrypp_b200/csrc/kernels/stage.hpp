@@ -229,15 +229,17 @@ void launch_element_stage_tma_visc(int nDims, int order, const ElemArgsT<R> &a, 
 template <typename R>
 void launch_elem_grad_tma(int nDims, int order, int E, const TpTablesT<R> &t, const TmaMaps &m,
                           unsigned int *err, cudaStream_t st);
-// 2-D precision-form element stage on the tensor cores (tcgen05 kind::tf32,
-// 3xTF32), 32 elements per CTA; the tile variant after the CUDA-core ones.
-// The operators are packed once on the host into the MMA operand layout.
-bool tc2d_supported(int nDims, int order);
-bool tc2d_pack_ops(int order, const double *const grad[2], const double *const extFn[2], const double *corr,
-                   const double *ext, std::vector<float> &blob);
-size_t tc2d_smem_bytes(int order);
-void launch_element_stage_tc2d(int order, const ElemArgsT<float> &a, const float *ops, const TmaMaps &m,
-                               cudaStream_t st);
+// Precision-form element stage on the tensor cores (tcgen05 kind::tf32,
+// 3xTF32) for 2-D orders 1..4 (32 elements per CTA) and 3-D order 1 (24);
+// the tile variant after the CUDA-core ones.  The operators are packed once
+// on the host into the MMA operand layout (grad/extFn: nDims pointers).
+bool tc_supported(int nDims, int order);
+int tc_elems_per_block(int nDims, int order);
+bool tc_pack_ops(int nDims, int order, const double *const grad[3], const double *const extFn[3],
+                 const double *corr, const double *ext, std::vector<float> &blob);
+size_t tc_smem_bytes(int nDims, int order);
+void launch_element_stage_tc(int nDims, int order, const ElemArgsT<float> &a, const float *ops, const TmaMaps &m,
+                             cudaStream_t st);
 template <typename R>
 int tp_elems_per_block(int nDims, int order);
 template <typename R>

@@ -1,4 +1,5 @@
-// 2-D element stage of the precision form on the 5th-generation tensor cores.
+// Element stage of the precision form on the 5th-generation tensor cores
+// (2-D orders 1..4, 3-D order 1).
 //
 // The same stage as k_elem_tma (flux, divergence, extrapolated normal flux,
 // correction, RK update, extrapolation to the flux points; reference:
@@ -8,19 +9,20 @@
 // split x = hi + lo into two TF32 values and a product is formed from
 // hi*hi + hi*lo + lo*hi (3xTF32: ~2^-22 relative, FP32-like).
 //
-// One CTA holds 32 elements; the 128 (element, field) columns of a tile are
-// the 128 rows of every MMA (M = 128, one TMEM lane each), so with the
-// element tile as the A operand and an operator as the B operand:
-//   GEMM1  D[:, 0:NSp | NSp:NSp+NFPp] = F^T [128 x 2NS] * [grad_x grad_y ; extFn_x extFn_y]^T
+// One CTA holds EB elements (2-D: 32 x 4 fields; 3-D: 24 x 5 fields, the
+// last 8 rows padding); the (element, field) columns of a tile are the rows
+// of every MMA (M = 128, one TMEM lane each), so with the element tile as
+// the A operand and an operator as the B operand:
+//   GEMM1  D[:, 0:NSp | NSp:NSp+NFPp] = F^T [128 x ND*NS] * [grad_d ... ; extFn_d ...]^T
 //          (divergence and extrapolated normal flux in one MMA chain)
 //   GEMM2  D[:, 0:NSp] += (Fn - disFn)^T [128 x NFP] * corr^T
 //   GEMM3  D[:, NSp:]   = U_new^T [128 x NS] * ext^T
 // The A operands are written by the threads that compute them, straight into
 // the K-major no-swizzle canonical layout (8-row x 16-byte core matrices);
 // the operators are packed in that layout on the host.  Tiles move by TMA as
-// in k_elem_tma (same tensor maps, 32-element boxes).  Orders 1..4 (the
-// operators of order 5 and all 3-D operators do not fit next to the tiles in
-// shared memory).
+// in k_elem_tma (same tensor maps, EB-element boxes).  2-D orders 1..4 and
+// 3-D order 1: the split dense operators and the A operands of larger orders
+// do not fit next to the tiles in shared memory (3-D P2: 287 KB of 227).
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -37,12 +39,13 @@ constexpr int r8(int x) { return (x + 7) / 8 * 8; }
 constexpr int r16(int x) { return (x + 15) / 16 * 16; }
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-template <int P>
+template <int ND, int P>
 struct Tc {
-  static constexpr int N = P + 1, NS = N * N, NFP = 4 * N, NF = 4, EB = 32, M = 128, NT = 128;
-  static constexpr int ROW = EB * NF;  // 128 values per point row of a tile
+  static constexpr int N = P + 1, NS = ND == 2 ? N * N : N * N * N, NFP = 2 * ND * (ND == 2 ? N : N * N);
+  static constexpr int NF = ND + 2, EB = ND == 2 ? 32 : 24, M = 128, NT = 128;
+  static constexpr int ROW = EB * NF;  // values per point row of a tile: 128 (2-D), 120 (3-D)
   static constexpr int NSp = r16(NS), NFPp = r16(NFP), N1 = NSp + NFPp;
-  static constexpr int K1p = r8(2 * NS), K2p = r8(NFP), K3p = r8(NS);
+  static constexpr int K1p = r8(ND * NS), K2p = r8(NFP), K3p = r8(NS);
   static constexpr int KAp = cmax(K1p, cmax(K2p, K3p));
   static constexpr int SB1 = N1 * K1p, SB2 = NSp * K2p, SB3 = NFPp * K3p;
   static constexpr int O_B1H = 0, O_B1L = SB1, O_B2H = 2 * SB1, O_B2L = 2 * SB1 + SB2;
@@ -59,11 +62,12 @@ struct Tc {
   static constexpr int O_CMP = O_ACC + al(NS * ROW);
   static constexpr int O_FN = O_CMP + al(NS * ROW);
   static constexpr int O_J = O_FN + al(NFP * ROW);
-  static constexpr int O_DET = O_J + al(2 * NS * EB * 2);
+  static constexpr int O_DET = O_J + al(ND * NS * EB * ND);
   static constexpr int O_BAR = O_DET + al(NS * EB);
   static constexpr size_t SMEM = 4 * (size_t)(O_BAR + 32) + 128;
   static_assert(SMEM <= 227 * 1024, "tensor-core tile set does not fit in shared memory");
   static_assert(N1 <= 256 && N1 % 16 == 0, "MMA N");
+  static_assert(ROW <= M, "element tile rows exceed the MMA rows");
 };
 
 // float offset of (row r, column k) in a K-major no-swizzle operand whose K
@@ -101,13 +105,13 @@ __device__ __forceinline__ void two_sum_tc(float a, float b, float &s, float &e)
 
 constexpr uint32_t kWait = 1u << 22;
 
-template <int P>
-__global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const float *__restrict__ ops,
-                                                   const __grid_constant__ TmaMaps mp) {
+template <int ND, int P>
+__global__ void __launch_bounds__(128) k_elem_tc(ElemArgsT<float> a, const float *__restrict__ ops,
+                                                 const __grid_constant__ TmaMaps mp) {
   pdl_wait();
   pdl_trigger();
-  using T = Tc<P>;
-  constexpr int NS = T::NS, NFP = T::NFP, NF = 4, EB = 32, ROW = T::ROW;
+  using T = Tc<ND, P>;
+  constexpr int NS = T::NS, NFP = T::NFP, NF = T::NF, EB = T::EB, ROW = T::ROW;
   constexpr int NSp = T::NSp, K1p = T::K1p, K2p = T::K2p, K3p = T::K3p;
   extern __shared__ __align__(128) unsigned char smem_bytes[];
   float *sm = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(smem_bytes) + 127) & ~uintptr_t(127));
@@ -121,9 +125,10 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
   const int tid = threadIdx.x, warp = tid >> 5;
   const int E = a.E, e0 = blockIdx.x * EB;
   const int nValid = min(EB, E - e0);
-  const int r = tid;                 // this thread's MMA row / TMEM lane: (element r/4, field r%4)
-  const int re = r >> 2;
-  const bool rvalid = re < nValid;
+  const int r = tid;                 // this thread's MMA row / TMEM lane: (element r/NF, field r%NF)
+  const int re = r / NF;
+  const bool rrow = r < ROW;         // rows ROW..127 (3-D) are padding: zero A rows, no tile access
+  const bool rvalid = rrow && re < nValid;
 
   const bool finalStage = a.mode == MODE_RK_FINAL || (a.mode == MODE_JAMESON && a.stage == a.nRK - 1);
   const bool needU0 = ((a.mode == MODE_RK_STAGE || a.mode == MODE_JAMESON) && a.stage > 0) ||
@@ -147,9 +152,9 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
   const uint32_t tlane = tbase + ((uint32_t)(warp * 32) << 16);
 
   if (tid == 0) {
-    mbar_arrive_expect_tx(&bar[0], 4u * (NS * ROW + 2 * NS * EB * 2));
+    mbar_arrive_expect_tx(&bar[0], 4u * (NS * ROW + ND * NS * EB * ND));
     tma_load_2d(sU, &mp.U, e0 * NF, 0, &bar[0]);
-    tma_load_3d(sJ, &mp.J, e0 * 2, 0, 0, &bar[0]);
+    tma_load_3d(sJ, &mp.J, e0 * ND, 0, 0, &bar[0]);
     uint32_t bytes = 4u * NFP * ROW;
     if (needU0) bytes += 4u * NS * ROW;
     if (needAcc) bytes += 4u * NS * ROW;
@@ -166,10 +171,18 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
   // columns of the first A operand
   for (int i = tid; i < T::OPS / 4; i += 128)
     reinterpret_cast<float4 *>(sOps)[i] = reinterpret_cast<const float4 *>(ops)[i];
-  constexpr int PAD1 = K1p - 2 * NS;
+  constexpr int PAD1 = K1p - ND * NS;
   if constexpr (PAD1 > 0) {
     for (int i = tid; i < 128 * PAD1; i += 128) {
-      const int rr = i / PAD1, k = 2 * NS + i % PAD1;
+      const int rr = i / PAD1, k = ND * NS + i % PAD1;
+      sAh[blk(rr, k, K1p)] = 0.0f;
+      sAl[blk(rr, k, K1p)] = 0.0f;
+    }
+  }
+  // padding rows of the first A operand (the flux loop writes rows < ROW)
+  if constexpr (ROW < 128) {
+    for (int i = tid; i < (128 - ROW) * ND * NS; i += 128) {
+      const int rr = ROW + i / (ND * NS), k = i % (ND * NS);
       sAh[blk(rr, k, K1p)] = 0.0f;
       sAl[blk(rr, k, K1p)] = 0.0f;
     }
@@ -185,23 +198,23 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
     // flux at (s, el): reference-space F_d into the A operand, column d*NS + s
     for (int it = tid; it < NS * EB; it += 128) {
       const int s = it / EB, el = it - (it / EB) * EB;
-      float Fp[2][NF];
+      float Fp[ND][NF];
       if (el < nValid) {
-        inviscid_flux<2, float>(&sU[s * ROW + el * NF], Fp, float(a.gamma));
+        inviscid_flux<ND, float>(&sU[s * ROW + el * NF], Fp, float(a.gamma));
       } else {
 #pragma unroll
-        for (int d = 0; d < 2; d++)
+        for (int d = 0; d < ND; d++)
 #pragma unroll
           for (int k = 0; k < NF; k++) Fp[d][k] = 0.0f;
       }
 #pragma unroll
-      for (int d1 = 0; d1 < 2; d1++) {
-        const float *Jr = &sJ[(d1 * NS + s) * EB * 2 + el * 2];
+      for (int d1 = 0; d1 < ND; d1++) {
+        const float *Jr = &sJ[(d1 * NS + s) * EB * ND + el * ND];
 #pragma unroll
         for (int k = 0; k < NF; k++) {
           float f = 0.0f;
 #pragma unroll
-          for (int d2 = 0; d2 < 2; d2++) f += Jr[d2] * Fp[d2][k];
+          for (int d2 = 0; d2 < ND; d2++) f += Jr[d2] * Fp[d2][k];
           split_store(sAh, sAl, blk(el * NF + k, d1 * NS + s, K1p), f);
           if (a.F_dbg && el < nValid) a.F_dbg[(((long long)d1 * NS + s) * E + e0 + el) * NF + k] = f;
         }
@@ -228,7 +241,7 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
       for (int i = 0; i < 8; i++) {
         const int f = c + i;
         if (f < NFP) {
-          const float q = sFn[f * ROW + r] - v[i];
+          const float q = rrow ? sFn[f * ROW + r] - v[i] : 0.0f;
           split_store(sAh, sAl, blk(r, f, K2p), q);
           if (a.disFn_dbg && rvalid) a.disFn_dbg[((long long)f * E + e0) * NF + r] = q;
         } else if (f < K2p) {
@@ -266,6 +279,11 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
       for (int i = 0; i < 8; i++) {
         const int s = c + i;
         if (s >= NS) break;
+        if (!rrow) {  // padding row: a zero row of the third A operand
+          sAh[blk(r, s, K3p)] = 0.0f;
+          sAl[blk(r, s, K3p)] = 0.0f;
+          continue;
+        }
         const int li = s * ROW + r;
         const long long gi = ((long long)s * E + e0) * NF + r;
         float dv = v[i];
@@ -324,7 +342,7 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
           tmem_ld8(tlane + NSp + c, v);
 #pragma unroll
           for (int i = 0; i < 8; i++)
-            if (c + i < NFP) sFn[(c + i) * ROW + r] = v[i];
+            if (c + i < NFP && rrow) sFn[(c + i) * ROW + r] = v[i];
         }
         fence_async_smem();
         __syncthreads();
@@ -351,12 +369,12 @@ __global__ void __launch_bounds__(128) k_elem_tc2d(ElemArgsT<float> a, const flo
   if (warp == 0) tmem_dealloc(tbase, T::TCOLS);
 }
 
-template <int P>
+template <int ND, int P>
 void launch_tc(const ElemArgsT<float> &a, const float *ops, const TmaMaps &m, cudaStream_t st) {
-  using T = Tc<P>;
+  using T = Tc<ND, P>;
   static std::atomic<unsigned long long> attrDev{0};
-  smem_attr(k_elem_tc2d<P>, (int)T::SMEM, attrDev);
-  launch_k(k_elem_tc2d<P>, (a.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, a, ops, m);
+  smem_attr(k_elem_tc<ND, P>, (int)T::SMEM, attrDev);
+  launch_k(k_elem_tc<ND, P>, (a.E + T::EB - 1) / T::EB, T::NT, T::SMEM, st, a, ops, m);
 }
 
 // host TF32 rounding, nearest with ties away from zero (as cvt.rna), low 13
@@ -370,10 +388,10 @@ float tf32_host(double x) {
   return f;
 }
 
-template <int P>
-void pack(const double *const grad[2], const double *const extFn[2], const double *corr, const double *ext,
+template <int ND, int P>
+void pack(const double *const grad[3], const double *const extFn[3], const double *corr, const double *ext,
           std::vector<float> &blob) {
-  using T = Tc<P>;
+  using T = Tc<ND, P>;
   constexpr int NS = T::NS, NFP = T::NFP;
   blob.assign(T::OPS, 0.0f);
   auto put = [&](int oH, int oL, int row, int k, int Kp, double x) {
@@ -381,7 +399,7 @@ void pack(const double *const grad[2], const double *const extFn[2], const doubl
     blob[oH + blk(row, k, Kp)] = h;
     blob[oL + blk(row, k, Kp)] = tf32_host(x - (double)h);
   };
-  for (int d = 0; d < 2; d++)
+  for (int d = 0; d < ND; d++)
     for (int s = 0; s < NS; s++) {
       for (int n = 0; n < NS; n++) put(T::O_B1H, T::O_B1L, n, d * NS + s, T::K1p, grad[d][(size_t)n * NS + s]);
       for (int f = 0; f < NFP; f++)
@@ -395,37 +413,53 @@ void pack(const double *const grad[2], const double *const extFn[2], const doubl
 
 }  // namespace
 
-bool tc2d_supported(int nDims, int order) { return nDims == 2 && order >= 1 && order <= 4; }
+bool tc_supported(int nDims, int order) {
+  return (nDims == 2 && order >= 1 && order <= 4) || (nDims == 3 && order == 1);
+}
 
-bool tc2d_pack_ops(int order, const double *const grad[2], const double *const extFn[2], const double *corr,
-                   const double *ext, std::vector<float> &blob) {
+int tc_elems_per_block(int nDims, int order) {
+  return tc_supported(nDims, order) ? (nDims == 2 ? Tc<2, 1>::EB : Tc<3, 1>::EB) : 0;
+}
+
+bool tc_pack_ops(int nDims, int order, const double *const grad[3], const double *const extFn[3],
+                 const double *corr, const double *ext, std::vector<float> &blob) {
+  if (nDims == 3) {
+    if (order != 1) return false;
+    pack<3, 1>(grad, extFn, corr, ext, blob);
+    return true;
+  }
   switch (order) {
-    case 1: pack<1>(grad, extFn, corr, ext, blob); return true;
-    case 2: pack<2>(grad, extFn, corr, ext, blob); return true;
-    case 3: pack<3>(grad, extFn, corr, ext, blob); return true;
-    case 4: pack<4>(grad, extFn, corr, ext, blob); return true;
+    case 1: pack<2, 1>(grad, extFn, corr, ext, blob); return true;
+    case 2: pack<2, 2>(grad, extFn, corr, ext, blob); return true;
+    case 3: pack<2, 3>(grad, extFn, corr, ext, blob); return true;
+    case 4: pack<2, 4>(grad, extFn, corr, ext, blob); return true;
     default: return false;
   }
 }
 
-size_t tc2d_smem_bytes(int order) {
+size_t tc_smem_bytes(int nDims, int order) {
+  if (nDims == 3) return order == 1 ? Tc<3, 1>::SMEM : 0;
   switch (order) {
-    case 1: return Tc<1>::SMEM;
-    case 2: return Tc<2>::SMEM;
-    case 3: return Tc<3>::SMEM;
-    case 4: return Tc<4>::SMEM;
+    case 1: return Tc<2, 1>::SMEM;
+    case 2: return Tc<2, 2>::SMEM;
+    case 3: return Tc<2, 3>::SMEM;
+    case 4: return Tc<2, 4>::SMEM;
     default: return 0;
   }
 }
 
-void launch_element_stage_tc2d(int order, const ElemArgsT<float> &a, const float *ops, const TmaMaps &m,
-                               cudaStream_t st) {
+void launch_element_stage_tc(int nDims, int order, const ElemArgsT<float> &a, const float *ops, const TmaMaps &m,
+                             cudaStream_t st) {
   if (a.E <= 0) return;
+  if (nDims == 3) {
+    if (order == 1) launch_tc<3, 1>(a, ops, m, st);
+    return;
+  }
   switch (order) {
-    case 1: return launch_tc<1>(a, ops, m, st);
-    case 2: return launch_tc<2>(a, ops, m, st);
-    case 3: return launch_tc<3>(a, ops, m, st);
-    case 4: return launch_tc<4>(a, ops, m, st);
+    case 1: return launch_tc<2, 1>(a, ops, m, st);
+    case 2: return launch_tc<2, 2>(a, ops, m, st);
+    case 3: return launch_tc<2, 3>(a, ops, m, st);
+    case 4: return launch_tc<2, 4>(a, ops, m, st);
     default: return;
   }
 }

@@ -790,7 +790,7 @@ int tma_elems_per_block<double>(int nDims, int order, int v) {
 }
 template <>
 int tma_elems_per_block<float>(int nDims, int order, int v) {
-  if (v == kFp32Variants) return tc2d_supported(nDims, order) ? 32 : 0;  // the tensor-core variant
+  if (v == kFp32Variants) return tc_elems_per_block(nDims, order);  // the tensor-core variant
   return v == 0 ? eb_of<float, 0>(nDims, order) : v == 1 ? eb_of<float, 1>(nDims, order) : eb_of<float, 2>(nDims, order);
 }
 template <>

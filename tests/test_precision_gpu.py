@@ -163,7 +163,8 @@ def test_mixed_batch_equals_alone(tmp_path):
 
 
 TC_CASES = ["vortex2d_p3_8", "channel2d_p2", "roe2d_p2", "hu2d_p3", "cplus2d_p2", "lobatto_sd2d_p4",
-            "jameson5_2d_p2", "euler_fwd2d_p1", "localdt_jameson2d_p3", "ic1_2d_p3"]
+            "jameson5_2d_p2", "euler_fwd2d_p1", "localdt_jameson2d_p3", "ic1_2d_p3",
+            "p1_3d"]  # 3-D: order 1 (24 elements and 120 of the 128 MMA rows per CTA)
 
 
 def tensor_case(meta, **kw):
@@ -190,8 +191,9 @@ def test_tensor_core_variant_residual_and_steps(case):
     assert rel_l2(s2.get_state(), a["U_final"]) < L2_TOL
 
 
-def test_tensor_core_variant_near_cuda_core_variant():
-    a, meta = load_golden("vortex2d_p3_8")
+@pytest.mark.parametrize("case", ["vortex2d_p3_8", "p1_3d"])
+def test_tensor_core_variant_near_cuda_core_variant(case):
+    a, meta = load_golden(case)
     out = []
     for v in (0, 3):
         s = mixed_case(meta, tile_variant=v)
