@@ -369,17 +369,19 @@ def test_residual_norm_matches_reference(case):
         assert np.allclose(s.residual_norm(rt), z[case + "__final"][rt - 1], rtol=1e-7, atol=0), rt
 
 
-def test_tgv16_matches_reference_element_sums():
-    """3-D Taylor-Green vortex, 16^3 hexes, P3, FP64, from the product's own
-    initial condition: per-element sums of the initial state (1e-14), of the
-    residual (1e-12 of the flux scale) and of the state after 5 RK4 steps
-    (1e-10) against the reference's, and the residual norms."""
+@pytest.mark.parametrize("n", [16, 32])
+def test_tgv_matches_reference_element_sums(n):
+    """3-D Taylor-Green vortex, 16^3 and 32^3 hexes (the benchmark's own
+    workload), P3, FP64, from the product's own initial condition:
+    per-element sums of the initial state (1e-14), of the residual (1e-12 of
+    the flux scale) and of the state after 5 RK4 steps (1e-10) against the
+    reference's, and the residual norms."""
     import json
     import os
 
     from conftest import ROOT
 
-    z = np.load(os.path.join(ROOT, "tests", "golden", "tgv3d_p3_16_sums.npz"))
+    z = np.load(os.path.join(ROOT, "tests", "golden", f"tgv3d_p3_{n}_sums.npz"))
     meta = json.loads(str(z["meta"]))
     s = fb.Solver(deck_path(meta))
     s.initialize_solution(fb.IC_TGV, (0.1,))
