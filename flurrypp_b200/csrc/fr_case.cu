@@ -926,6 +926,18 @@ struct fr_case {
           if (op.extFn[d][(size_t)f * nS + c] != (on && d == dn ? EF[side * n + b[dn]] : 0.0)) return false;
       }
     }
+    // the two flux points at the ends of each line (side 0 first), so that
+    // one pass over a line's points extrapolates to both
+    std::vector<int> pair;
+    for (int f = 0; f < nFp; f++) {
+      if (fSide[f] != 0) continue;
+      int g = -1;
+      for (int h = 0; h < nFp; h++)
+        if (fSide[h] == 1 && fBase[h] == fBase[f] && fDn[h] == fDn[f]) g = h;
+      if (g < 0) return false;
+      pair.push_back(f | g << 16);
+    }
+    if ((int)pair.size() * 2 != nFp) return false;
     const int nFaces = 2 * nDims;
     std::vector<int> cF((size_t)nS * nFaces);
     std::vector<double> cV((size_t)nS * nFaces);
@@ -953,10 +965,11 @@ struct fr_case {
         if (cF[(size_t)sp * nFaces + fc] <= cF[(size_t)sp * nFaces + fc - 1]) return false;
     }
     double *dD, *dE1, *dEF, *dcV;
-    int *dfB, *dfD, *dfS, *dcF;
+    int *dfB, *dfD, *dfS, *dcF, *dLP;
     if (!upload(dD, D) || !upload(dE1, E1) || !upload(dEF, EF) || !upload(dfB, fBase) || !upload(dfD, fDn) ||
-        !upload(dfS, fSide) || !upload(dcF, cF) || !upload(dcV, cV))
+        !upload(dfS, fSide) || !upload(dcF, cF) || !upload(dcV, cV) || !upload(dLP, pair))
       return false;
+    tp.linePair = f32.tp.linePair = dLP;
     tp.D = dD;
     tp.E1 = dE1;
     tp.EFn1 = dEF;

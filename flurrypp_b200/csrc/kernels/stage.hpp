@@ -149,6 +149,7 @@ struct TpTablesT {
   const int *fptBase = nullptr;     // [nFp] first solution point of the line
   const int *fptDn = nullptr;       // [nFp] normal dimension
   const int *fptSide = nullptr;     // [nFp]
+  const int *linePair = nullptr;    // [nFp/2] the two ends of a line: side-0 fpt | side-1 fpt << 16
   const int *corrFpt = nullptr;     // [nS][2*nDims]
   const R *corrVal = nullptr;       // [nS][2*nDims]
 };

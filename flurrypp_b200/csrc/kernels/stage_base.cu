@@ -119,11 +119,17 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
 // points per thread at 128 threads per CTA keep a third more loads in flight
 // per SM than one point per thread at the register-limited occupancy
 // (measured: 3-D FP64 faces 0.090 -> 0.083 ms, FP32 0.054 -> 0.050 ms).
+// The FP64 3-D kernel's registers are capped for five CTAs per SM (118
+// uncapped, 96 with 76 bytes spilled: 0.0835 -> 0.0799 ms at 32^3 P3; a cap
+// of 80 for six CTAs, 124 bytes spilled, is slower, 0.0864 ms).  The FP32
+// kernels are below the cap; the 2-D FP64 one (112) is left uncapped.
 constexpr int kFacePpt = 2, kFaceNt = 128;
+template <int ND, typename R>
+constexpr int face_min_ctas() { return ND == 3 && sizeof(R) == 8 ? 5 : 1; }
 
 
 template <int ND, typename R, int PPT>
-__global__ void __launch_bounds__(kFaceNt) k_faces_interior_ilp(int n, const int *__restrict__ slotL,
+__global__ void __launch_bounds__(kFaceNt, face_min_ctas<ND, R>()) k_faces_interior_ilp(int n, const int *__restrict__ slotL,
                                                            const int *__restrict__ slotR, const R *__restrict__ nrm,
                                                            const R *__restrict__ dAL, const R *__restrict__ dAR,
                                                            const R *__restrict__ Uf, R *__restrict__ Fn,

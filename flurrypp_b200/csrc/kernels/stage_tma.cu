@@ -102,8 +102,8 @@ struct Tm {
   static constexpr bool GTAB = !VS;
   static constexpr int NCT = GTAB ? 0 : NS * 2 * ND;
   static constexpr int O_CV = O_TAB + al(N * N + 4 * N);
-  static constexpr int O_IDX = O_CV + al(NCT);                // ints: fpt line [NFP], corrFpt
-  static constexpr int O_BAR = O_IDX + al((int)((NFP + NCT) * 4 / sizeof(R)) + 1);
+  static constexpr int O_IDX = O_CV + al(NCT);  // ints: fpt line [NFP], corrFpt [NCT], line ends [NFP/2]
+  static constexpr int O_BAR = O_IDX + al((int)((NFP + NCT + NFP / 2) * 4 / sizeof(R)) + 1);
   static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
   static_assert(SMEM <= kMaxSmem, "TMA tile set does not fit in shared memory");
   static_assert(NT <= 1024, "too many threads");
@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
   R *sCV = smem + T::O_CV;
   int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);  // base | dn << 16 | side << 20
   int *sCF = sLine + NFP;
+  int *sPair = sCF + T::NCT;  // side-0 fpt | side-1 fpt << 16 of each line
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::O_BAR);
 
   const int E = a.E;
@@ -241,6 +242,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     sEF[i] = t.EFn1[i];
   }
   for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
+  for (int i = tid; i < NFP / 2; i += NT) sPair[i] = t.linePair[i];
   if constexpr (!T::GTAB)
     for (int i = tid; i < NS * 2 * ND; i += NT) {
       sCF[i] = t.corrFpt[i];
@@ -365,32 +367,41 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     return;
   }
 
-  // C2: Fn - extrapolated normal flux, in place in the Fn tile
-  for (int it = tid; it < NFP * EB; it += NT) {
-    const int f = it / EB, fe = it - (it / EB) * EB;
-    const int ln = sLine[f];
-    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
+  // C2: Fn - extrapolated normal flux, in place in the Fn tile; one pass
+  // over a line's points gives both of its ends
+  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+    const int l = it / EB, fe = it - (it / EB) * EB;
+    const int pr = sPair[l];
+    const int ln = sLine[pr & 0xffff];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[NF];
+    R acc[2][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[k] = R(0);
+    for (int k = 0; k < NF; k++) acc[0][k] = acc[1][k] = R(0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev = sEF[side * N + m];
+      const R ev0 = sEF[m], ev1 = sEF[N + m];
       R x[NF];
       ldp<NF, R>(&sF[fidx(dn, base + m * stride) + fe * NF], x);
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+      for (int k = 0; k < NF; k++) {
+        acc[0][k] += ev0 * x[k];
+        acc[1][k] += ev1 * x[k];
+      }
     }
-    R *q = &sFn[f * ROW + fe * NF];
-    R qv[NF];
-    ldp<NF, R>(q, qv);
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      qv[k] = qv[k] - acc[k];
-      if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = qv[k];
+    for (int side = 0; side < 2; side++) {
+      const int f = side ? pr >> 16 : pr & 0xffff;
+      R *q = &sFn[f * ROW + fe * NF];
+      R qv[NF];
+      ldp<NF, R>(q, qv);
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        qv[k] = qv[k] - acc[side][k];
+        if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = qv[k];
+      }
+      stp<NF, R>(q, qv);
     }
-    stp<NF, R>(q, qv);
   }
   if (tid == 0) tma_wait_read_all();  // the U0 store has read sU
   __syncthreads();
@@ -490,27 +501,33 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     return;
   }
 
-  // E: new state at the flux points, into the Fn tile
-  for (int it = tid; it < NFP * EB; it += NT) {
-    const int f = it / EB, fe = it - (it / EB) * EB;
-    const int ln = sLine[f];
-    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
+  // E: new state at the flux points, into the Fn tile (both ends of a line
+  // per pass)
+  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+    const int l = it / EB, fe = it - (it / EB) * EB;
+    const int pr = sPair[l];
+    const int ln = sLine[pr & 0xffff];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[NF];
+    R acc[2][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[k] = R(0);
+    for (int k = 0; k < NF; k++) acc[0][k] = acc[1][k] = R(0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev = sE[side * N + m];
+      const R ev0 = sE[m], ev1 = sE[N + m];
       R x[NF];
       if (PADDED)
         ldp<NF, R>(&sF[fidx(0, base + m * stride) + fe * NF], x);
       else
         ldp<NF, R>(&sU[(base + m * stride) * ROW + fe * NF], x);
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+      for (int k = 0; k < NF; k++) {
+        acc[0][k] += ev0 * x[k];
+        acc[1][k] += ev1 * x[k];
+      }
     }
-    stp<NF, R>(&sFn[f * ROW + fe * NF], acc);
+    stp<NF, R>(&sFn[(pr & 0xffff) * ROW + fe * NF], acc[0]);
+    stp<NF, R>(&sFn[(pr >> 16) * ROW + fe * NF], acc[1]);
   }
   fence_async_smem();
   __syncthreads();
@@ -590,7 +607,7 @@ struct Tg2 {
   static constexpr int O_TAB = O_G + al(ND * NS * ROW);
   static constexpr int O_CV = O_TAB + al(N * N + 2 * N);
   static constexpr int O_IDX = O_CV + al(NS * 2 * ND);
-  static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1);
+  static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND + NFP / 2) * 4 / sizeof(R)) + 1);
   static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
   static_assert(SMEM <= kMaxSmem, "gradient tile set does not fit in shared memory");
 };
@@ -615,6 +632,7 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
   R *sCV = smem + T::O_CV;
   int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);
   int *sCF = sLine + NFP;
+  int *sPair = sCF + NS * 2 * ND;  // side-0 fpt | side-1 fpt << 16 of each line
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::O_BAR);
 
   const int e0 = blockIdx.x * EB;
@@ -638,6 +656,7 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
   for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
   for (int i = tid; i < 2 * N; i += NT) sE[i] = t.E1[i];
   for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
+  for (int i = tid; i < NFP / 2; i += NT) sPair[i] = t.linePair[i];
   for (int i = tid; i < NS * 2 * ND; i += NT) {
     sCF[i] = t.corrFpt[i];
     sCV[i] = t.corrVal[i];
@@ -708,25 +727,35 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
     tma_store_3d(&mp.dUs, e0 * NF, 0, 0, sG);
     tma_commit();
   }
-  for (int it = tid; it < NFP * EB; it += NT) {
-    const int f = it / EB, fe = it - (it / EB) * EB;
-    const int ln = sLine[f];
-    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side = ln >> 20;
+  // both ends of a line per pass over its points
+  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+    const int l = it / EB, fe = it - (it / EB) * EB;
+    const int pr = sPair[l];
+    const int f0 = pr & 0xffff, f1 = pr >> 16;
+    const int ln = sLine[f0];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-      R acc[NF];
+      R acc0[NF], acc1[NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+      for (int k = 0; k < NF; k++) acc0[k] = acc1[k] = R(0.0);
 #pragma unroll
       for (int m = 0; m < N; m++) {
-        const R ev = sE[side * N + m];
+        const R ev0 = sE[m], ev1 = sE[N + m];
         const R *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
-        for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+        for (int k = 0; k < NF; k++) {
+          const R xv = x[k];
+          acc0[k] += ev0 * xv;
+          acc1[k] += ev1 * xv;
+        }
       }
 #pragma unroll
-      for (int k = 0; k < NF; k++) sGf[(d * NFP + f) * ROW + fe * NF + k] = acc[k];
+      for (int k = 0; k < NF; k++) {
+        sGf[(d * NFP + f0) * ROW + fe * NF + k] = acc0[k];
+        sGf[(d * NFP + f1) * ROW + fe * NF + k] = acc1[k];
+      }
     }
   }
   fence_async_smem();

@@ -108,8 +108,12 @@ __device__ __forceinline__ void ldg_interior_flux(const R *UL, const R *UR,
     for (int k = 0; k < NF; k++) Fn[k] += Fc[d][k] * n[d];
 }
 
+// Registers capped for four 128-thread CTAs per SM: the FP64 3-D kernel
+// needs 148 uncapped (three CTAs) and spills 48 bytes at 128 (NS TGV 40^3
+// P4 face pass 1.707 -> 1.659 ms; a cap of 96, 196 bytes spilled, is
+// slower); the FP32 and 2-D kernels are below the cap.
 template <int ND, typename R>
-__global__ void k_faces_visc_interior(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
+__global__ void __launch_bounds__(128, 4) k_faces_visc_interior(int n, const int *__restrict__ slotL, const int *__restrict__ slotR,
                                       const R *__restrict__ nrm, const R *__restrict__ dAL,
                                       const R *__restrict__ dAR, const R *__restrict__ Uf,
                                       const R *__restrict__ dUf, long long dStride, R *__restrict__ Fn,
