@@ -154,28 +154,39 @@ __device__ __forceinline__ void elem_tp_block(const ElemArgsT<R> &a, const TpTab
     for (int k = 0; k < NF; k++) div[k] = d == 0 ? acc[k] : div[k] + acc[k];
   }
 
-  // C2: Fn - extrapolated normal flux at every (fpt, el)
-  for (int it = tid; act && it < NFP * EB; it += NT) {
-    const int f = it / EB, fe = it - (it / EB) * EB;
+  // C2: Fn - extrapolated normal flux at every (fpt, el); one pass over a
+  // line's points gives both of its ends
+  for (int it = tid; act && it < (NFP / 2) * EB; it += NT) {
+    const int l = it / EB, fe = it - (it / EB) * EB;
     const int ee = e0 + fe;
-    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int pr = __ldg(&t.linePair[l]);
+    const int f0 = pr & 0xffff;
+    const int base = __ldg(&t.fptBase[f0]), dn = __ldg(&t.fptDn[f0]);
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[NF];
+    R acc[2][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+    for (int k = 0; k < NF; k++) acc[0][k] = acc[1][k] = R(0.0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev = sEF[side * N + m];
+      const R ev0 = sEF[m], ev1 = sEF[N + m];
       const R *x = &sF[(dn * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+      for (int k = 0; k < NF; k++) {
+        const R xv = x[k];
+        acc[0][k] += ev0 * xv;
+        acc[1][k] += ev1 * xv;
+      }
     }
     const bool v = fe < nValid;
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const R q = v ? a.Fn[((long long)f * E + ee) * NF + k] - acc[k] : R(0.0);
-      sQ[f * ROW + fe * NF + k] = q;
-      if (a.disFn_dbg && v) a.disFn_dbg[((long long)f * E + ee) * NF + k] = q;
+    for (int side = 0; side < 2; side++) {
+      const int f = side ? pr >> 16 : f0;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        const R q = v ? a.Fn[((long long)f * E + ee) * NF + k] - acc[side][k] : R(0.0);
+        sQ[f * ROW + fe * NF + k] = q;
+        if (a.disFn_dbg && v) a.disFn_dbg[((long long)f * E + ee) * NF + k] = q;
+      }
     }
   }
   __syncthreads();
@@ -249,25 +260,34 @@ __device__ __forceinline__ void elem_tp_block(const ElemArgsT<R> &a, const TpTab
   if (a.mode == MODE_RESIDUAL || !a.Ufpts_out) return;
   __syncthreads();
 
-  // E: new state at the flux points
-  for (int it = tid; act && it < NFP * EB; it += NT) {
-    const int f = it / EB, fe = it - (it / EB) * EB;
+  // E: new state at the flux points (both ends of a line per pass)
+  for (int it = tid; act && it < (NFP / 2) * EB; it += NT) {
+    const int l = it / EB, fe = it - (it / EB) * EB;
     if (fe >= nValid) continue;
     const int ee = e0 + fe;
-    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int pr = __ldg(&t.linePair[l]);
+    const int f0 = pr & 0xffff, f1 = pr >> 16;
+    const int base = __ldg(&t.fptBase[f0]), dn = __ldg(&t.fptDn[f0]);
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[NF];
+    R acc0[NF], acc1[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+    for (int k = 0; k < NF; k++) acc0[k] = acc1[k] = R(0.0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev = sE[side * N + m];
+      const R ev0 = sE[m], ev1 = sE[N + m];
       const R *x = &sU[(base + m * stride) * ROW + fe * NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+      for (int k = 0; k < NF; k++) {
+        const R xv = x[k];
+        acc0[k] += ev0 * xv;
+        acc1[k] += ev1 * xv;
+      }
     }
 #pragma unroll
-    for (int k = 0; k < NF; k++) a.Ufpts_out[((long long)f * E + ee) * NF + k] = acc[k];
+    for (int k = 0; k < NF; k++) {
+      a.Ufpts_out[((long long)f0 * E + ee) * NF + k] = acc0[k];
+      a.Ufpts_out[((long long)f1 * E + ee) * NF + k] = acc1[k];
+    }
   }
 }
 

@@ -322,25 +322,35 @@ __global__ void __launch_bounds__(Tg<ND, P, R>::NT) k_elem_grad(GradArgsT<R> g, 
       if (valid) g.dUs[(long long)d2 * g.sStride + ((long long)s * E + e) * NF + k] = v;
     }
   __syncthreads();
-  for (int it = tid; it < NFP * EB; it += NT) {
-    const int f = it / EB, fe = it - (it / EB) * EB;
+  // both ends of a line per pass over its points
+  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+    const int l = it / EB, fe = it - (it / EB) * EB;
     if (fe >= nValid) continue;
-    const int base = __ldg(&t.fptBase[f]), dn = __ldg(&t.fptDn[f]), side = __ldg(&t.fptSide[f]);
+    const int pr = __ldg(&t.linePair[l]);
+    const int f0 = pr & 0xffff, f1 = pr >> 16;
+    const int base = __ldg(&t.fptBase[f0]), dn = __ldg(&t.fptDn[f0]);
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-      R acc[NF];
+      R acc0[NF], acc1[NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+      for (int k = 0; k < NF; k++) acc0[k] = acc1[k] = R(0.0);
 #pragma unroll
       for (int m = 0; m < N; m++) {
-        const R ev = sE[side * N + m];
+        const R ev0 = sE[m], ev1 = sE[N + m];
         const R *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
-        for (int k = 0; k < NF; k++) acc[k] += ev * x[k];
+        for (int k = 0; k < NF; k++) {
+          const R xv = x[k];
+          acc0[k] += ev0 * xv;
+          acc1[k] += ev1 * xv;
+        }
       }
 #pragma unroll
-      for (int k = 0; k < NF; k++) g.dUf[(long long)d * g.fStride + ((long long)f * E + e0 + fe) * NF + k] = acc[k];
+      for (int k = 0; k < NF; k++) {
+        g.dUf[(long long)d * g.fStride + ((long long)f0 * E + e0 + fe) * NF + k] = acc0[k];
+        g.dUf[(long long)d * g.fStride + ((long long)f1 * E + e0 + fe) * NF + k] = acc1[k];
+      }
     }
   }
 }
