@@ -122,10 +122,11 @@ __global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__rest
 // The FP64 3-D kernel's registers are capped for five CTAs per SM (118
 // uncapped, 96 with 76 bytes spilled: 0.0835 -> 0.0799 ms at 32^3 P3; a cap
 // of 80 for six CTAs, 124 bytes spilled, is slower, 0.0864 ms).  The FP32
-// kernels are below the cap; the 2-D FP64 one (112) is left uncapped.
+// kernels are below the cap; the 2-D FP64 one (112) is left uncapped (0:
+// no minimum, which leaves its register allocation as without the bound).
 constexpr int kFacePpt = 2, kFaceNt = 128;
 template <int ND, typename R>
-constexpr int face_min_ctas() { return ND == 3 && sizeof(R) == 8 ? 5 : 1; }
+constexpr int face_min_ctas() { return ND == 3 && sizeof(R) == 8 ? 5 : 0; }
 
 
 template <int ND, typename R, int PPT>

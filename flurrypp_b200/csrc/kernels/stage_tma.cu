@@ -86,6 +86,9 @@ struct Tm {
   static constexpr int EB = F32 ? shrink(eb32_want()) : shrink64(eb64());
   static constexpr int NT = NS * EB;
   static constexpr int ROW = EB * NF;
+  // the flux-point phases take one line (both of its ends) per thread where
+  // one flux point per thread would need more than one round of the CTA
+  static constexpr bool PAIR = NFP * EB > NT;
   static constexpr int SLAB = NS * ROW + padF();  // one dimension's flux tile
   static constexpr int O_U = 0;
   static constexpr int O_U0 = O_U + al(NS * ROW);
@@ -367,37 +370,40 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     return;
   }
 
-  // C2: Fn - extrapolated normal flux, in place in the Fn tile; one pass
-  // over a line's points gives both of its ends
-  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+  // C2: Fn - extrapolated normal flux, in place in the Fn tile, per flux
+  // point or (PAIR) per line: one pass over a line's points gives both ends
+  constexpr int NE = T::PAIR ? 2 : 1;  // flux points per work item
+  for (int it = tid; it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
-    const int pr = sPair[l];
+    const int pr = T::PAIR ? sPair[l] : l;  // side-0 fpt | side-1 fpt << 16, or the fpt
     const int ln = sLine[pr & 0xffff];
-    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side0 = T::PAIR ? 0 : ln >> 20;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[2][NF];
+    R acc[NE][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[0][k] = acc[1][k] = R(0);
+    for (int j = 0; j < NE; j++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[j][k] = R(0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev0 = sEF[m], ev1 = sEF[N + m];
       R x[NF];
       ldp<NF, R>(&sF[fidx(dn, base + m * stride) + fe * NF], x);
 #pragma unroll
-      for (int k = 0; k < NF; k++) {
-        acc[0][k] += ev0 * x[k];
-        acc[1][k] += ev1 * x[k];
+      for (int j = 0; j < NE; j++) {
+        const R ev = sEF[(j ? 1 : side0) * N + m];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[j][k] += ev * x[k];
       }
     }
 #pragma unroll
-    for (int side = 0; side < 2; side++) {
-      const int f = side ? pr >> 16 : pr & 0xffff;
+    for (int j = 0; j < NE; j++) {
+      const int f = j ? pr >> 16 : pr & 0xffff;
       R *q = &sFn[f * ROW + fe * NF];
       R qv[NF];
       ldp<NF, R>(q, qv);
 #pragma unroll
       for (int k = 0; k < NF; k++) {
-        qv[k] = qv[k] - acc[side][k];
+        qv[k] = qv[k] - acc[j][k];
         if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = qv[k];
       }
       stp<NF, R>(q, qv);
@@ -501,33 +507,35 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     return;
   }
 
-  // E: new state at the flux points, into the Fn tile (both ends of a line
-  // per pass)
-  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+  // E: new state at the flux points, into the Fn tile (per flux point or,
+  // PAIR, per line as in C2)
+  for (int it = tid; it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
-    const int pr = sPair[l];
+    const int pr = T::PAIR ? sPair[l] : l;
     const int ln = sLine[pr & 0xffff];
-    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side0 = T::PAIR ? 0 : ln >> 20;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[2][NF];
+    R acc[NE][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[0][k] = acc[1][k] = R(0);
+    for (int j = 0; j < NE; j++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[j][k] = R(0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev0 = sE[m], ev1 = sE[N + m];
       R x[NF];
       if (PADDED)
         ldp<NF, R>(&sF[fidx(0, base + m * stride) + fe * NF], x);
       else
         ldp<NF, R>(&sU[(base + m * stride) * ROW + fe * NF], x);
 #pragma unroll
-      for (int k = 0; k < NF; k++) {
-        acc[0][k] += ev0 * x[k];
-        acc[1][k] += ev1 * x[k];
+      for (int j = 0; j < NE; j++) {
+        const R ev = sE[(j ? 1 : side0) * N + m];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[j][k] += ev * x[k];
       }
     }
-    stp<NF, R>(&sFn[(pr & 0xffff) * ROW + fe * NF], acc[0]);
-    stp<NF, R>(&sFn[(pr >> 16) * ROW + fe * NF], acc[1]);
+#pragma unroll
+    for (int j = 0; j < NE; j++) stp<NF, R>(&sFn[(j ? pr >> 16 : pr & 0xffff) * ROW + fe * NF], acc[j]);
   }
   fence_async_smem();
   __syncthreads();
@@ -593,6 +601,7 @@ template <int ND, int P, typename R>
 struct Tg2 {
   using T = Tm<ND, P, R, 0>;
   static constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
+  static constexpr bool PAIR = T::PAIR;
   static constexpr int AL = T::AL;
   static constexpr int al(int n) { return (n + AL - 1) / AL * AL; }
   // the flux-point gradient tile reuses the input tiles (U, dUc, JGinv,
@@ -727,34 +736,36 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
     tma_store_3d(&mp.dUs, e0 * NF, 0, 0, sG);
     tma_commit();
   }
-  // both ends of a line per pass over its points
-  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+  // per flux point, or (PAIR) per line: both ends from one pass over it
+  constexpr int NE = T::PAIR ? 2 : 1;
+  for (int it = tid; it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
-    const int pr = sPair[l];
-    const int f0 = pr & 0xffff, f1 = pr >> 16;
-    const int ln = sLine[f0];
-    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
+    const int pr = T::PAIR ? sPair[l] : l;
+    const int ln = sLine[pr & 0xffff];
+    const int base = ln & 0xffff, dn = (ln >> 16) & 0xf, side0 = T::PAIR ? 0 : ln >> 20;
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-      R acc0[NF], acc1[NF];
+      R acc[NE][NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc0[k] = acc1[k] = R(0.0);
+      for (int j = 0; j < NE; j++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[j][k] = R(0.0);
 #pragma unroll
       for (int m = 0; m < N; m++) {
-        const R ev0 = sE[m], ev1 = sE[N + m];
         const R *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
-        for (int k = 0; k < NF; k++) {
-          const R xv = x[k];
-          acc0[k] += ev0 * xv;
-          acc1[k] += ev1 * xv;
+        for (int j = 0; j < NE; j++) {
+          const R ev = sE[(j ? 1 : side0) * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[j][k] += ev * x[k];
         }
       }
 #pragma unroll
-      for (int k = 0; k < NF; k++) {
-        sGf[(d * NFP + f0) * ROW + fe * NF + k] = acc0[k];
-        sGf[(d * NFP + f1) * ROW + fe * NF + k] = acc1[k];
+      for (int j = 0; j < NE; j++) {
+        const int f = j ? pr >> 16 : pr & 0xffff;
+#pragma unroll
+        for (int k = 0; k < NF; k++) sGf[(d * NFP + f) * ROW + fe * NF + k] = acc[j][k];
       }
     }
   }

@@ -31,6 +31,9 @@ struct Tp {
   static constexpr int EB = NS >= 256 ? 1 : (NS * 2 > 256 ? 1 : (NS * 4 > 256 ? 2 : (NS * 8 > 256 ? 4 : (NS * 16 > 256 ? 8 : (NS * 32 > 256 ? 16 : 32)))));
   static constexpr int NT = NS * EB;
   static constexpr int ROW = EB * NF;  // values per point row of a tile
+  // flux-point phases per line (both ends) where one flux point per thread
+  // would need more than one round of the block
+  static constexpr bool PAIR = NFP * EB > NT;
   static constexpr size_t SMEM = sizeof(R) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 4 * N);
 };
 
@@ -44,10 +47,14 @@ __device__ __forceinline__ void two_sum_tp(float a, float b, float &s, float &e)
 // One element block (EB elements from element blk * EB) of the stage; the
 // block's threads are threads 0..NT-1 of the CTA, and further threads of a
 // larger CTA (the many-order kernel below) only take part in its barriers.
-template <int ND, int P, bool VISC, typename R>
+// LINES allows the per-line flux-point phases (the many-order kernel keeps
+// one flux point per thread: its CTA holds every order's code, and the line
+// form's registers for the small orders cost it a CTA per SM).
+template <int ND, int P, bool VISC, typename R, bool LINES = true>
 __device__ __forceinline__ void elem_tp_block(const ElemArgsT<R> &a, const TpTablesT<R> &t, int blk,
                                               unsigned char *smem_bytes) {
   using T = Tp<ND, P, R>;
+  constexpr bool PAIR = LINES && T::PAIR;
   constexpr bool F32 = std::is_same<R, float>::value;
   constexpr int N = T::N, NF = T::NF, NS = T::NS, NFP = T::NFP, EB = T::EB, NT = T::NT, ROW = T::ROW;
   R *smem = reinterpret_cast<R *>(smem_bytes);
@@ -154,36 +161,39 @@ __device__ __forceinline__ void elem_tp_block(const ElemArgsT<R> &a, const TpTab
     for (int k = 0; k < NF; k++) div[k] = d == 0 ? acc[k] : div[k] + acc[k];
   }
 
-  // C2: Fn - extrapolated normal flux at every (fpt, el); one pass over a
-  // line's points gives both of its ends
-  for (int it = tid; act && it < (NFP / 2) * EB; it += NT) {
+  // C2: Fn - extrapolated normal flux at every (fpt, el), per flux point
+  // or (PAIR) per line: one pass over a line's points gives both ends
+  constexpr int NE = PAIR ? 2 : 1;  // flux points per work item
+  for (int it = tid; act && it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
     const int ee = e0 + fe;
-    const int pr = __ldg(&t.linePair[l]);
+    const int pr = PAIR ? __ldg(&t.linePair[l]) : l;
     const int f0 = pr & 0xffff;
     const int base = __ldg(&t.fptBase[f0]), dn = __ldg(&t.fptDn[f0]);
+    const int side0 = PAIR ? 0 : __ldg(&t.fptSide[f0]);
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc[2][NF];
+    R acc[NE][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc[0][k] = acc[1][k] = R(0.0);
+    for (int j = 0; j < NE; j++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[j][k] = R(0.0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev0 = sEF[m], ev1 = sEF[N + m];
       const R *x = &sF[(dn * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) {
-        const R xv = x[k];
-        acc[0][k] += ev0 * xv;
-        acc[1][k] += ev1 * xv;
+      for (int j = 0; j < NE; j++) {
+        const R ev = sEF[(j ? 1 : side0) * N + m];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[j][k] += ev * x[k];
       }
     }
     const bool v = fe < nValid;
 #pragma unroll
-    for (int side = 0; side < 2; side++) {
-      const int f = side ? pr >> 16 : f0;
+    for (int j = 0; j < NE; j++) {
+      const int f = j ? pr >> 16 : f0;
 #pragma unroll
       for (int k = 0; k < NF; k++) {
-        const R q = v ? a.Fn[((long long)f * E + ee) * NF + k] - acc[side][k] : R(0.0);
+        const R q = v ? a.Fn[((long long)f * E + ee) * NF + k] - acc[j][k] : R(0.0);
         sQ[f * ROW + fe * NF + k] = q;
         if (a.disFn_dbg && v) a.disFn_dbg[((long long)f * E + ee) * NF + k] = q;
       }
@@ -260,33 +270,36 @@ __device__ __forceinline__ void elem_tp_block(const ElemArgsT<R> &a, const TpTab
   if (a.mode == MODE_RESIDUAL || !a.Ufpts_out) return;
   __syncthreads();
 
-  // E: new state at the flux points (both ends of a line per pass)
-  for (int it = tid; act && it < (NFP / 2) * EB; it += NT) {
+  // E: new state at the flux points (per flux point or, PAIR, per line)
+  for (int it = tid; act && it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
     if (fe >= nValid) continue;
     const int ee = e0 + fe;
-    const int pr = __ldg(&t.linePair[l]);
-    const int f0 = pr & 0xffff, f1 = pr >> 16;
+    const int pr = PAIR ? __ldg(&t.linePair[l]) : l;
+    const int f0 = pr & 0xffff;
     const int base = __ldg(&t.fptBase[f0]), dn = __ldg(&t.fptDn[f0]);
+    const int side0 = PAIR ? 0 : __ldg(&t.fptSide[f0]);
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
-    R acc0[NF], acc1[NF];
+    R acc[NE][NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) acc0[k] = acc1[k] = R(0.0);
+    for (int j = 0; j < NE; j++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) acc[j][k] = R(0.0);
 #pragma unroll
     for (int m = 0; m < N; m++) {
-      const R ev0 = sE[m], ev1 = sE[N + m];
       const R *x = &sU[(base + m * stride) * ROW + fe * NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) {
-        const R xv = x[k];
-        acc0[k] += ev0 * xv;
-        acc1[k] += ev1 * xv;
+      for (int j = 0; j < NE; j++) {
+        const R ev = sE[(j ? 1 : side0) * N + m];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[j][k] += ev * x[k];
       }
     }
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      a.Ufpts_out[((long long)f0 * E + ee) * NF + k] = acc0[k];
-      a.Ufpts_out[((long long)f1 * E + ee) * NF + k] = acc1[k];
+    for (int j = 0; j < NE; j++) {
+      const int f = j ? pr >> 16 : f0;
+#pragma unroll
+      for (int k = 0; k < NF; k++) a.Ufpts_out[((long long)f * E + ee) * NF + k] = acc[j][k];
     }
   }
 }
@@ -324,12 +337,12 @@ __global__ void __launch_bounds__(kMultiNT) k_elem_multi(const __grid_constant__
     while (g + 1 < m.nGroups && w >= m.start[g + 1]) g++;
     const int blk = w - m.start[g];
     switch (m.order[g]) {
-      case 0: elem_tp_block<ND, 0, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
-      case 1: elem_tp_block<ND, 1, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
-      case 2: elem_tp_block<ND, 2, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
-      case 3: elem_tp_block<ND, 3, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
-      case 4: elem_tp_block<ND, 4, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
-      default: elem_tp_block<ND, 5, false, R>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 0: elem_tp_block<ND, 0, false, R, false>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 1: elem_tp_block<ND, 1, false, R, false>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 2: elem_tp_block<ND, 2, false, R, false>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 3: elem_tp_block<ND, 3, false, R, false>(m.a[g], m.t[g], blk, smem_bytes); break;
+      case 4: elem_tp_block<ND, 4, false, R, false>(m.a[g], m.t[g], blk, smem_bytes); break;
+      default: elem_tp_block<ND, 5, false, R, false>(m.a[g], m.t[g], blk, smem_bytes); break;
     }
     __syncthreads();  // the next block reuses the shared memory
   }

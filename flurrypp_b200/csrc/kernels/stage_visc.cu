@@ -233,6 +233,7 @@ struct Tg {
   static constexpr int EB = NS >= 128 ? 1 : (NS * 2 > 128 ? 1 : (NS * 4 > 128 ? 2 : (NS * 8 > 128 ? 4 : (NS * 16 > 128 ? 8 : (NS * 32 > 128 ? 16 : 32)))));
   static constexpr int NT = NS * EB;
   static constexpr int ROW = EB * NF;
+  static constexpr bool PAIR = NFP * EB > NT;  // extrapolation per line (both ends)
   static constexpr size_t SMEM = sizeof(R) * ((size_t)ROW * (NS * (1 + ND) + NFP) + N * N + 2 * N);
 };
 
@@ -322,34 +323,38 @@ __global__ void __launch_bounds__(Tg<ND, P, R>::NT) k_elem_grad(GradArgsT<R> g, 
       if (valid) g.dUs[(long long)d2 * g.sStride + ((long long)s * E + e) * NF + k] = v;
     }
   __syncthreads();
-  // both ends of a line per pass over its points
-  for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+  // per flux point, or (PAIR) per line: both ends from one pass over it
+  constexpr int NE = T::PAIR ? 2 : 1;
+  for (int it = tid; it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
     if (fe >= nValid) continue;
-    const int pr = __ldg(&t.linePair[l]);
-    const int f0 = pr & 0xffff, f1 = pr >> 16;
+    const int pr = T::PAIR ? __ldg(&t.linePair[l]) : l;
+    const int f0 = pr & 0xffff;
     const int base = __ldg(&t.fptBase[f0]), dn = __ldg(&t.fptDn[f0]);
+    const int side0 = T::PAIR ? 0 : __ldg(&t.fptSide[f0]);
     const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-      R acc0[NF], acc1[NF];
+      R acc[NE][NF];
 #pragma unroll
-      for (int k = 0; k < NF; k++) acc0[k] = acc1[k] = R(0.0);
+      for (int j = 0; j < NE; j++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[j][k] = R(0.0);
 #pragma unroll
       for (int m = 0; m < N; m++) {
-        const R ev0 = sE[m], ev1 = sE[N + m];
         const R *x = &sG[(d * NS + base + m * stride) * ROW + fe * NF];
 #pragma unroll
-        for (int k = 0; k < NF; k++) {
-          const R xv = x[k];
-          acc0[k] += ev0 * xv;
-          acc1[k] += ev1 * xv;
+        for (int j = 0; j < NE; j++) {
+          const R ev = sE[(j ? 1 : side0) * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[j][k] += ev * x[k];
         }
       }
 #pragma unroll
-      for (int k = 0; k < NF; k++) {
-        g.dUf[(long long)d * g.fStride + ((long long)f0 * E + e0 + fe) * NF + k] = acc0[k];
-        g.dUf[(long long)d * g.fStride + ((long long)f1 * E + e0 + fe) * NF + k] = acc1[k];
+      for (int j = 0; j < NE; j++) {
+        const int f = j ? pr >> 16 : f0;
+#pragma unroll
+        for (int k = 0; k < NF; k++) g.dUf[(long long)d * g.fStride + ((long long)f * E + e0 + fe) * NF + k] = acc[j][k];
       }
     }
   }
