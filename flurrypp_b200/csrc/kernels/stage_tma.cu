@@ -89,6 +89,15 @@ struct Tm {
   // the flux-point phases take one line (both of its ends) per thread where
   // one flux point per thread would need more than one round of the CTA
   static constexpr bool PAIR = NFP * EB > NT;
+  // 3-D: the divergence and the extrapolated normal flux in one pass per
+  // (line, element) over the line's flux values (LP), instead of a pass per
+  // solution point for the divergence and one per line for the flux points
+  // (3-D P3 32^3: FP32 element stage 0.1142 -> 0.1130 ms, FP64 0.1830 ->
+  // 0.1818 ms with the register cap below; NS TGV 40^3 P4 1.047 -> 1.032 ms
+  // FP64, 0.525 -> 0.509 ms FP32); FP64 inviscid at P2 and P3, where the
+  // register cap below keeps the CTAs per SM with a few bytes spilled (at P0
+  // and P1 the line pass would raise the registers from 72-80 to 96-126)
+  static constexpr bool LP = ND == 3 && (F32 || VS || (P >= 2 && P <= 3));
   static constexpr int SLAB = NS * ROW + padF();  // one dimension's flux tile
   static constexpr int O_U = 0;
   static constexpr int O_U0 = O_U + al(NS * ROW);
@@ -110,6 +119,11 @@ struct Tm {
   static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
   static_assert(SMEM <= kMaxSmem, "TMA tile set does not fit in shared memory");
   static_assert(NT <= 1024, "too many threads");
+  // minimum CTAs per SM for the register allocation (0: none): the FP64
+  // inviscid line pass holds a line's N records in registers, which uncapped
+  // (100 registers at P3) costs a CTA per SM (0.205 ms instead of 0.182)
+  static constexpr int CTAS = (int)((228 * 1024) / (SMEM + 1024));
+  static constexpr int MINB = (LP && !F32 && !VS && 65536 / (NT * CTAS) >= 80) ? CTAS : 0;
   static_assert(!F32 || EB % 4 == 0, "FP32 tiles need 16-byte x offsets");
 };
 
@@ -152,7 +166,7 @@ __device__ __forceinline__ void stp(R *p, const R (&v)[NF]) {
 }
 
 template <int ND, int P, typename R, int V, bool VISC>
-__global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgsT<R> a, TpTablesT<R> t,
+__global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VISC>::MINB) k_elem_tma(ElemArgsT<R> a, TpTablesT<R> t,
                                                                   const __grid_constant__ TmaMaps mp) {
   pdl_wait();
   pdl_trigger();
@@ -329,14 +343,14 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
   }
   __syncthreads();
 
-  // C1: flux divergence at (s, el)
+  // C1: flux divergence at (s, el) (LP: formed per line below)
   int idx3[3];
   idx3[0] = s % N;
   idx3[1] = ND > 1 ? (s / N) % N : 0;
   idx3[2] = ND > 2 ? s / (N * N) : 0;
   R div[NF];
 #pragma unroll
-  for (int d = 0; d < ND; d++) {
+  for (int d = 0; d < (T::LP ? 0 : ND); d++) {
     const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
     const int base = s - idx3[d] * stride;
     const R *Dr = &sD[idx3[d] * N];
@@ -370,10 +384,61 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
     return;
   }
 
+  constexpr int NE = T::PAIR ? 2 : 1;  // flux points per work item
+  if constexpr (T::LP) {
+    // C (LP): per (line, element), the line's N flux values of its
+    // direction once into registers; the divergence along the line at its N
+    // points replaces them in the flux tile (only this item reads them), and
+    // Fn - extrapolated normal flux is formed at both of its ends
+    for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+      const int l = it / EB, fe = it - (it / EB) * EB;
+      const int pr = sPair[l];
+      const int ln = sLine[pr & 0xffff];
+      const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
+      const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+      R x[N][NF];
+#pragma unroll
+      for (int m = 0; m < N; m++) ldp<NF, R>(&sF[fidx(dn, base + m * stride) + fe * NF], x[m]);
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        R acc[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+          const R dv = sD[i * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[k] += dv * x[m][k];
+        }
+        stp<NF, R>(&sF[fidx(dn, base + i * stride) + fe * NF], acc);
+      }
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        R acc[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+          const R ev = sEF[j * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[k] += ev * x[m][k];
+        }
+        const int f = j ? pr >> 16 : pr & 0xffff;
+        R *q = &sFn[f * ROW + fe * NF];
+        R qv[NF];
+        ldp<NF, R>(q, qv);
+#pragma unroll
+        for (int k = 0; k < NF; k++) {
+          qv[k] = qv[k] - acc[k];
+          if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = qv[k];
+        }
+        stp<NF, R>(q, qv);
+      }
+    }
+  }
   // C2: Fn - extrapolated normal flux, in place in the Fn tile, per flux
   // point or (PAIR) per line: one pass over a line's points gives both ends
-  constexpr int NE = T::PAIR ? 2 : 1;  // flux points per work item
-  for (int it = tid; it < (NFP / NE) * EB; it += NT) {
+  for (int it = tid; !T::LP && it < (NFP / NE) * EB; it += NT) {
     const int l = it / EB, fe = it - (it / EB) * EB;
     const int pr = T::PAIR ? sPair[l] : l;  // side-0 fpt | side-1 fpt << 16, or the fpt
     const int ln = sLine[pr & 0xffff];
@@ -411,6 +476,16 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT) k_elem_tma(ElemArgs
   }
   if (tid == 0) tma_wait_read_all();  // the U0 store has read sU
   __syncthreads();
+  if constexpr (T::LP) {
+    // the divergence at (s, el): the three directions' parts, x, y, z
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      R x[NF];
+      ldp<NF, R>(&sF[fidx(d, s) + el * NF], x);
+#pragma unroll
+      for (int k = 0; k < NF; k++) div[k] = d == 0 ? x[k] : div[k] + x[k];
+    }
+  }
 
   // D: correction and RK update at (s, el), in place in sU / sAcc / sCmp
   {
