@@ -57,7 +57,7 @@ DECK_GPU = os.path.join(ROOT, "flurrypp_b200", "decks", "tgv3d_p3_32.deck")
 DECK_CPU = os.path.join(ROOT, "flurrypp_b200", "decks", "tgv3d_p3_16.deck")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "fr_ref_harness_omp")
 METRIC = "DOF·RK-stage/s"
-E2E_CASES = 3  # cases in flight in the end-to-end measurement
+E2E_CASES = 4  # cases in flight in the end-to-end measurement (default of --e2e-cases)
 WORKLOAD = "3D Euler Taylor-Green vortex, 32^3 hexes, P=3, RK4, Rusanov, FP64 plain form"
 
 
@@ -774,7 +774,9 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=12)
+    ap.add_argument("--e2e-steps", type=int, default=24)
+    ap.add_argument("--e2e-cases", type=int, default=E2E_CASES,
+                    help="independent cases in flight in the end-to-end measurement")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="vortex32_1000,precision_tgv32,precision_ns_tgv40,batch256,serve",
@@ -866,12 +868,12 @@ def main():
     # end to end through the C ABI with host buffers (pinned): every step
     # copies its case's state in from pinned host memory, advances it one RK
     # step and copies the result back out, and the next step of that case
-    # starts from the copy that came back.  E2E_CASES independent cases, each
+    # starts from the copy that came back.  --e2e-cases independent cases, each
     # on its own stream, are in flight together, so one case's copy in, another
     # case's step and a third case's copy out overlap (the two PCIe directions
     # and the SMs are separate engines).
     flight = [(s, stream)]
-    for _ in range(E2E_CASES - 1):
+    for _ in range(args.e2e_cases - 1):
         sx, stx = fb.Solver(DECK_GPU, device=local, tile_variant=args.tile_variant), torch.cuda.Stream()
         sx.set_stream(stx.cuda_stream)
         sx.initialize_solution(fb.IC_TGV, (0.1,))
@@ -963,7 +965,7 @@ def main():
             "data": "synthetic (Taylor-Green initial condition, seeded-free analytic field)",
             "config": headline_config(world), "dt": dt,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8,
-                    "cases_in_flight": E2E_CASES, "steps": args.e2e_steps,
+                    "cases_in_flight": args.e2e_cases, "steps": args.e2e_steps,
                     "copy_bound": e2e_copy_bound, "frac_of_copy_bound": e2e / e2e_copy_bound},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
