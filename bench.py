@@ -659,6 +659,8 @@ PROFILE_CASES = {
     "fp64_tgv32_p3": ("tgv", 3, 32, 0, -1),
     "fp32_tgv32_p3": ("tgv", 3, 32, 1, -1),
     "fp32_vortex256_p3": ("vortex", 3, 256, 1, -1),
+    "fp64_vortex512_p3": ("vortex", 3, 512, 0, -1),
+    "fp64_vortex512_p2": ("vortex", 2, 512, 0, -1),
     "tc_vortex256_p3": ("vortex", 3, 256, 1, 3),
     "fp32_tgv64_p1": ("tgv", 1, 64, 1, -1),
     "tc_tgv64_p1": ("tgv", 1, 64, 1, 3),

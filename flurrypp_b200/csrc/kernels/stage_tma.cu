@@ -137,19 +137,47 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
 
 // One point's NF values of a tile row.  With 4 fields (2-D) the record is
 // 16-byte aligned and moves as one 128-bit shared-memory access (two for
-// FP64): four times fewer instructions than per-field accesses and no bank
-// conflicts; otherwise per field.
+// FP64): four times fewer instructions than per-field accesses; otherwise
+// per field.  A 128-bit access serves a quarter warp (8 lanes, normally 8
+// consecutive records) per wavefront.  FP64 records are 32 bytes, so the
+// first halves of 8 consecutive records fall on 16 of the 32 banks, twice
+// each; every lane therefore takes its two halves in the order given by
+// bit 7 of the record's address (bit 2 of its index), which pairs each
+// first half with a second half of the record 128 bytes away and covers
+// all 32 banks once (2-D FP64 element stage: 46 % of its shared-memory
+// wavefronts were such conflicts).
+template <int NF, typename R>
+__device__ __forceinline__ int half_order(const R *p) {
+  return (int)((reinterpret_cast<uintptr_t>(p) >> 7) & 1);
+}
 template <int NF, typename R>
 __device__ __forceinline__ void ldp(const R *p, R (&v)[NF]) {
   if constexpr (NF == 4 && std::is_same<R, float>::value) {
     const float4 t = *reinterpret_cast<const float4 *>(p);
     v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
   } else if constexpr (NF == 4 && std::is_same<R, double>::value) {
-    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
-    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+    const int h = half_order<NF, R>(p);
+    const double2 a = reinterpret_cast<const double2 *>(p)[h], b = reinterpret_cast<const double2 *>(p)[h ^ 1];
+    v[0] = h ? b.x : a.x, v[1] = h ? b.y : a.y, v[2] = h ? a.x : b.x, v[3] = h ? a.y : b.y;
   } else {
 #pragma unroll
     for (int k = 0; k < NF; k++) v[k] = p[k];
+  }
+}
+// One row of a point's metric (ND values of JGinv); in 2-D the pair moves as
+// one 8- or 16-byte access, which keeps consecutive lanes on consecutive
+// banks (two scalar accesses at a 2-value stride conflict two ways).
+template <int ND, typename R>
+__device__ __forceinline__ void ldj(const R *p, R (&v)[ND]) {
+  if constexpr (ND == 2 && std::is_same<R, double>::value) {
+    const double2 t = *reinterpret_cast<const double2 *>(p);
+    v[0] = t.x, v[1] = t.y;
+  } else if constexpr (ND == 2 && std::is_same<R, float>::value) {
+    const float2 t = *reinterpret_cast<const float2 *>(p);
+    v[0] = t.x, v[1] = t.y;
+  } else {
+#pragma unroll
+    for (int d = 0; d < ND; d++) v[d] = p[d];
   }
 }
 template <int NF, typename R>
@@ -157,8 +185,9 @@ __device__ __forceinline__ void stp(R *p, const R (&v)[NF]) {
   if constexpr (NF == 4 && std::is_same<R, float>::value) {
     *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
   } else if constexpr (NF == 4 && std::is_same<R, double>::value) {
-    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
-    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+    const int h = half_order<NF, R>(p);
+    reinterpret_cast<double2 *>(p)[h] = h ? make_double2(v[2], v[3]) : make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[h ^ 1] = h ? make_double2(v[0], v[1]) : make_double2(v[2], v[3]);
   } else {
 #pragma unroll
     for (int k = 0; k < NF; k++) p[k] = v[k];
@@ -311,7 +340,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VIS
       R Fr[ND][NF];
 #pragma unroll
       for (int d1 = 0; d1 < ND; d1++) {
-        const R *Jr = &sJ[(d1 * NS + s) * EB * ND + el * ND];
+        R Jr[ND];
+        ldj<ND, R>(&sJ[(d1 * NS + s) * EB * ND + el * ND], Jr);
 #pragma unroll
         for (int k = 0; k < NF; k++) {
           R f = R(0);
@@ -327,7 +357,8 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VIS
     } else {
 #pragma unroll
       for (int d1 = 0; d1 < ND; d1++) {
-        const R *Jr = &sJ[(d1 * NS + s) * EB * ND + el * ND];
+        R Jr[ND];
+        ldj<ND, R>(&sJ[(d1 * NS + s) * EB * ND + el * ND], Jr);
         R fk[NF];
 #pragma unroll
         for (int k = 0; k < NF; k++) {
