@@ -661,6 +661,10 @@ PROFILE_CASES = {
     "fp32_vortex256_p3": ("vortex", 3, 256, 1, -1),
     "fp64_vortex512_p3": ("vortex", 3, 512, 0, -1),
     "fp64_vortex512_p2": ("vortex", 2, 512, 0, -1),
+    "fp64_vortex384_p4": ("vortex", 4, 384, 0, -1),
+    "fp32_vortex384_p4": ("vortex", 4, 384, 1, -1),
+    "fp64_vortex320_p5": ("vortex", 5, 320, 0, -1),
+    "fp32_vortex320_p5": ("vortex", 5, 320, 1, -1),
     "tc_vortex256_p3": ("vortex", 3, 256, 1, 3),
     "fp32_tgv64_p1": ("tgv", 1, 64, 1, -1),
     "tc_tgv64_p1": ("tgv", 1, 64, 1, 3),
