@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <type_traits>
 
 #include "launch.cuh"
 #include "stage.hpp"
@@ -46,6 +47,50 @@ __global__ void k_apply_op(int nRows, const int *__restrict__ rp, const int *__r
   out[(long long)r * N + n] = o;
 }
 
+// A point's NF values in a global [slot][field] array, and a face point's
+// ND normal components: in 2-D (four fields, two components, 16- or
+// 32-byte and 8- or 16-byte aligned) as vector accesses, which issue a
+// quarter of the memory instructions of per-value accesses; otherwise per
+// value.
+template <int NF, typename R>
+__device__ __forceinline__ void ld_rec(const R *__restrict__ p, R (&v)[NF]) {
+  if constexpr (NF == 4 && std::is_same<R, float>::value) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else if constexpr (NF == 4 && std::is_same<R, double>::value) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; k++) v[k] = p[k];
+  }
+}
+template <int NF, typename R>
+__device__ __forceinline__ void st_rec(R *__restrict__ p, const R (&v)[NF]) {
+  if constexpr (NF == 4 && std::is_same<R, float>::value) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (NF == 4 && std::is_same<R, double>::value) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; k++) p[k] = v[k];
+  }
+}
+template <int ND, typename R>
+__device__ __forceinline__ void ld_nrm(const R *__restrict__ p, R (&v)[ND]) {
+  if constexpr (ND == 2 && std::is_same<R, float>::value) {
+    const float2 t = *reinterpret_cast<const float2 *>(p);
+    v[0] = t.x, v[1] = t.y;
+  } else if constexpr (ND == 2 && std::is_same<R, double>::value) {
+    const double2 t = *reinterpret_cast<const double2 *>(p);
+    v[0] = t.x, v[1] = t.y;
+  } else {
+#pragma unroll
+    for (int d = 0; d < ND; d++) v[d] = p[d];
+  }
+}
+
 // Interior face point i: Rusanov (or 2-D Roe) on the left normal, written to
 // both sides (reference: face.cpp:163-208, intFace.cpp:147-154).
 template <int ND, typename R>
@@ -57,12 +102,9 @@ __device__ __forceinline__ void face_interior(int i, const int *__restrict__ slo
   const int sL = slotL[i];
   const int sR = slotR[i];
   R UL[NF], UR[NF], nv[ND], F[NF];
-#pragma unroll
-  for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
-#pragma unroll
-  for (int k = 0; k < NF; k++) UR[k] = Uf[(long long)sR * NF + k];
-#pragma unroll
-  for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
+  ld_rec<NF, R>(&Uf[(long long)sL * NF], UL);
+  ld_rec<NF, R>(&Uf[(long long)sR * NF], UR);
+  ld_nrm<ND, R>(&nrm[(long long)i * ND], nv);
   if (ND == 2 && roe) {
     roe2d<R>(UL, UR, nv, gam, F);
   } else {
@@ -70,11 +112,14 @@ __device__ __forceinline__ void face_interior(int i, const int *__restrict__ slo
     if (waveSp) waveSp[sL] = ws;  // null when no CFL time step reads it
   }
   const R aL = dAL[i], aR = dAR[i];
+  R FL[NF], FR[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    Fn[(long long)sL * NF + k] = F[k] * aL;
-    Fn[(long long)sR * NF + k] = -F[k] * aR;
+    FL[k] = F[k] * aL;
+    FR[k] = -F[k] * aR;
   }
+  st_rec<NF, R>(&Fn[(long long)sL * NF], FL);
+  st_rec<NF, R>(&Fn[(long long)sR * NF], FR);
 }
 
 // Boundary face point i: ghost state from the BC, then Rusanov (boundaries
@@ -88,16 +133,15 @@ __device__ __forceinline__ void face_boundary(int i, const int *__restrict__ slo
   const int sL = slotL[i];
   const int bc = -slotR[i] - 2;
   R UL[NF], UR[NF], nv[ND], F[NF];
-#pragma unroll
-  for (int k = 0; k < NF; k++) UL[k] = Uf[(long long)sL * NF + k];
-#pragma unroll
-  for (int d = 0; d < ND; d++) nv[d] = nrm[(long long)i * ND + d];
+  ld_rec<NF, R>(&Uf[(long long)sL * NF], UL);
+  ld_nrm<ND, R>(&nrm[(long long)i * ND], nv);
   boundary_state<ND, R>(bc, UL, nv, ph, UR);
   const R ws = rusanov<ND, R>(UL, UR, nv, R(ph.gamma), F);
   if (waveSp) waveSp[sL] = ws;
   const R aL = dAL[i];
 #pragma unroll
-  for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
+  for (int k = 0; k < NF; k++) F[k] = F[k] * aL;
+  st_rec<NF, R>(&Fn[(long long)sL * NF], F);
 }
 
 // Interior points only (no boundary-condition code, fewer registers).
@@ -150,13 +194,9 @@ __global__ void __launch_bounds__(kFaceNt, face_min_ctas<ND, R>()) k_faces_inter
   R UL[PPT][NF], UR[PPT][NF], nv[PPT][ND], aL[PPT], aR[PPT];
 #pragma unroll
   for (int q = 0; q < PPT; q++) {
-#pragma unroll
-#pragma unroll
-    for (int k = 0; k < NF; k++) UL[q][k] = Uf[(long long)sL[q] * NF + k];
-#pragma unroll
-    for (int k = 0; k < NF; k++) UR[q][k] = Uf[(long long)sR[q] * NF + k];
-#pragma unroll
-    for (int d = 0; d < ND; d++) nv[q][d] = nrm[(long long)ii[q] * ND + d];
+    ld_rec<NF, R>(&Uf[(long long)sL[q] * NF], UL[q]);
+    ld_rec<NF, R>(&Uf[(long long)sR[q] * NF], UR[q]);
+    ld_nrm<ND, R>(&nrm[(long long)ii[q] * ND], nv[q]);
     aL[q] = dAL[ii[q]];
     aR[q] = dAR[ii[q]];
   }
@@ -170,11 +210,14 @@ __global__ void __launch_bounds__(kFaceNt, face_min_ctas<ND, R>()) k_faces_inter
       const R ws = rusanov<ND, R>(UL[q], UR[q], nv[q], gam, F);
       if (waveSp) waveSp[sL[q]] = ws;
     }
+    R FL[NF], FR[NF];
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      Fn[(long long)sL[q] * NF + k] = F[k] * aL[q];
-      Fn[(long long)sR[q] * NF + k] = -F[k] * aR[q];
+      FL[k] = F[k] * aL[q];
+      FR[k] = -F[k] * aR[q];
     }
+    st_rec<NF, R>(&Fn[(long long)sL[q] * NF], FL);
+    st_rec<NF, R>(&Fn[(long long)sR[q] * NF], FR);
   }
 }
 
