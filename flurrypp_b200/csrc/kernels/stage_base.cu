@@ -144,20 +144,6 @@ __device__ __forceinline__ void face_boundary(int i, const int *__restrict__ slo
   st_rec<NF, R>(&Fn[(long long)sL * NF], F);
 }
 
-// Interior points only (no boundary-condition code, fewer registers).
-template <int ND, typename R>
-__global__ void __launch_bounds__(256) k_faces_interior(int n, const int *__restrict__ slotL,
-                                                        const int *__restrict__ slotR, const R *__restrict__ nrm,
-                                                        const R *__restrict__ dAL, const R *__restrict__ dAR,
-                                                        const R *__restrict__ Uf, R *__restrict__ Fn,
-                                                        double *__restrict__ waveSp, R gam, int roe) {
-  pdl_wait();
-  pdl_trigger();
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  face_interior<ND, R>(i, slotL, slotR, nrm, dAL, dAR, Uf, Fn, waveSp, gam, roe);
-}
-
 // PPT face points per thread (points i and i + grid size), all gathers
 // issued before any flux is formed: the gather is latency-bound, and two
 // points per thread at 128 threads per CTA keep a third more loads in flight
@@ -716,8 +702,10 @@ void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R
                waveSp, ph);
     return;
   }
-  if (nI > 0 && (nDims == 3 || sizeof(R) == 8)) {
-    // two points per thread except 2-D FP32, where one measured faster
+  if (nI > 0) {
+    // two points per thread (2-D FP32 with the vector record accesses:
+    // vortex 512^2 P3 face pass 0.0412 -> 0.0350 ms against one point per
+    // thread; with per-value accesses one point per thread had been faster)
     const int per = kFaceNt * kFacePpt;
     const int g = (nI + per - 1) / per;
     if (nDims == 2)
@@ -726,14 +714,6 @@ void launch_faces_inviscid(int nDims, const FaceTableT<R> &ft, const R *Ufpts, R
     else
       launch_k(k_faces_interior_ilp<3, R, kFacePpt>, g, kFaceNt, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL,
                ft.dAR, Ufpts, Fn, waveSp, R(ph.gamma), 0);
-  } else if (nI > 0) {
-    const int g = (nI + b - 1) / b;
-    if (nDims == 2)
-      launch_k(k_faces_interior<2, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
-                                              R(ph.gamma), ph.riemannType == 1);
-    else
-      launch_k(k_faces_interior<3, R>, g, b, 0, st, nI, ft.slotL, ft.slotR, ft.nrm, ft.dAL, ft.dAR, Ufpts, Fn, waveSp,
-                                              R(ph.gamma), 0);
   }
   if (nB > 0) {
     const int g = (nB + b - 1) / b;
