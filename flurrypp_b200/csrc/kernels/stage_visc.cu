@@ -147,11 +147,12 @@ __global__ void __launch_bounds__(128, 4) k_faces_visc_interior(int n, const int
   }
   ldg_interior_flux<ND, R>(UL, UR, gL, gR, nv, ph, F);
   const R aL = dAL[i], aR = dAR[i];
+  // the left record, then the right one (stores interleaved field by field
+  // between the two records measured 20-30 % slower in the inviscid kernel)
 #pragma unroll
-  for (int k = 0; k < NF; k++) {
-    Fn[(long long)sL * NF + k] = F[k] * aL;
-    Fn[(long long)sR * NF + k] = -F[k] * aR;
-  }
+  for (int k = 0; k < NF; k++) Fn[(long long)sL * NF + k] = F[k] * aL;
+#pragma unroll
+  for (int k = 0; k < NF; k++) Fn[(long long)sR * NF + k] = -F[k] * aR;
 }
 
 template <int ND, typename R>
