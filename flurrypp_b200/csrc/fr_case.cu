@@ -964,12 +964,33 @@ struct fr_case {
       for (int fc = 1; fc < nFaces; fc++)
         if (cF[(size_t)sp * nFaces + fc] <= cF[(size_t)sp * nFaces + fc - 1]) return false;
     }
-    double *dD, *dE1, *dEF, *dcV;
+    // the correction values as a function of the side of the face and the
+    // point's index along its normal (tensor product), checked bit for bit:
+    // the 3-D element kernels apply the correction line by line
+    std::vector<double> LC(2 * n, 0.0);
+    std::vector<char> seen(2 * n, 0);
+    for (int sp = 0; sp < nS; sp++) {
+      int a[3];
+      ijk(sp, a);
+      for (int fc = 0; fc < nFaces; fc++) {
+        const int f = cF[(size_t)sp * nFaces + fc];
+        const int k = fSide[f] * n + a[fDn[f]];
+        const double v = cV[(size_t)sp * nFaces + fc];
+        if (!seen[k]) {
+          LC[k] = v;
+          seen[k] = 1;
+        } else if (LC[k] != v) {
+          return false;
+        }
+      }
+    }
+    double *dD, *dE1, *dEF, *dcV, *dLC;
     int *dfB, *dfD, *dfS, *dcF, *dLP;
     if (!upload(dD, D) || !upload(dE1, E1) || !upload(dEF, EF) || !upload(dfB, fBase) || !upload(dfD, fDn) ||
-        !upload(dfS, fSide) || !upload(dcF, cF) || !upload(dcV, cV) || !upload(dLP, pair))
+        !upload(dfS, fSide) || !upload(dcF, cF) || !upload(dcV, cV) || !upload(dLP, pair) || !upload(dLC, LC))
       return false;
     tp.linePair = f32.tp.linePair = dLP;
+    tp.lineCorr = dLC;
     tp.D = dD;
     tp.E1 = dE1;
     tp.EFn1 = dEF;
@@ -979,13 +1000,15 @@ struct fr_case {
     tp.corrFpt = f32.tp.corrFpt = dcF;
     tp.corrVal = dcV;
     if (mixed) {
-      float *fD, *fE1, *fEF, *fcV;
-      if (!upload(fD, narrow(D)) || !upload(fE1, narrow(E1)) || !upload(fEF, narrow(EF)) || !upload(fcV, narrow(cV)))
+      float *fD, *fE1, *fEF, *fcV, *fLC;
+      if (!upload(fD, narrow(D)) || !upload(fE1, narrow(E1)) || !upload(fEF, narrow(EF)) || !upload(fcV, narrow(cV)) ||
+          !upload(fLC, narrow(LC)))
         return false;
       f32.tp.D = fD;
       f32.tp.E1 = fE1;
       f32.tp.EFn1 = fEF;
       f32.tp.corrVal = fcV;
+      f32.tp.lineCorr = fLC;
     }
     return true;
   }

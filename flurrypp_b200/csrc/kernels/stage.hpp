@@ -152,6 +152,7 @@ struct TpTablesT {
   const int *linePair = nullptr;    // [nFp/2] the two ends of a line: side-0 fpt | side-1 fpt << 16
   const int *corrFpt = nullptr;     // [nS][2*nDims]
   const R *corrVal = nullptr;       // [nS][2*nDims]
+  const R *lineCorr = nullptr;      // [2][n] corrVal by side and index along the face normal
 };
 using TpTables = TpTablesT<double>;
 bool tp_supported(int nDims, int order);

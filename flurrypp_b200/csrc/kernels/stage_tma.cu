@@ -63,7 +63,7 @@ struct Tm {
   static constexpr size_t smem_for(int eb) {
     // U, U0, acc, comp tiles; Fn; J; det; F; tables; indices; barriers
     return sizeof(R) * (size_t)(4 * al(NS * eb * NF) + al(NFP * eb * NF) + al(ND * NS * eb * ND) + al(NS * eb) +
-                                al(ND * (NS * eb * NF + padF())) + al(N * N + 4 * N) + al(NS * 2 * ND) +
+                                al(ND * (NS * eb * NF + padF())) + al(N * N + 6 * N) + al(NS * 2 * ND) +
                                 al((int)((NFP + NS * 2 * ND) * 4 / sizeof(R)) + 1) + AL) +
            128;
   }
@@ -98,6 +98,13 @@ struct Tm {
   // register cap below keeps the CTAs per SM with a few bytes spilled (at P0
   // and P1 the line pass would raise the registers from 72-80 to 96-126)
   static constexpr bool LP = ND == 3 && (F32 || VS || (P >= 2 && P <= 3));
+  // the line pass also applies the correction from the line's two ends (the
+  // solution points then need no pass over the flux-point records): FP32
+  // (3-D P3 32^3 element stage 0.1113 -> 0.1026 ms; NS TGV 40^3 P4 0.500 ->
+  // 0.476 ms); in FP64 the registers it needs cost more than it saves
+  // (inviscid P3: 144 bytes spilled under the cap; viscous P4: 1.032 ->
+  // 1.051 ms)
+  static constexpr bool LPC = LP && F32;
   static constexpr int SLAB = NS * ROW + padF();  // one dimension's flux tile
   static constexpr int O_U = 0;
   static constexpr int O_U0 = O_U + al(NS * ROW);
@@ -113,7 +120,7 @@ struct Tm {
   // (4.6 KB per FP64 CTA at 3-D P3, one more CTA per SM)
   static constexpr bool GTAB = !VS;
   static constexpr int NCT = GTAB ? 0 : NS * 2 * ND;
-  static constexpr int O_CV = O_TAB + al(N * N + 4 * N);
+  static constexpr int O_CV = O_TAB + al(N * N + 6 * N);
   static constexpr int O_IDX = O_CV + al(NCT);  // ints: fpt line [NFP], corrFpt [NCT], line ends [NFP/2]
   static constexpr int O_BAR = O_IDX + al((int)((NFP + NCT + NFP / 2) * 4 / sizeof(R)) + 1);
   static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
@@ -229,6 +236,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VIS
   R *sD = smem + T::O_TAB;
   R *sE = sD + N * N;
   R *sEF = sE + 2 * N;
+  R *sCg = sEF + 2 * N;  // correction values by side and index along the line (LP)
   R *sCV = smem + T::O_CV;
   int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);  // base | dn << 16 | side << 20
   int *sCF = sLine + NFP;
@@ -286,6 +294,7 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VIS
   for (int i = tid; i < 2 * N; i += NT) {
     sE[i] = t.E1[i];
     sEF[i] = t.EFn1[i];
+    if (T::LPC) sCg[i] = t.lineCorr[i];
   }
   for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
   for (int i = tid; i < NFP / 2; i += NT) sPair[i] = t.linePair[i];
@@ -416,11 +425,67 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VIS
   }
 
   constexpr int NE = T::PAIR ? 2 : 1;  // flux points per work item
-  if constexpr (T::LP) {
+  if constexpr (T::LPC) {
     // C (LP): per (line, element), the line's N flux values of its
-    // direction once into registers; the divergence along the line at its N
-    // points replaces them in the flux tile (only this item reads them), and
-    // Fn - extrapolated normal flux is formed at both of its ends
+    // direction once into registers; Fn - extrapolated normal flux at both
+    // of its ends; then at its N points the divergence along the line plus
+    // the correction from both ends, which replaces the flux values in the
+    // flux tile (only this item reads them)
+    for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+      const int l = it / EB, fe = it - (it / EB) * EB;
+      const int pr = sPair[l];
+      const int ln = sLine[pr & 0xffff];
+      const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
+      const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+      R x[N][NF];
+#pragma unroll
+      for (int m = 0; m < N; m++) ldp<NF, R>(&sF[fidx(dn, base + m * stride) + fe * NF], x[m]);
+      R q[2][NF];
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        R acc[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+          const R ev = sEF[j * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[k] += ev * x[m][k];
+        }
+        const int f = j ? pr >> 16 : pr & 0xffff;
+        ldp<NF, R>(&sFn[f * ROW + fe * NF], q[j]);
+#pragma unroll
+        for (int k = 0; k < NF; k++) {
+          q[j][k] = q[j][k] - acc[k];
+          if (a.disFn_dbg && fe < nValid) a.disFn_dbg[((long long)f * E + e0 + fe) * NF + k] = q[j][k];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        R acc[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[k] = R(0);
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+          const R dv = sD[i * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[k] += dv * x[m][k];
+        }
+        const R c0 = sCg[i], c1 = sCg[N + i];
+#pragma unroll
+        for (int k = 0; k < NF; k++) {
+          R c = c0 * q[0][k];
+          c += c1 * q[1][k];
+          acc[k] = c + acc[k];
+        }
+        stp<NF, R>(&sF[fidx(dn, base + i * stride) + fe * NF], acc);
+      }
+    }
+  }
+  if constexpr (T::LP && !T::LPC) {
+    // C (LP without the correction): the divergence along the line at its N
+    // points replaces the flux values in the flux tile, and Fn - extrapolated
+    // normal flux is formed in place at both ends for the correction in D
     for (int it = tid; it < (NFP / 2) * EB; it += NT) {
       const int l = it / EB, fe = it - (it / EB) * EB;
       const int pr = sPair[l];
@@ -518,13 +583,14 @@ __global__ void __launch_bounds__(Tm<ND, P, R, V, VISC>::NT, Tm<ND, P, R, V, VIS
     }
   }
 
-  // D: correction and RK update at (s, el), in place in sU / sAcc / sCmp
+  // D: correction (LPC: already in the line sums) and RK update at (s, el),
+  // in place in sU / sAcc / sCmp
   {
     R cq[NF];
 #pragma unroll
     for (int k = 0; k < NF; k++) cq[k] = R(0);
 #pragma unroll
-    for (int fc = 0; fc < 2 * ND; fc++) {
+    for (int fc = 0; fc < (T::LPC ? 0 : 2 * ND); fc++) {
       const int fp = T::GTAB ? __ldg(&t.corrFpt[s * 2 * ND + fc]) : sCF[s * 2 * ND + fc];
       const R cv = T::GTAB ? __ldg(&t.corrVal[s * 2 * ND + fc]) : sCV[s * 2 * ND + fc];
       R x[NF];
