@@ -785,10 +785,15 @@ struct Tg2 {
   static constexpr int IN_END = O_DET + al(NS * EB);
   static constexpr int O_GF = O_U;
   static constexpr int O_G = IN_END > al(ND * NFP * ROW) ? IN_END : al(ND * NFP * ROW);
+  // 3-D: the reference gradient is formed per (line, element) with the
+  // correction values by side and index along the line (GLP), so the
+  // per-point correction tables are not staged
+  static constexpr bool GLP = ND == 3;
+  static constexpr int NCT = GLP ? 0 : NS * 2 * ND;
   static constexpr int O_TAB = O_G + al(ND * NS * ROW);
-  static constexpr int O_CV = O_TAB + al(N * N + 2 * N);
-  static constexpr int O_IDX = O_CV + al(NS * 2 * ND);
-  static constexpr int O_BAR = O_IDX + al((int)((NFP + NS * 2 * ND + NFP / 2) * 4 / sizeof(R)) + 1);
+  static constexpr int O_CV = O_TAB + al(N * N + 4 * N);
+  static constexpr int O_IDX = O_CV + al(NCT);
+  static constexpr int O_BAR = O_IDX + al((int)((NFP + NCT + NFP / 2) * 4 / sizeof(R)) + 1);
   static constexpr size_t SMEM = sizeof(R) * (size_t)(O_BAR + AL) + 128;
   static_assert(SMEM <= kMaxSmem, "gradient tile set does not fit in shared memory");
 };
@@ -810,10 +815,11 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
   R *sGf = smem + T::O_GF;    // [ND][NFP][ROW] at the flux points
   R *sD = smem + T::O_TAB;
   R *sE = sD + N * N;
+  R *sCg = sE + 2 * N;  // GLP: correction values by side and index along the line
   R *sCV = smem + T::O_CV;
   int *sLine = reinterpret_cast<int *>(smem + T::O_IDX);
   int *sCF = sLine + NFP;
-  int *sPair = sCF + NS * 2 * ND;  // side-0 fpt | side-1 fpt << 16 of each line
+  int *sPair = sCF + T::NCT;  // side-0 fpt | side-1 fpt << 16 of each line
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::O_BAR);
 
   const int e0 = blockIdx.x * EB;
@@ -835,10 +841,13 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
     tma_load_2d(sDet, &mp.det, e0, 0, &bar[0]);
   }
   for (int i = tid; i < N * N; i += NT) sD[i] = t.D[i];
-  for (int i = tid; i < 2 * N; i += NT) sE[i] = t.E1[i];
+  for (int i = tid; i < 2 * N; i += NT) {
+    sE[i] = t.E1[i];
+    if (T::GLP) sCg[i] = t.lineCorr[i];
+  }
   for (int i = tid; i < NFP; i += NT) sLine[i] = t.fptBase[i] | (t.fptDn[i] << 16) | (t.fptSide[i] << 20);
   for (int i = tid; i < NFP / 2; i += NT) sPair[i] = t.linePair[i];
-  for (int i = tid; i < NS * 2 * ND; i += NT) {
+  for (int i = tid; i < T::NCT; i += NT) {
     sCF[i] = t.corrFpt[i];
     sCV[i] = t.corrVal[i];
   }
@@ -860,8 +869,58 @@ __global__ void __launch_bounds__(Tg2<ND, P, R>::NT) k_grad_tma(int E, TpTablesT
   idx3[1] = ND > 1 ? (s / N) % N : 0;
   idx3[2] = ND > 2 ? s / (N * N) : 0;
   R gr[ND][NF];
+  if constexpr (T::GLP) {
+    // per (line, element): the line's N states once into registers; at its N
+    // points the reference gradient along the line plus the correction from
+    // the jumps at its two ends, in the order of the per-point form (the two
+    // faces normal to the line, the side-0 face first as in the hex face
+    // numbering; corrVal times -1 on side 0), into sG[dn][point]
+    for (int it = tid; it < (NFP / 2) * EB; it += NT) {
+      const int l = it / EB, fe = it - (it / EB) * EB;
+      const int pr = sPair[l];
+      const int f0 = pr & 0xffff, f1 = pr >> 16;
+      const int ln = sLine[f0];
+      const int base = ln & 0xffff, dn = (ln >> 16) & 0xf;
+      const int stride = dn == 0 ? 1 : (dn == 1 ? N : N * N);
+      R x[N][NF], q0[NF], q1[NF];
 #pragma unroll
-  for (int d = 0; d < ND; d++) {
+      for (int m = 0; m < N; m++)
+#pragma unroll
+        for (int k = 0; k < NF; k++) x[m][k] = sU[(base + m * stride) * ROW + fe * NF + k];
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        q0[k] = sC[f0 * ROW + fe * NF + k];
+        q1[k] = sC[f1 * ROW + fe * NF + k];
+      }
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        R acc[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc[k] = R(0.0);
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+          const R dv = sD[i * N + m];
+#pragma unroll
+          for (int k = 0; k < NF; k++) acc[k] += dv * x[m][k];
+        }
+        const R cv0 = sCg[i] * -R(1.0), cv1 = sCg[N + i] * R(1.0);
+#pragma unroll
+        for (int k = 0; k < NF; k++) {
+          R cq = R(0.0);
+          cq += cv0 * q0[k];
+          cq += cv1 * q1[k];
+          sG[(dn * NS + base + i * stride) * ROW + fe * NF + k] = cq + acc[k];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < ND; d++)
+#pragma unroll
+      for (int k = 0; k < NF; k++) gr[d][k] = sG[(d * NS + s) * ROW + el * NF + k];
+  }
+#pragma unroll
+  for (int d = 0; d < (T::GLP ? 0 : ND); d++) {
     const int stride = d == 0 ? 1 : (d == 1 ? N : N * N);
     const int base = s - idx3[d] * stride;
     const R *Dr = &sD[idx3[d] * N];
