@@ -138,6 +138,11 @@ struct fr_case {
   int EB = 1;
   frk::Phys ph{};
   cudaGraphExec_t graph = nullptr;
+  // kRunChunk steps in one graph, for runs of at least that many steps (one
+  // graph launch instead of kRunChunk)
+  static constexpr int kRunChunk = 10;
+  cudaGraphExec_t graphK = nullptr;
+  int graphKernelsK = 0;
   bool ownStream = false;
   bool hostOnly = false;  // set up without a device: setup arrays only
   // P-multigrid (reference: multigrid.cpp:47-384): coarse levels share the
@@ -270,6 +275,7 @@ struct fr_case {
     if (cp.copy) cudaStreamDestroy(cp.copy);
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
+    if (graphK) cudaGraphExecDestroy(graphK);
     levels.clear();  // coarse levels use this case's stream: release them first
     for (auto &b : allocs) {
       if (b.fp32) note_fp32(b.p, b.bytes, false);
@@ -1748,7 +1754,8 @@ struct fr_case {
       n--;
     }
     if (n <= 0) return true;
-    if (!graph) {
+    // the steady-state step (or kRunChunk of them) captured once
+    auto capture = [&](int steps, cudaGraphExec_t &exec, int &kernels) {
       if (!stream) return fail(FR_ERR_STATE, "graph capture needs a non-default stream");
       cudaGraph_t g;
       long long saveIter = iter;
@@ -1756,17 +1763,25 @@ struct fr_case {
       if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return fail(FR_ERR_CUDA, "begin capture");
       long long before = total_launches();
-      step_once();
-      graphKernels = (int)(total_launches() - before);
-      launches -= graphKernels;  // counted again at every replay
+      for (int i = 0; i < steps; i++) step_once();
+      kernels = (int)(total_launches() - before);
+      launches -= kernels;  // counted again at every replay
       if (cudaStreamEndCapture(stream, &g) != cudaSuccess) return fail(FR_ERR_CUDA, "end capture");
       iter = saveIter;
-      if (cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) {
+      if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
         cudaGraphDestroy(g);
         return fail(FR_ERR_CUDA, "graph instantiate");
       }
       cudaGraphDestroy(g);
+      return true;
+    };
+    if (n >= kRunChunk && !graphK && !capture(kRunChunk, graphK, graphKernelsK)) return false;
+    for (; n >= kRunChunk; n -= kRunChunk) {
+      iter += kRunChunk;
+      if (cudaGraphLaunch(graphK, stream) != cudaSuccess) return fail(FR_ERR_CUDA, "graph launch");
+      launches += graphKernelsK;
     }
+    if (n > 0 && !graph && !capture(1, graph, graphKernels)) return false;
     for (int i = 0; i < n; i++) {
       iter++;
       if (cudaGraphLaunch(graph, stream) != cudaSuccess) return fail(FR_ERR_CUDA, "graph launch");
@@ -2390,7 +2405,15 @@ int fr_set_stream(fr_case *c, void *stream) {
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
   }
+  if (c->graphK) {
+    cudaGraphExecDestroy(c->graphK);
+    c->graphK = nullptr;
+  }
   c->stream = (cudaStream_t)stream;
+  // the coarse P-multigrid levels run on the case's stream too (left on the
+  // old one, a captured step would miss their work)
+  for (auto &L : c->levels)
+    if (L) L->stream = c->stream;
   return FR_OK;
 }
 

@@ -88,6 +88,29 @@ def test_graph_run_equals_update_loop(case):
     assert np.array_equal(s1.get_state(), s2.get_state())
 
 
+@pytest.mark.parametrize("precision", [fb.FR_PREC_FP64, fb.FR_PREC_MIXED])
+@pytest.mark.parametrize("case", ["pmg_vortex2d_p3_8", "chbump_p2_pmg"])
+def test_pmg_run_on_caller_stream_equals_update_loop(case, precision):
+    """A P-multigrid case put on a stream of the caller's (fr_set_stream) and
+    advanced by fr_run in one eager step, one ten-step graph and two one-step
+    graphs gives the same bits as update() + pmg_cycle() on its own stream:
+    the coarse levels move to the caller's stream with the case."""
+    import torch
+
+    a, meta = load_golden(case)
+    s1, s2 = gpu_case(meta, precision=precision), gpu_case(meta, precision=precision)
+    st = torch.cuda.Stream()
+    s2.set_stream(st.cuda_stream)
+    s1.set_state(a["U_init"])
+    s2.set_state(a["U_init"])
+    n = 13
+    for _ in range(n):
+        s1.update()
+        s1.pmg_cycle()
+    s2.run(n)
+    assert np.array_equal(s1.get_state(), s2.get_state())
+
+
 @pytest.mark.parametrize("case", golden_cases())
 def test_initial_condition_matches_reference(case):
     a, meta = load_golden(case)
