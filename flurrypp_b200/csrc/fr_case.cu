@@ -1724,8 +1724,14 @@ struct fr_case {
       element_stage(frk::MODE_JAMESON, nRK - 1, in.RKa[nRK], 0.0, nRK == 1, pmgSource);
     else
       element_stage(frk::MODE_RK_FINAL, nRK - 1, 0.0, in.RKb[nRK - 1], nRK == 1, pmgSource);
-    frk::launch_add_time(dt, timeAcc, stream);
-    launches++;
+    // a coarse P-multigrid level's own time is read only by grid motion (each
+    // level advances its own copy of the time, multigrid.cpp:130-135 with
+    // solver.cpp:362): static levels skip the update, one launch fewer per
+    // coarse step (12 a driver step at P3 with two smoothing steps)
+    if (!pmgCoarse || in.motion) {
+      frk::launch_add_time(dt, timeAcc, stream);
+      launches++;
+    }
     fptsFresh = true;
     return cuda_ok("update");
   }
