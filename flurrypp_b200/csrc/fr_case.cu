@@ -826,9 +826,13 @@ struct fr_case {
 
   // solver::update with motion (src/solver.cpp:319-363): the metrics move
   // with every stage, and a standard RK step combines its stored stage
-  // residuals at the end with the last stage's metrics.
-  bool update_motion() {
+  // residuals at the end with the last stage's metrics.  A P-multigrid level
+  // moves its own mesh with its own time, which its updates advance
+  // (multigrid.cpp:130-135: every level solves with its own copy of the
+  // inputs), and adds its source term to each stage residual.
+  bool update_motion(bool pmgSource) {
     const double *eDt = in.dtType == 2 ? eleDt : nullptr;
+    const double *srcU = pmgSource ? src : nullptr;
     const long long nSE = (long long)nS * E;
     const bool jameson = in.timeType >= 5;
     for (int step = 0; step < nRK - 1; step++) {
@@ -836,7 +840,7 @@ struct fr_case {
       move_mesh(in.RKa[step]);
       if (step == 0) cudaMemcpyAsync(U0, U, (size_t)nSE * nF * sizeof(double), cudaMemcpyDeviceToDevice, stream);
       residual_motion(step);
-      frk::launch_motion_step_a(nSE, nF, E, U0, divF[step], detJ, dt, eDt, in.RKa[step + 1], U, stream);
+      frk::launch_motion_step_a(nSE, nF, E, U0, divF[step], srcU, detJ, dt, eDt, in.RKa[step + 1], U, stream);
       launches++;
     }
     move_mesh(in.RKa[nRK - 1]);
@@ -849,9 +853,9 @@ struct fr_case {
         stg.divF[s2] = divF[s2];
         stg.rkb[s2] = in.RKb[s2];
       }
-      frk::launch_motion_step_b(nSE, nF, E, nRK > 1 ? U0 : U, stg, detJ, dt, eDt, U, stream);
+      frk::launch_motion_step_b(nSE, nF, E, nRK > 1 ? U0 : U, stg, srcU, detJ, dt, eDt, U, stream);
     } else {
-      frk::launch_motion_step_a(nSE, nF, E, U0, divF[nRK - 1], detJ, dt, eDt, in.RKa[nRK], U, stream);
+      frk::launch_motion_step_a(nSE, nF, E, U0, divF[nRK - 1], srcU, detJ, dt, eDt, in.RKa[nRK], U, stream);
     }
     frk::launch_add_time(dt, timeAcc, stream);
     launches += 2;
@@ -1709,7 +1713,7 @@ struct fr_case {
 
   // solver::update (solver.cpp:319-363)
   bool update_once(bool pmgSource) {
-    if (mo.on) return update_motion();
+    if (mo.on) return update_motion(pmgSource);
     if (!fptsFresh) extrapolate();
     const bool jameson = in.timeType >= 5;
     for (int step = 0; step < nRK - 1; step++) {
@@ -1724,11 +1728,10 @@ struct fr_case {
       element_stage(frk::MODE_JAMESON, nRK - 1, in.RKa[nRK], 0.0, nRK == 1, pmgSource);
     else
       element_stage(frk::MODE_RK_FINAL, nRK - 1, 0.0, in.RKb[nRK - 1], nRK == 1, pmgSource);
-    // a coarse P-multigrid level's own time is read only by grid motion (each
-    // level advances its own copy of the time, multigrid.cpp:130-135 with
-    // solver.cpp:362): static levels skip the update, one launch fewer per
-    // coarse step (12 a driver step at P3 with two smoothing steps)
-    if (!pmgCoarse || in.motion) {
+    // a static coarse P-multigrid level's own time is never read (moving
+    // levels advance theirs in update_motion): one launch fewer per coarse
+    // step, 12 a driver step at P3 with two smoothing steps
+    if (!pmgCoarse) {
       frk::launch_add_time(dt, timeAcc, stream);
       launches++;
     }
@@ -3125,6 +3128,10 @@ int fr_read_restart(fr_case *c, const char *path) {
   if (c->mo.on) {  // the mesh at the restart time (src/solver.cpp:1855-1857)
     PdlScope pdlScope(c);
     c->move_mesh(0.0);
+    // P-multigrid levels keep their own time, which starts at zero: they copy
+    // the inputs before the finest level reads the restart file and reset
+    // their time in their own setup (multigrid.cpp:52, 131-136 with
+    // solver.cpp:76)
     if (!c->cuda_ok("restart")) return FR_ERR_CUDA;
   }
   return FR_OK;

@@ -232,8 +232,8 @@ bool finalize_input(Input &in, std::string &err) {
     err = "motion must be 0 (static) or one of the reference's laws 1..5";
     return false;
   }
-  if (in.motion != 0 && (in.viscous || in.riemannType != 0 || in.PMG)) {
-    err = "moving meshes run the inviscid Rusanov path without P-multigrid";
+  if (in.motion != 0 && (in.viscous || in.riemannType != 0)) {
+    err = "moving meshes run the inviscid Rusanov path";
     return false;
   }
   if (in.motion == 5 && in.nDims != 3) {

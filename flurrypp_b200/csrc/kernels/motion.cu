@@ -421,10 +421,30 @@ __global__ void k_motion_correct(MotionArgs m, const double *__restrict__ disFn,
   for (int k = 0; k < NF; k++) out[k] = acc[k] + out[k];
 }
 
-// U = U0 - RKval divF / detJ dt (timeStepA, src/solver.cpp:470-500).
+// U = U0 - RKval (divF + src) / detJ dt (timeStepA, src/solver.cpp:470-500;
+// src is the P-multigrid source term of a coarse level, or null).
 __global__ void k_motion_step_a(long long nSE, int nF, int E, const double *__restrict__ U0,
-                                const double *__restrict__ divF, const double *__restrict__ detJ,
-                                const double *__restrict__ dt, const double *__restrict__ eleDt, double rk,
+                                const double *__restrict__ divF, const double *__restrict__ src,
+                                const double *__restrict__ detJ, const double *__restrict__ dt,
+                                const double *__restrict__ eleDt, double rk, double *__restrict__ U) {
+  pdl_wait();
+  pdl_trigger();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nSE * nF) return;
+  const long long se = t / nF;
+  const double h = eleDt ? eleDt[se % E] : *dt;
+  const double d = src ? divF[t] + src[t] : divF[t];
+  U[t] = U0[t] - rk * d / detJ[se] * h;
+}
+
+// The final combination of a standard RK step: U = U0 (or U for a
+// one-stage scheme), then U -= RKb[s] divF[s] / detJ dt for every stage in
+// order, all with the metrics of the last stage (timeStepB, src/solver.cpp:344-355, 502-535).
+// A coarse P-multigrid level adds its source term to every stage residual
+// (src/solver.cpp:470-535 with PMG_Source).
+__global__ void k_motion_step_b(long long nSE, int nF, int E, const double *__restrict__ base,
+                                MotionStages st, const double *__restrict__ src, const double *__restrict__ detJ,
+                                const double *__restrict__ dt, const double *__restrict__ eleDt,
                                 double *__restrict__ U) {
   pdl_wait();
   pdl_trigger();
@@ -432,23 +452,11 @@ __global__ void k_motion_step_a(long long nSE, int nF, int E, const double *__re
   if (t >= nSE * nF) return;
   const long long se = t / nF;
   const double h = eleDt ? eleDt[se % E] : *dt;
-  U[t] = U0[t] - rk * divF[t] / detJ[se] * h;
-}
-
-// The final combination of a standard RK step: U = U0 (or U for a
-// one-stage scheme), then U -= RKb[s] divF[s] / detJ dt for every stage in
-// order, all with the metrics of the last stage (timeStepB, src/solver.cpp:344-355, 502-535).
-__global__ void k_motion_step_b(long long nSE, int nF, int E, const double *__restrict__ base,
-                                MotionStages st, const double *__restrict__ detJ, const double *__restrict__ dt,
-                                const double *__restrict__ eleDt, double *__restrict__ U) {
-  pdl_wait();
-  pdl_trigger();
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nSE * nF) return;
-  const long long se = t / nF;
-  const double h = eleDt ? eleDt[se % E] : *dt;
   double u = base[t];
-  for (int s = 0; s < st.n; s++) u -= st.rkb[s] * st.divF[s][t] / detJ[se] * h;
+  for (int s = 0; s < st.n; s++) {
+    const double d = src ? st.divF[s][t] + src[t] : st.divF[s][t];
+    u -= st.rkb[s] * d / detJ[se] * h;
+  }
   U[t] = u;
 }
 
@@ -511,17 +519,20 @@ void launch_motion_residual(const MotionArgs &m, const double *U, const double *
   }
 }
 
-void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const double *divF, const double *detJ,
-                          const double *dt, const double *eleDt, double rk, double *U, cudaStream_t st) {
+void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const double *divF, const double *src,
+                          const double *detJ, const double *dt, const double *eleDt, double rk, double *U,
+                          cudaStream_t st) {
   const long long n = nSE * nF;
-  if (n > 0) launch_k(k_motion_step_a, blocks_for(n, 256), 256, 0, st, nSE, nF, E, U0, divF, detJ, dt, eleDt, rk, U);
+  if (n > 0)
+    launch_k(k_motion_step_a, blocks_for(n, 256), 256, 0, st, nSE, nF, E, U0, divF, src, detJ, dt, eleDt, rk, U);
 }
 
 void launch_motion_step_b(long long nSE, int nF, int E, const double *base, const MotionStages &stages,
-                          const double *detJ, const double *dt, const double *eleDt, double *U, cudaStream_t st) {
+                          const double *src, const double *detJ, const double *dt, const double *eleDt, double *U,
+                          cudaStream_t st) {
   const long long n = nSE * nF;
   if (n > 0)
-    launch_k(k_motion_step_b, blocks_for(n, 256), 256, 0, st, nSE, nF, E, base, stages, detJ, dt, eleDt, U);
+    launch_k(k_motion_step_b, blocks_for(n, 256), 256, 0, st, nSE, nF, E, base, stages, src, detJ, dt, eleDt, U);
 }
 
 }  // namespace frk

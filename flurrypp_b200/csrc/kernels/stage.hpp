@@ -347,10 +347,13 @@ void launch_wavesp_motion(int nDims, int nFp, int E, const double *Uf, const dou
                           double gamma, double *waveSp, cudaStream_t st);
 void launch_motion_residual(const MotionArgs &m, const double *U, const double *Fn, double gamma, double *F,
                             double *disFn, double *divF, cudaStream_t st);
-void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const double *divF, const double *detJ,
-                          const double *dt, const double *eleDt, double rk, double *U, cudaStream_t st);
+// src: the P-multigrid source term added to every stage residual, or null
+void launch_motion_step_a(long long nSE, int nF, int E, const double *U0, const double *divF, const double *src,
+                          const double *detJ, const double *dt, const double *eleDt, double rk, double *U,
+                          cudaStream_t st);
 void launch_motion_step_b(long long nSE, int nF, int E, const double *base, const MotionStages &stages,
-                          const double *detJ, const double *dt, const double *eleDt, double *U, cudaStream_t st);
+                          const double *src, const double *detJ, const double *dt, const double *eleDt, double *U,
+                          cudaStream_t st);
 
 // ---- boundary monitors: wall forces and mass flux (monitor.cu) -----------
 template <typename R>

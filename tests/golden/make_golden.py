@@ -84,6 +84,9 @@ CASES = {
     "pmg_vortex2d_p3_8": ("pmg_vortex2d_p3_8", ["--ic", "vortex", "--vortex", "5,0,0,0.5"], 5, "all"),
     "pmg_tgv3d_p3_3": ("pmg_tgv3d_p3_3", ["--ic", "tgv", "--tgv-mach", "0.2", "--cfl-dt", "0.4"], 3, "all"),
     "chbump_p2_pmg": ("chbump_p2_pmg", [], 5, "all"),
+    "pmg_ns_vortex2d_p3": ("pmg_ns_vortex2d_p3", ["--ic", "vortex", "--vortex", "3,0,0,0.5", "--cfl-dt", "0.3"], 6,
+                           "all"),
+    "pmg_motion2d_p2": ("pmg_motion2d_p2", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 6, "all"),
     "chbump_p3": ("chbump_p3", ["--monitors"], 10, "all"),
     "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5", "--monitors"], 5, "all"),
     "curved2d_q2_p3": ("curved2d_q2_p3", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),

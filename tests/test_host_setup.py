@@ -139,10 +139,10 @@ def test_curved_element_shapes_refused_like_the_reference(tmp_path):
 
 
 @pytest.mark.parametrize("extra", ["viscous 1\nRe 100\nMachBound 0.2\nMachWall 0\n", "riemannType 1\n",
-                                   "PMG 1\nlowOrder 1\n", "motion 7\n"])
+                                   "motion 7\n"])
 def test_moving_mesh_option_limits(extra, tmp_path):
-    """Moving meshes run the inviscid Rusanov path without P-multigrid, with
-    one of the reference's laws 1..5; other combinations are refused."""
+    """Moving meshes run the inviscid Rusanov path (P-multigrid included),
+    with one of the reference's laws 1..5; other combinations are refused."""
     d = tmp_path / "m.deck"
     d.write_text(("motion 2\n" if "motion" not in extra else "") + extra +
                  open(deck_path({"deck": "vortex2d_p3_8"})).read())

@@ -295,6 +295,30 @@ def test_async_state_copy(precision):
     assert np.array_equal(pinned, s.get_state())
 
 
+def test_moving_mesh_pmg_run_equals_update_loop():
+    """A moving mesh with P-multigrid (every level moves its own mesh with its
+    own time): the graph-replayed run, ten steps per graph launch and then
+    single steps, equals update + pmg_cycle step by step, bit for bit, and
+    the reference after its six steps."""
+    a, meta = load_golden("pmg_motion2d_p2")
+    outs = []
+    for graph in (True, False):
+        s = gpu_case(meta)
+        s.set_state(a["U_init"])
+        if graph:
+            s.run(meta["steps"])
+            s.run(11)
+        else:
+            for i in range(meta["steps"] + 11):
+                s.update()
+                s.pmg_cycle()
+                if i == meta["steps"] - 1:
+                    assert rel_err(s.get_state(), a["U_final"]) < STEP_TOL
+        outs.append(s.get_state())
+    assert np.isfinite(outs[0]).all()
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_moving_mesh_cases_are_not_batched():
     a, meta = load_golden("motion1_2d_p3")
     s = gpu_case(meta)
