@@ -74,6 +74,10 @@ struct Input {
          nyBound = 0.0, nzBound = 0.0, MachWall = 0.0, nxWall = 1.0,
          nyWall = 0.0, nzWall = 0.0;
   double mu_inf = 0.0, rt_inf = 0.0, c_sth = 0.0, muBound = 0.0;
+  // the viscous free-stream values are non-dimensional (done once, when the
+  // deck is read, as input::readInputFile does; a Gmsh mesh read afterwards
+  // finalises the inputs again for its nDims)
+  bool nonDimensional = false;
   double uWall = 0.0, vWall = 0.0, wWall = 0.0;
   // mesh
   int meshType = 1;

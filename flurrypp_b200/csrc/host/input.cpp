@@ -284,8 +284,9 @@ bool finalize_input(Input &in, std::string &err) {
       return false;
   }
   if (in.nDims == 2) in.wBound = 0;
-  if (in.viscous) {
-    // Non-dimensionalisation (reference: src/input.cpp:526-596)
+  if (in.viscous && !in.nonDimensional) {
+    in.nonDimensional = true;
+    // Non-dimensionalisation (reference: src/input.cpp:521, 526-596)
     if (in.nDims == 2) in.nzBound = 0;
     double nMag = std::sqrt(in.nxBound * in.nxBound + in.nyBound * in.nyBound +
                             in.nzBound * in.nzBound);

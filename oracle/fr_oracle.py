@@ -644,6 +644,10 @@ def params_from_deck(path: str) -> dict:
         rhoRef = rhoB
         pRef = rhoRef * UB * UB
         muRef = rhoRef * UB * Lref
+        # the moving wall's velocity (src/input.cpp:551-554, 583-585)
+        UW = f("MachWall", 0.0) * np.sqrt(g * RGas * TWall)
+        nxW, nyW, nzW = f("nxWall", 1.0), f("nyWall", 0.0), f("nzWall", 0.0)
+        p.update(uWall=UW * nxW / UB, vWall=UW * nyW / UB, wWall=UW * nzW / UB)
         p.update(c_sth=SGas / TGas, mu_inf=muGas / muRef, rt_inf=TGas * RGas / (UB * UB),
                  RGas=RGas * TBound / (UB * UB), rhoBound=1.0, uBound=UB * nxB / UB, vBound=UB * nyB / UB,
                  wBound=UB * nzB / UB, pBound=pB / pRef, TWall=TWall / TBound,

@@ -88,6 +88,14 @@ CASES = {
                            "all"),
     "pmg_motion2d_p2": ("pmg_motion2d_p2", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 6, "all"),
     "chbump_p3": ("chbump_p3", ["--monitors"], 10, "all"),
+    # the reference's own Couette test deck (viscous, moving isothermal top
+    # wall, periodic sides, Jameson RK with local dt, P-multigrid)
+    "couette_p2_pmg": ("couette_p2_pmg", ["--monitors"], 10, "all"),
+    # the reference's runnable Cartesian-mesh test decks (tests/euler/vortex/
+    # input_vortex, input_vortex3D on a smaller box, tests/euler/wedge/input_supwall)
+    "ref_vortex2d_p3_20": ("ref_vortex2d_p3_20", [], 10, "all"),
+    "ref_vortex3d_p4_4": ("ref_vortex3d_p4_4", [], 6, "all"),
+    "ref_supwall_p1_30": ("ref_supwall_p1_30", ["--monitors"], 10, "all"),
     "wallchar3d_p2": ("wallchar3d_p2", ["--ic", "vortex", "--vortex", "0.3,0,0.4,0.35", "--cfl-dt", "0.5", "--monitors"], 5, "all"),
     "curved2d_q2_p3": ("curved2d_q2_p3", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),
     "curved2d_q4_p2": ("curved2d_q4_p2", ["--ic", "vortex", "--vortex", "3,5,5,0.3", "--cfl-dt", "0.5"], 10, "all"),
@@ -204,6 +212,13 @@ def write_meshes() -> None:
     from flurrypp_b200.meshgen import curved_box, write_gmsh_ho
     for name, (nd, n, q, length, ser) in CURVED.items():
         write_gmsh_ho(os.path.join(DECKS, name), curved_box(nd, n, q, length, serendipity=ser))
+    # the reference's Couette test geometry (tests/navier-stokes/couette/couette.geo:
+    # [-1, 1] x [0, 1], 4 x 2 quads), written here with lower-case physical names
+    from flurrypp_b200.meshgen import channel_bump, write_gmsh
+    m = channel_bump(4, 2, 0.0, -1.0, 1.0, 1.0)
+    m["edges"] = {"bottom": m["edges"]["bottom"], "top": m["edges"]["top"],
+                  "left": m["edges"]["inlet"], "right": m["edges"]["outlet"]}
+    write_gmsh(os.path.join(DECKS, "couette_4x2.msh"), m)
     for name, rel in REF_MESHES.items():
         src = os.path.join(REFERENCE, rel)
         if name.endswith(".gz"):
