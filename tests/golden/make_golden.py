@@ -91,6 +91,7 @@ CASES = {
     # the reference's own Couette test deck (viscous, moving isothermal top
     # wall, periodic sides, Jameson RK with local dt, P-multigrid)
     "couette_p2_pmg": ("couette_p2_pmg", ["--monitors"], 10, "all"),
+    "cyl_visc2d_p2": ("cyl_visc2d_p2", ["--monitors"], 6, "all"),
     # the reference's runnable Cartesian-mesh test decks (tests/euler/vortex/
     # input_vortex, input_vortex3D on a smaller box, tests/euler/wedge/input_supwall)
     "ref_vortex2d_p3_20": ("ref_vortex2d_p3_20", [], 10, "all"),
