@@ -351,8 +351,33 @@ def large_tgv(n: int = 16) -> None:
     print(f"{name}: {os.path.getsize(os.path.join(HERE, name + '.npz')) / 1e3:.0f} kB")
 
 
+# the reference's own test meshes that are too large to keep whole (NACA 0012,
+# 2,724 9-node quads at P4; the 3-D cylinder, 3,756 hexes at P2), run from the
+# deck's initial condition: per-element sums of the initial state, the
+# initial residual and the state after the steps, with the residual norms
+# and the boundary monitors after the steps
+def large_mesh_sums(deck: str, steps: int) -> None:
+    args = ["--monitors"]
+    with tempfile.TemporaryDirectory() as td, tempfile.TemporaryDirectory() as wd:
+        cmd = [HARNESS, stage_deck(deck, wd), td] + args + ["--steps", str(steps), "--norms"]
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        arrays, meta = read_dump(td)
+    out = {"divF_0_elem_sum": arrays["divF_0"].sum(axis=0), "U_init_elem_sum": arrays["U_init"].sum(axis=0),
+           "U_final_elem_sum": arrays["U_final"].sum(axis=0), "divF_0_absmax": np.abs(arrays["divF_0"]).max(axis=(0, 1)),
+           "F_spts_absmax": np.abs(arrays["F_spts"]).max(axis=(0, 1, 2)), "time_dt": arrays["time_dt"],
+           "res_norms": arrays["res_norms"], "res_norms_final": arrays["res_norms_final"],
+           "wall_force": arrays["wall_force"], "mass_flux": arrays["mass_flux"]}
+    name = f"{deck}_sums"
+    meta.update({"case": name, "deck": deck, "harness_args": args, "steps": steps})
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: {os.path.getsize(os.path.join(HERE, name + '.npz')) / 1e3:.0f} kB")
+
+
 EXTRA = {"restart_p2_to_p3": lambda: restart_across_orders(), "res_norms": reference_norms,
-         "tgv3d_p3_16_sums": lambda: large_tgv(16), "tgv3d_p3_32_sums": lambda: large_tgv(32)}
+         "tgv3d_p3_16_sums": lambda: large_tgv(16), "tgv3d_p3_32_sums": lambda: large_tgv(32),
+         "naca_p4_sums": lambda: large_mesh_sums("naca_p4", 10),
+         "cyl3d_p2_sums": lambda: large_mesh_sums("cyl3d_p2", 5)}
 
 
 def main(argv: list[str]) -> None:

@@ -446,3 +446,44 @@ def test_tgv_matches_reference_element_sums(n):
     s.calc_residual(0)
     for rt in (1, 2, 3):
         assert np.allclose(s.residual_norm(rt), z["res_norms_final"][rt - 1], rtol=1e-7, atol=0), rt
+
+
+@pytest.mark.parametrize("case", ["naca_p4_sums", "cyl3d_p2_sums"])
+def test_reference_test_meshes_match_element_sums(case, tmp_path):
+    """The reference's own NACA 0012 (2,724 9-node quads, P4, CFL-based dt)
+    and 3-D cylinder (3,756 hexes, P2) test meshes, from the deck's initial
+    condition: per-element sums of the initial state (1e-14), of the
+    residual (1e-12 of the flux scale) and of the state after the steps
+    (1e-10) against the reference's, the residual norms before and after,
+    and the boundary monitors after the steps."""
+    import json
+    import os
+
+    from conftest import ROOT
+
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import stage_deck  # the meshes are kept gzip-compressed
+
+    z = np.load(os.path.join(ROOT, "tests", "golden", f"{case}.npz"))
+    meta = json.loads(str(z["meta"]))
+    s = fb.Solver(stage_deck(meta["deck"], str(tmp_path)))
+    s.initialize_solution()
+    nS = s.shape[0]
+    assert rel_err(s.get_state().sum(axis=0), z["U_init_elem_sum"]) < 1e-14
+    s.calc_residual(0)
+    fscale = nS * max(float(z["divF_0_absmax"].max()), float(z["F_spts_absmax"].max()))
+    assert rel_err(s.get_residual(0).sum(axis=0), z["divF_0_elem_sum"], fscale) < RESID_TOL
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), z["res_norms"][rt - 1], rtol=1e-9, atol=0), rt
+    s.run(meta["steps"])
+    assert rel_err(s.get_state().sum(axis=0), z["U_final_elem_sum"]) < STEP_TOL
+    assert abs(s.info().time - z["time_dt"][0]) <= 1e-12 * max(1.0, abs(z["time_dt"][0]))
+    s.calc_residual(0)
+    for rt in (1, 2, 3):
+        assert np.allclose(s.residual_norm(rt), z["res_norms_final"][rt - 1], rtol=1e-7, atol=0), rt
+    want = z["wall_force"]
+    assert np.max(np.abs(s.wall_force() - want)) <= 1e-9 * max(np.max(np.abs(want)), 1e-3)
+    for norm in range(3):
+        got, flux = s.mass_flux(norm), z["mass_flux"][norm]
+        assert np.max(np.abs(got - flux)) <= 1e-10 * max(1.0, np.max(np.abs(flux))), (norm, got, flux)
