@@ -377,7 +377,8 @@ def large_mesh_sums(deck: str, steps: int) -> None:
 EXTRA = {"restart_p2_to_p3": lambda: restart_across_orders(), "res_norms": reference_norms,
          "tgv3d_p3_16_sums": lambda: large_tgv(16), "tgv3d_p3_32_sums": lambda: large_tgv(32),
          "naca_p4_sums": lambda: large_mesh_sums("naca_p4", 10),
-         "cyl3d_p2_sums": lambda: large_mesh_sums("cyl3d_p2", 5)}
+         "cyl3d_p2_sums": lambda: large_mesh_sums("cyl3d_p2", 5),
+         "cyl3d_visc_p2_sums": lambda: large_mesh_sums("cyl3d_visc_p2", 4)}
 
 
 def main(argv: list[str]) -> None:

@@ -448,7 +448,7 @@ def test_tgv_matches_reference_element_sums(n):
         assert np.allclose(s.residual_norm(rt), z["res_norms_final"][rt - 1], rtol=1e-7, atol=0), rt
 
 
-@pytest.mark.parametrize("case", ["naca_p4_sums", "cyl3d_p2_sums"])
+@pytest.mark.parametrize("case", ["naca_p4_sums", "cyl3d_p2_sums", "cyl3d_visc_p2_sums"])
 def test_reference_test_meshes_match_element_sums(case, tmp_path):
     """The reference's own NACA 0012 (2,724 9-node quads, P4, CFL-based dt)
     and 3-D cylinder (3,756 hexes, P2) test meshes, from the deck's initial
