@@ -122,6 +122,7 @@ CASES = {
                             10, "all"),
     "motion2_3d_p2": ("motion2_3d_p2", ["--ic", "vortex", "--vortex", "3,0.13,-0.21,0.5", "--cfl-dt", "0.5"], 4, "all"),
     "motion5_3d_p1": ("motion5_3d_p1", ["--ic", "vortex", "--vortex", "1,1.5,1.5,0.5"], 6, "all"),
+    "motion3_2d_p3": ("motion3_2d_p3", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 8, "all"),
     "err_ic1_2d_p3": ("err_ic1_2d_p3", ["--cfl-dt", "0.5", "--error"], 10, "all"),
     "err_ic2_2d_p3": ("err_ic2_2d_p3", ["--cfl-dt", "0.5", "--error"], 10, "all"),
     # the reference's own run of its icType 1 vortex at 32x32 P3, the deck's dt:
