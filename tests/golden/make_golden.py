@@ -78,6 +78,10 @@ CASES = {
     "ns_tgv3d_p2_4_perturbed": ("ns_tgv3d_p2_4", ["--ic", "tgv", "--tgv-mach", "0.1", "--perturb", "5,0.05",
                                                   "--cfl-dt", "0.3"], 4, "all"),
     "ns_tgv3d_p3_3": ("ns_tgv3d_p3_3", ["--ic", "tgv", "--tgv-mach", "0.1", "--cfl-dt", "0.3"], 3, "all"),
+    "ns_lobatto_hu3d_p3": ("ns_lobatto_hu3d_p3", ["--ic", "tgv", "--tgv-mach", "0.1", "--perturb", "29,0.05",
+                                                  "--cfl-dt", "0.3"], 3, "all"),
+    "ns_lobatto_sd2d_p3": ("ns_lobatto_sd2d_p3", ["--ic", "vortex", "--vortex", "3,0.2,-0.1,0.5", "--cfl-dt", "0.3"],
+                           8, "all"),
     "ns_vortex2d_p3_6": ("ns_vortex2d_p3_6", ["--ic", "vortex", "--vortex", "3,0,0,0.5", "--cfl-dt", "0.3"], 10, "all"),
     "ns_walls2d_p2": ("ns_walls2d_p2", ["--ic", "uniform", "--cfl-dt", "0.2", "--monitors"], 10, "all"),
     "ns_sutherland2d_p3": ("ns_sutherland2d_p3", ["--ic", "vortex", "--vortex", "2,0,0,0.3"], 10, "all"),
