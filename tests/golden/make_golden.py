@@ -91,6 +91,7 @@ CASES = {
     "pmg_ns_vortex2d_p3": ("pmg_ns_vortex2d_p3", ["--ic", "vortex", "--vortex", "3,0,0,0.5", "--cfl-dt", "0.3"], 6,
                            "all"),
     "pmg_motion2d_p2": ("pmg_motion2d_p2", ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"], 6, "all"),
+    "pmg_ns_tgv3d_p3": ("pmg_ns_tgv3d_p3", ["--ic", "tgv", "--tgv-mach", "0.1", "--cfl-dt", "0.3"], 3, "all"),
     "chbump_p3": ("chbump_p3", ["--monitors"], 10, "all"),
     # the reference's own Couette test deck (viscous, moving isothermal top
     # wall, periodic sides, Jameson RK with local dt, P-multigrid)
