@@ -214,6 +214,35 @@ def restart_across_orders() -> None:
     print(f"restart_p2_to_p3: {len(out) - 1} arrays")
 
 
+def restart_moving_pmg() -> None:
+    """restart_pmg_motion2d_p2: the moving-mesh P-multigrid case written by
+    the reference after 4 steps, then restarted from that file for 4 more
+    (the finest level takes the file's time and moves its mesh there; the
+    coarse levels, set up from the inputs before the file is read, keep
+    their own time from zero: flurry.cpp:103-114, multigrid.cpp:52,
+    131-136, solver.cpp:76); keeps the file and the reference's final state."""
+    base = open(os.path.join(DECKS, "pmg_motion2d_p2.deck")).read()
+    args = ["--ic", "vortex", "--vortex", "4,0.13,-0.21,0.5"]
+    with tempfile.TemporaryDirectory() as wd, tempfile.TemporaryDirectory() as td:
+        d1 = os.path.join(wd, "a.deck")
+        with open(d1, "w") as f:
+            f.write(base)
+        subprocess.run([HARNESS, d1, "-"] + args + ["--steps", "4", "--write-vtu", os.path.join(wd, "w")],
+                       check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        d2 = os.path.join(wd, "b.deck")
+        with open(d2, "w") as f:
+            f.write(f"restart 1\nrestartIter 4\ndataFileName {os.path.join(wd, 'w')}\n" + base)
+        subprocess.run([HARNESS, d2, td, "--steps", "4"], check=True, stdout=subprocess.DEVNULL, cwd=wd)
+        arrays, meta = read_dump(td)
+        out = {"ref_vtu_gz": gz_bytes(os.path.join(wd, "w_000000004.vtu")), "ref_U_restart": arrays["U_init"],
+               "U_restarted_final": arrays["U_final"], "time_dt_restarted": arrays["time_dt"]}
+    meta.update({"case": "restart_pmg_motion2d_p2", "deck": "pmg_motion2d_p2", "harness_args": [], "steps": 4,
+                 "restart_iter": 4})
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "restart_pmg_motion2d_p2.npz"), **out)
+    print(f"restart_pmg_motion2d_p2: {len(out) - 1} arrays")
+
+
 def write_meshes() -> None:
     sys.path.insert(0, ROOT)
     from flurrypp_b200.meshgen import curved_box, write_gmsh_ho
@@ -381,6 +410,7 @@ def large_mesh_sums(deck: str, steps: int) -> None:
 
 
 EXTRA = {"restart_p2_to_p3": lambda: restart_across_orders(), "res_norms": reference_norms,
+         "restart_pmg_motion2d_p2": lambda: restart_moving_pmg(),
          "tgv3d_p3_16_sums": lambda: large_tgv(16), "tgv3d_p3_32_sums": lambda: large_tgv(32),
          "naca_p4_sums": lambda: large_mesh_sums("naca_p4", 10),
          "cyl3d_p2_sums": lambda: large_mesh_sums("cyl3d_p2", 5),

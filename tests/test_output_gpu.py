@@ -159,6 +159,23 @@ def test_restart_across_orders_matches_the_reference(tmp_path):
     assert rel_err(s.get_state(), a["ref_U_restart"]) < 1e-14
 
 
+def test_moving_mesh_pmg_restart_matches_the_reference(tmp_path):
+    """A moving-mesh P-multigrid case restarted from the reference's file
+    after 4 steps and run 4 more: the finest level takes the file's time and
+    mesh position, the coarse levels keep their own time from zero (as the
+    reference's levels, set up before the file is read); the reference's
+    state and time after the 4 steps."""
+    a, meta = load_golden("restart_pmg_motion2d_p2")
+    s = case_solver(meta)
+    s.read_restart(ref_file(a, "ref_vtu_gz", tmp_path / "w.vtu"))
+    assert rel_err(s.get_state(), a["ref_U_restart"]) < 1e-14
+    for _ in range(meta["steps"]):
+        s.update()
+        s.pmg_cycle()
+    assert rel_err(s.get_state(), a["U_restarted_final"]) < 1e-10
+    assert abs(s.info().time - a["time_dt_restarted"][0]) <= 1e-12
+
+
 @pytest.mark.skipif(not os.path.exists(HARNESS), reason="reference build not present")
 @pytest.mark.parametrize("case", ["vortex2d_p3_8", "curved2d_q2_p3"])
 def test_reference_reads_the_product_file(case, tmp_path):
